@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 MSD radix string sort (one JSON line on rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload urls_50m|zipf_words_100m|uniform_1m]
+
+A step is one complete sort of the workload (perm + LCP) from inputs resident
+in HBM.  `value` is strings/s over the whole job; `e2e` repeats the
+measurement through the host-buffer entry point (ssort_sort_host) with the
+host<->device copies inside the timed region.  The plain sort is a
+single-GPU routine: with N GPUs every rank sorts its own replica of the
+workload ("replicas", weak scaling) and the time is the max over ranks.
+
+--impl reference times the reference's own msd_CE6 (compiled from its sources
+into oracle/_ref/libref.so) on the host cores, on a bounded sample of the same
+workload per step.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "string-sorting_b200"))
+
+import numpy as np  # noqa: E402
+
+import pyssort  # noqa: E402
+
+METRIC = "sort throughput (strings/s)"
+UNIT = "strings/s"
+DEFAULT_WORKLOAD = "urls_50m"
+CPU_SAMPLE = {"urls_50m": 4_000_000, "zipf_words_100m": 8_000_000, "uniform_1m": 1_000_000}
+DESCRIPTIONS = {
+    "urls_50m": "50,000,000 URLs: 'http://' + Zipf(1.1) host of 4,096 (8-24 [a-z]) + 1-6 "
+                "'/'-segments of 3-12 [a-z0-9]; seed 2; uint64 offsets",
+    "zipf_words_100m": "100,000,000 copies of Zipf(1.0) words from 1,000,000 distinct "
+                       "geometric(0.15)-length [a-z] words clipped to [1,24]; seed 3; uint64 offsets",
+    "uniform_1m": "1,000,000 strings, length U[1,20], bytes U{'a'..'z'}; seed 1",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(pyssort.WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---- clocks sampler -----------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---- algorithmic bytes -----------------------------------------------------------
+def kernel_bytes(st, w):
+    """Algorithmic bytes each kernel must move for one sort, from the per-kernel
+    string counts: gather reads idx (4) + offset (w) + 8 key bytes and writes the
+    key (8); count reads keys (8); scatter reads and writes key+idx (2x12);
+    on-chip sorts read idx (4) + offset (w) + 8 key bytes when they gather
+    themselves, or key+idx (12) otherwise, and write idx + lcp (8); equality
+    buckets copy idx (8) and/or write lcp (4)."""
+    fresh = st.tiny_fresh + st.small_fresh
+    keyed = st.tiny_keyed + st.small_keyed
+    return {
+        "gather": st.gather_elems * (4 + w + 8 + 8),
+        "count": st.partitioned * 8,
+        "scatter": st.partitioned * 24,
+        "small": (st.small_fresh * (4 + w + 8) + st.small_keyed * 12
+                  + (st.small_fresh + st.small_keyed) * 8),
+        "tiny": (st.tiny_fresh * (4 + w + 8) + st.tiny_keyed * 12
+                 + (st.tiny_fresh + st.tiny_keyed) * 8),
+        "equal": st.equal_moved * 8 + st.equal_final * 4,
+        "_sorts_total_elems": fresh + keyed,
+    }
+
+
+def sort_algorithmic_bytes(st, w):
+    """Bytes each round must touch: per live string idx (4) + offset (w) + key
+    (8) + one read and one write of (key, idx) (2x12); plus perm + lcp writes."""
+    live = [int(st.live[i]) for i in range(min(st.rounds, pyssort.SSORT_MAX_ROUNDS))]
+    return sum(m * (4 + w + 8 + 24) for m in live) + st.n * 8
+
+
+# ---- our arm ---------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank, dist):
+    import torch
+    torch.cuda.set_device(local_rank)
+    ss = pyssort.WORKLOADS[args.workload]()
+    n = ss.n
+    w = ss.offs.dtype.itemsize
+    arena_t = torch.from_numpy(ss.arena)
+    d_arena = arena_t.to(f"cuda:{local_rank}")
+    d_offs = torch.from_numpy(ss.offs.view(np.int64)).to(f"cuda:{local_rank}")
+    d_perm = torch.empty(n, dtype=torch.int32, device=f"cuda:{local_rank}")
+    d_lcp = torch.empty(n, dtype=torch.int32, device=f"cuda:{local_rank}")
+    sorter = pyssort.Sorter(local_rank)
+    stream = torch.cuda.Stream(device=local_rank)
+    ab = ss.arena.nbytes
+
+    def step():
+        sorter.sort_device(d_arena, ab, d_offs, w, n, d_perm, d_lcp, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local_rank)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    sorter.set_profiling(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        dist.barrier()
+    ktimes = sorter.kernel_times()
+    sorter.set_profiling(False)
+    st = sorter.stats()
+
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # ---- end to end through the host-buffer entry point (pinned buffers) ------
+    e2e = None
+    if not args.no_e2e:
+        h_arena = torch.empty(ab, dtype=torch.uint8, pin_memory=True)
+        h_arena.numpy()[:] = ss.arena
+        h_offs = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        h_offs.numpy()[:] = ss.offs.view(np.int64)
+        h_perm = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        h_lcp = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        na, no = h_arena.numpy(), h_offs.numpy().view(np.uint64)
+        pp, pl = h_perm.numpy().view(np.uint32), h_lcp.numpy().view(np.uint32)
+        sorter.sort_host(na, no, perm=pp, lcp=pl)  # warm the staging buffers
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sorter.sort_host(na, no, perm=pp, lcp=pl)
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": n * args.steps * world / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(ab + n * w), "d2h_bytes_per_step": int(n * 8),
+               "ms_per_step": 1000 * e2e_s / args.steps,
+               "api": "ssort_sort_host (pinned host buffers)"}
+    clocks.stop()
+
+    if rank != 0:
+        return None
+
+    # ---- roofline of the dominant kernel ---------------------------------------
+    peak, peak_kind = peaks()
+    kb = kernel_bytes(st, w)
+    per_kernel = {}
+    for name, (kms, launches) in ktimes.items():
+        entry = {"ms_total": round(kms, 4), "launches": int(launches),
+                 "ms_per_step": round(kms / args.steps, 4)}
+        if name in kb:
+            entry["algorithmic_bytes_per_step"] = int(kb[name])
+            entry["gbs"] = round(kb[name] * args.steps / (kms / 1e3) / 1e9, 1) if kms > 0 else None
+        per_kernel[name] = entry
+    timed = {k: v for k, v in per_kernel.items() if k in kb}
+    dom = max(timed, key=lambda k: timed[k]["ms_total"]) if timed else None
+    roofline = None
+    if dom:
+        d = per_kernel[dom]
+        per_launch_bytes = kb[dom] * args.steps / d["launches"]
+        per_launch_s = d["ms_total"] / 1e3 / d["launches"]
+        ach = per_launch_bytes / per_launch_s / 1e9
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
+                    "traffic": None, "algorithmic_bytes_per_launch": int(per_launch_bytes),
+                    "launch_ms": round(per_launch_s * 1e3, 4)}
+    sort_bytes = sort_algorithmic_bytes(st, w)
+    sort_s = ms / 1e3 / args.steps
+    sort_roof = {"bound": "hbm", "algorithmic_bytes_per_sort": int(sort_bytes),
+                 "achieved": round(sort_bytes / sort_s / 1e9, 1), "peak": peak,
+                 "frac": round(sort_bytes / sort_s / 1e9 / peak, 4),
+                 "frac_of_8tbs": round(sort_bytes / sort_s / 1e9 / 8000, 4),
+                 "formula": "sum_r m_r*(4+W+8+24) + n*8"}
+    launches = sum(v["launches"] * (3 if k == "scan" else 1) for k, v in per_kernel.items())
+
+    cpu = None
+    if not args.no_cpu and world == 1:
+        cpu = cpu_baseline(args.workload, ss)
+
+    lens_mean = ss.text_bytes / n - 1
+    out = {
+        "metric": METRIC, "value": n * args.steps * world / (ms / 1e3), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
+        "config": {"workload": args.workload, "description": DESCRIPTIONS.get(args.workload),
+                   "n_strings": n, "key_bytes": int(ss.text_bytes), "mean_len": round(lens_mean, 2),
+                   "offset_width": w, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": f"inputs larger than L2 (arena {ab / 1e9:.2f} GB)"},
+        "key_gbs": round(ss.text_bytes * args.steps * world / (ms / 1e3) / 1e9, 2),
+        "roofline": roofline, "sort_roofline": sort_roof, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(launches), "clocks": clocks.summary(),
+        "stats": {k: v for k, v in st.as_dict().items()}, "kernels": per_kernel,
+    }
+    return out
+
+
+def _ref_lib():
+    p = os.path.join(ROOT, "oracle", "_ref", "libref.so")
+    if not os.path.exists(p):
+        return None
+    L = ctypes.CDLL(p)
+    L.ref_time_sort.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_size_t]
+    L.ref_time_sort.restype = ctypes.c_double
+    return L
+
+
+def _port_lib():
+    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    L.oracle_sort_arena.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                    ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]
+    return L
+
+
+def time_cpu_sort(ss, m):
+    """Seconds for one sort of the first m strings: the reference's msd_CE6
+    timed around its routine call, or the oracle port when the reference
+    library is absent.  Returns (seconds, kind)."""
+    L = _ref_lib()
+    if L is not None:
+        s = L.ref_time_sort(b"msd_CE6", ss.arena.ctypes.data, ss.offs.ctypes.data, m)
+        if s < 0:
+            raise RuntimeError("reference sort failed")
+        return s, "reference"
+    P = _port_lib()
+    perm = np.empty(m, dtype=np.uint32)
+    t0 = time.perf_counter()
+    P.oracle_sort_arena(ss.arena.ctypes.data, ss.offs.ctypes.data, 8, m, perm.ctypes.data, None)
+    return time.perf_counter() - t0, "port"
+
+
+def cpu_baseline(workload, ss, reps=3):
+    m = min(ss.n, CPU_SAMPLE.get(workload, 2_000_000))
+    ts = []
+    kind = None
+    for _ in range(reps):
+        t, kind = time_cpu_sort(ss, m)
+        ts.append(t)
+    t = statistics.median(ts)
+    return {"value": m / t, "unit": UNIT, "cores": 1, "kind": kind,
+            "routine": "msd_CE6" if kind == "reference" else "oracle port of msd_CE6",
+            "sample": f"first {m:,} strings of {workload}, median of {reps} runs "
+                      f"({t:.3f} s each), single thread",
+            "host": {"cpu": cpu_model(), "nproc": os.cpu_count()}}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    ss = pyssort.WORKLOADS[args.workload]()
+    m = min(ss.n, CPU_SAMPLE.get(args.workload, 2_000_000))
+    for _ in range(args.warmup):
+        time_cpu_sort(ss, m)
+    total = 0.0
+    kind = None
+    for _ in range(args.steps):
+        t, kind = time_cpu_sort(ss, m)
+        total += t
+    v = m * args.steps / total
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
+        "config": {"workload": args.workload, "description": DESCRIPTIONS.get(args.workload),
+                   "n_strings": ss.n, "sample_strings": m},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+                         "routine": "msd_CE6 (single-threaded by design: function-static "
+                                    "bucket arrays, src/msd_ce.cpp:392)",
+                         "sample": f"first {m:,} strings of {args.workload} per step",
+                         "host": {"cpu": cpu_model(), "nproc": os.cpu_count()}},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                 device_id=torch.device(f"cuda:{local_rank}"))
+        dist = tdist
+    try:
+        out = run_ours(args, rank, world, local_rank, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,123 @@
+/*
+ * ssort_b200.h -- C ABI of the B200 MSD radix string sort (libssort_b200.so).
+ *
+ * Plain C: pointers, sizes and status codes only.  Every entry point that can
+ * fail returns an int status (SSORT_OK = 0, negative on error); the drop-in
+ * routine msd_gpu follows the reference's convention instead and aborts with
+ * a message, since struct routine::f has no return value.
+ *
+ * Sort contract (all entry points): the output order is the stable byte-order
+ * sort of the NUL-terminated strings, i.e. the order the reference's msd_CE6
+ * produces (rantala/string-sorting src/msd_ce.cpp:367-419; stable because its
+ * counting sort is, :396-397, and its insertion sort breaks ties on <=,
+ * src/util/insertion_sort.h:42).  Bytes compare as unsigned char.
+ * perm[k] is the input index of the k-th string in that order.  The LCP array
+ * uses the reference's lcp() (src/mergesort_lcp.cpp:88-100): lcp[0] = 0 and
+ * lcp[k] = number of equal leading bytes of strings perm[k-1] and perm[k],
+ * stopping at the first difference or at the NUL of the first string.
+ */
+#ifndef SSORT_B200_H
+#define SSORT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SSORT_OK 0
+#define SSORT_EINVAL (-1)    /* bad argument (null pointer, bad width, n too big) */
+#define SSORT_ENOMEM (-2)    /* device or pinned host allocation failed */
+#define SSORT_ECUDA (-3)     /* a CUDA runtime call failed */
+#define SSORT_ENODEV (-4)    /* no usable CUDA device */
+#define SSORT_EINTERNAL (-5) /* an internal consistency check failed */
+
+/* Largest number of strings one sort accepts (indices are 32-bit). */
+#define SSORT_MAX_N 0xFFFFFFFEull
+#define SSORT_MAX_ROUNDS 64
+
+typedef struct ssort_ctx ssort_ctx;
+
+/*
+ * Drop-in routine.  Same signature and contract as the reference's
+ * struct routine::f (src/routine.h:32-37), registered through
+ * ROUTINE_REGISTER_SINGLECORE(msd_gpu, ...) (src/routine.h:55-56) exactly
+ * where msd_CE6 registers (src/msd_ce.cpp:418-419).  Permutes strings[0..n)
+ * in place into stable byte order; never touches the string bytes.  Works on
+ * any pointers (one text buffer as in sortstring, or separately allocated
+ * strings as in unit-test/main.cpp:220-270).  Uses one process-wide context
+ * on the current CUDA device.  Aborts with a message on any CUDA error (the
+ * reference's convention, src/routines.c:33-40); there is no CPU fallback.
+ */
+void msd_gpu(unsigned char **strings, size_t n);
+
+/* Human-readable name of a status code, and the message of the last error
+ * raised on the calling thread. */
+const char *ssort_strerror(int status);
+const char *ssort_last_error(void);
+
+/* A context owns a CUDA stream and the device workspace; workspaces grow on
+ * demand and are reused across calls.  One context must not be used by two
+ * threads at once; separate contexts are independent. */
+int ssort_ctx_create(int device, ssort_ctx **out);
+void ssort_ctx_destroy(ssort_ctx *ctx);
+
+/*
+ * Device-resident sort: d_arena holds the strings (8-byte aligned base
+ * address, arena_bytes long), d_offs holds n offsets of width off_width
+ * (4 or 8 bytes; string i starts at d_arena + d_offs[i] and is NUL-terminated
+ * inside the arena).  Writes d_perm[n] and, if d_lcp is not NULL, d_lcp[n].
+ * `stream` is a cudaStream_t (NULL = the context's own stream).  Returns when
+ * the results are complete on the device.
+ */
+int ssort_sort_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                      const void *d_offs, int off_width, uint64_t n, uint32_t *d_perm,
+                      uint32_t *d_lcp, void *stream);
+
+/* The same from host buffers: copies arena and offsets to the device, sorts,
+ * and copies perm (and lcp when not NULL) back.  Pinned host buffers make the
+ * copies faster but are not required. */
+int ssort_sort_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes,
+                    const void *offs, int off_width, uint64_t n, uint32_t *perm,
+                    uint32_t *lcp);
+
+/* Pointer-array form behind msd_gpu with a status return: permutes
+ * strings[0..n) in place and, when lcp_out is not NULL, writes the LCP array
+ * of the sorted order. */
+int ssort_sort_strings(ssort_ctx *ctx, unsigned char **strings, size_t n, uint32_t *lcp_out);
+
+/* Per-call statistics of the last sort on this context. */
+typedef struct {
+    uint64_t n;                              /* strings sorted */
+    uint32_t rounds;                         /* 8-byte refinement rounds run */
+    uint32_t partition_levels;               /* sample-partition passes run */
+    uint64_t live[SSORT_MAX_ROUNDS];         /* strings live entering each round */
+    uint64_t partitioned;                    /* elements moved by partition scatters */
+    uint64_t small_segments;                 /* segments sorted on chip */
+    uint64_t device_bytes;                   /* device workspace currently held */
+    double device_ms;                        /* device time of the sort (events) */
+    /* strings handled per kernel, summed over rounds: keys gathered for large
+     * segments; strings sorted by warps / CTAs with keys loaded in the kernel
+     * ("fresh") or taken from the key buffer ("keyed"); equality-bucket
+     * strings moved between buffers / finalised; partition boundaries. */
+    uint64_t gather_elems;
+    uint64_t tiny_fresh, tiny_keyed, small_fresh, small_keyed;
+    uint64_t equal_moved, equal_final;
+    uint64_t boundaries;
+} ssort_stats;
+
+int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
+
+/* Kernel-level timing: when enabled, each kernel launch of a sort is bracketed
+ * by CUDA events and its time is accumulated per kernel name. */
+int ssort_set_profiling(ssort_ctx *ctx, int enabled);
+/* Fills up to max entries; returns the number of distinct kernels recorded. */
+int ssort_get_kernel_times(const ssort_ctx *ctx, const char **names, double *total_ms,
+                           uint64_t *launches, int max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSORT_B200_H */

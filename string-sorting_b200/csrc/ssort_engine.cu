@@ -1,0 +1,673 @@
+// ssort_engine.cu -- host side of the B200 MSD radix string sort: the context
+// and its device workspace, the round loop that drives the kernels, and the
+// C ABI declared in include/ssort_b200.h (including the drop-in routine
+// msd_gpu that registers through the reference's ROUTINE_REGISTER,
+// src/routine.h:41-59).
+#include "ssort_b200.h"
+#include "ssort_internal.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <omp.h>
+
+using namespace ssort;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(SSORT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define SS_CUDA(call)                                        \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+    } while (0)
+
+#define SS_TRY(call)                 \
+    do {                             \
+        int r_ = (call);             \
+        if (r_ != SSORT_OK) return r_; \
+    } while (0)
+
+struct DBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+struct HBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace
+
+struct ssort_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t st = nullptr;
+
+    // workspace
+    DBuf idx1, key0, key1, lcp, R, N, T, S, E, B, L, L2, spl, nspl, ntiles, cm_size, tile_base,
+        cm_base, tmp, cm, partials, ctr;
+    DBuf arena, offs, perm;  // staging for the host-buffer entry points
+    HBuf h_offs, h_arena, h_perm;
+    Counters *h_ctr = nullptr;
+
+    ssort_stats stats{};
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+
+    bool prof = false;
+    struct Rec {
+        const char *name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::map<std::string, std::pair<double, uint64_t>> ktimes;
+
+    int ensure(DBuf &b, size_t bytes) {
+        if (b.cap >= bytes) return SSORT_OK;
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&b.p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return fail(SSORT_ENOMEM, "device allocation of " + std::to_string(want) +
+                                          " bytes failed: " + cudaGetErrorString(e));
+        }
+        b.cap = want;
+        return SSORT_OK;
+    }
+
+    int ensure_host(HBuf &b, size_t bytes) {
+        if (b.cap >= bytes) return SSORT_OK;
+        if (b.p) cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        cudaError_t e = cudaHostAlloc(&b.p, std::max<size_t>(bytes, 256), cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return fail(SSORT_ENOMEM, "pinned host allocation failed");
+        }
+        b.cap = std::max<size_t>(bytes, 256);
+        return SSORT_OK;
+    }
+
+    cudaEvent_t pool_event() {
+        if (ev_used == ev_pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
+
+    void prof_begin(const char *name) {
+        if (!prof) return;
+        Rec r{name, pool_event(), pool_event()};
+        cudaEventRecord(r.a, st);
+        recs.push_back(r);
+    }
+    void prof_end() {
+        if (!prof) return;
+        cudaEventRecord(recs.back().b, st);
+    }
+    void prof_collect() {
+        for (auto &r : recs) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            auto &slot = ktimes[r.name];
+            slot.first += ms;
+            slot.second += 1;
+        }
+        recs.clear();
+        ev_used = 0;
+    }
+
+    int check_launch(const char *name) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, name);
+        return SSORT_OK;
+    }
+
+    int sync_counters() {
+        SS_CUDA(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        SS_CUDA(cudaStreamSynchronize(st));
+        return SSORT_OK;
+    }
+
+    int grid_for(int per_sm) const { return num_sms * per_sm; }
+
+    int reserve(uint32_t n, bool need_lcp);
+    int scan(const uint32_t *in, uint32_t *out, uint32_t n);
+    int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
+            uint32_t n, uint32_t *d_perm, uint32_t *d_lcp);
+};
+
+#define LAUNCH(ctx, name, call)                 \
+    do {                                        \
+        (ctx)->prof_begin(name);                \
+        call;                                   \
+        (ctx)->prof_end();                      \
+        SS_TRY((ctx)->check_launch(name));      \
+    } while (0)
+
+int ssort_ctx::reserve(uint32_t n, bool need_internal_lcp) {
+    const size_t half = (size_t)n / 2 + 2;
+    const size_t nlarge = (size_t)n / (SMALL_CAP + 1) + 2;
+    SS_TRY(ensure(idx1, (size_t)n * 4));
+    SS_TRY(ensure(key0, (size_t)n * 8));
+    SS_TRY(ensure(key1, (size_t)n * 8));
+    if (need_internal_lcp) SS_TRY(ensure(lcp, (size_t)n * 4));
+    SS_TRY(ensure(R, half * sizeof(Seg)));
+    SS_TRY(ensure(N, half * sizeof(Seg)));
+    SS_TRY(ensure(T, half * sizeof(Seg)));
+    SS_TRY(ensure(S, half * sizeof(Seg)));
+    SS_TRY(ensure(E, half * sizeof(Seg)));
+    SS_TRY(ensure(B, ((size_t)n + 2) * sizeof(uint2)));
+    SS_TRY(ensure(L, nlarge * sizeof(Seg)));
+    SS_TRY(ensure(L2, nlarge * sizeof(Seg)));
+    SS_TRY(ensure(spl, nlarge * SPL_STRIDE * sizeof(uint64_t)));
+    SS_TRY(ensure(nspl, nlarge * 4));
+    SS_TRY(ensure(ntiles, nlarge * 4));
+    SS_TRY(ensure(cm_size, nlarge * 4));
+    SS_TRY(ensure(cm_base, (nlarge + 1) * 4));
+    SS_TRY(ensure(tile_base, (half + 1) * 4));
+    SS_TRY(ensure(tmp, (half + 1) * 4));
+    SS_TRY(ensure(partials, (size_t)scan_partials_needed((uint32_t)half) * 4));
+    SS_TRY(ensure(ctr, sizeof(Counters)));
+    if (!h_ctr) {
+        SS_CUDA(cudaHostAlloc((void **)&h_ctr, sizeof(Counters), cudaHostAllocDefault));
+    }
+    return SSORT_OK;
+}
+
+int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n) {
+    SS_TRY(ensure(partials, (size_t)scan_partials_needed(n) * 4));
+    LAUNCH(this, "scan", launch_scan(in, out, n, (uint32_t *)partials.p, st));
+    return SSORT_OK;
+}
+
+// The round loop.  Every position's final index lands in d_perm (= idx[0]);
+// every lcp entry is written exactly once: inside a small/tiny sort or an
+// equality bucket for pairs in the same leaf, by the boundary pass for pairs
+// split by a partition, and lcp[0] = 0 up front.
+int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
+                   int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp) {
+    SS_TRY(reserve(n, d_lcp == nullptr));
+    SortArgs a{};
+    a.arena = arena_p;
+    a.arena_bytes = arena_bytes;
+    a.offs = offs_p;
+    a.off_width = off_width;
+    a.n = n;
+    a.idx[0] = d_perm;
+    a.idx[1] = (uint32_t *)idx1.p;
+    a.key[0] = (uint64_t *)key0.p;
+    a.key[1] = (uint64_t *)key1.p;
+    a.lcp = d_lcp ? d_lcp : (uint32_t *)lcp.p;
+
+    Seg *cur = (Seg *)R.p, *nxt = (Seg *)N.p;
+    Counters *dc = (Counters *)ctr.p;
+
+    LAUNCH(this, "iota", launch_iota(d_perm, n, st));
+    SS_CUDA(cudaMemsetAsync(a.lcp, 0, 4, st));
+    if (n < 2) return SSORT_OK;
+    Seg first{0, n, 0, 0};
+    SS_CUDA(cudaMemcpyAsync(cur, &first, sizeof(Seg), cudaMemcpyHostToDevice, st));
+    uint32_t n_cur = 1;
+    uint64_t live = n;
+    uint32_t round = 0;
+
+    while (n_cur) {
+        if (round < SSORT_MAX_ROUNDS) stats.live[round] = live;
+        SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+        LAUNCH(this, "classify",
+               launch_classify(cur, n_cur, (Seg *)T.p, (Seg *)S.p, (Seg *)L.p, dc, st));
+        SS_TRY(sync_counters());
+        uint32_t n_large = h_ctr->n_large;
+        Seg *lcur = (Seg *)L.p, *lnext = (Seg *)L2.p;
+        if (n_large) {
+            // Keys of the large segments at this depth.
+            LAUNCH(this, "tile_counts",
+                   launch_tile_counts(lcur, n_large, GATHER_TILE, (uint32_t *)tmp.p, st));
+            SS_TRY(scan((uint32_t *)tmp.p, (uint32_t *)tile_base.p, n_large));
+            uint32_t total_tiles = 0;
+            SS_CUDA(cudaMemcpyAsync(&total_tiles, (uint32_t *)tile_base.p + n_large, 4,
+                                    cudaMemcpyDeviceToHost, st));
+            SS_CUDA(cudaStreamSynchronize(st));
+            LAUNCH(this, "gather",
+                   launch_gather(a, lcur, n_large, (const uint32_t *)tile_base.p, total_tiles,
+                                 std::min<uint32_t>(total_tiles, grid_for(8)), st));
+        }
+        uint32_t levels_this_round = 0;
+        while (n_large) {
+            // Every level strictly shrinks each range bucket (its splitter keys
+            // leave for equality buckets), so this bound is never reached on
+            // valid input; it turns a logic error into a status, not a hang.
+            if (++levels_this_round > 4096)
+                return fail(SSORT_EINTERNAL, "partition levels exceeded 4096");
+            stats.partition_levels++;
+            LAUNCH(this, "sample",
+                   launch_sample(a, lcur, n_large, (uint64_t *)spl.p, (uint32_t *)nspl.p,
+                                 (uint32_t *)ntiles.p, (uint32_t *)cm_size.p, st));
+            SS_TRY(scan((const uint32_t *)ntiles.p, (uint32_t *)tile_base.p, n_large));
+            SS_TRY(scan((const uint32_t *)cm_size.p, (uint32_t *)cm_base.p, n_large));
+            uint32_t totals[2] = {0, 0};
+            SS_CUDA(cudaMemcpyAsync(&totals[0], (uint32_t *)tile_base.p + n_large, 4,
+                                    cudaMemcpyDeviceToHost, st));
+            SS_CUDA(cudaMemcpyAsync(&totals[1], (uint32_t *)cm_base.p + n_large, 4,
+                                    cudaMemcpyDeviceToHost, st));
+            SS_CUDA(cudaStreamSynchronize(st));
+            const uint32_t total_tiles = totals[0], cm_total = totals[1];
+            SS_TRY(ensure(cm, ((size_t)cm_total + 1) * 4));
+            const int pg = std::min<uint32_t>(total_tiles, grid_for(4));
+            LAUNCH(this, "count",
+                   launch_count(a, lcur, n_large, (const uint32_t *)tile_base.p, total_tiles,
+                                (const uint64_t *)spl.p, (const uint32_t *)nspl.p,
+                                (const uint32_t *)cm_base.p, (uint32_t *)cm.p, pg, st));
+            SS_TRY(scan((const uint32_t *)cm.p, (uint32_t *)cm.p, cm_total));
+            LAUNCH(this, "scatter",
+                   launch_scatter(a, lcur, n_large, (const uint32_t *)tile_base.p, total_tiles,
+                                  (const uint64_t *)spl.p, (const uint32_t *)nspl.p,
+                                  (const uint32_t *)cm_base.p, (const uint32_t *)cm.p, pg, st));
+            LAUNCH(this, "emit",
+                   launch_emit(a, lcur, n_large, (const uint32_t *)tile_base.p,
+                               (const uint32_t *)nspl.p, (const uint32_t *)cm_base.p,
+                               (const uint32_t *)cm.p, (Seg *)T.p, (Seg *)S.p, lnext, (Seg *)E.p,
+                               (uint2 *)B.p, dc, st));
+            SS_TRY(sync_counters());
+            n_large = h_ctr->n_large_next;
+            SS_CUDA(cudaMemsetAsync(&dc->n_large_next, 0, 4, st));
+            std::swap(lcur, lnext);
+        }
+        const uint32_t nT = h_ctr->n_tiny, nS = h_ctr->n_small, nE = h_ctr->n_equal,
+                       nB = h_ctr->n_bound;
+        stats.small_segments += nT + nS;
+        LAUNCH(this, "tiny", launch_tiny(a, (Seg *)T.p, nT, nxt, dc, grid_for(8), st));
+        LAUNCH(this, "small", launch_small(a, (Seg *)S.p, nS, nxt, dc, grid_for(8), st));
+        if (nE) {
+            LAUNCH(this, "tile_counts",
+                   launch_tile_counts((Seg *)E.p, nE, EQ_TILE, (uint32_t *)tmp.p, st));
+            SS_TRY(scan((uint32_t *)tmp.p, (uint32_t *)tile_base.p, nE));
+            uint32_t total_tiles = 0;
+            SS_CUDA(cudaMemcpyAsync(&total_tiles, (uint32_t *)tile_base.p + nE, 4,
+                                    cudaMemcpyDeviceToHost, st));
+            SS_CUDA(cudaStreamSynchronize(st));
+            LAUNCH(this, "equal",
+                   launch_equal(a, (Seg *)E.p, nE, (const uint32_t *)tile_base.p, total_tiles,
+                                nxt, dc, grid_for(8), st));
+        }
+        LAUNCH(this, "boundary", launch_boundary(a, (uint2 *)B.p, nB, st));
+        SS_TRY(sync_counters());
+        stats.partitioned += h_ctr->partitioned;
+        stats.gather_elems += h_ctr->gather_elems;
+        stats.tiny_fresh += h_ctr->tiny_fresh;
+        stats.tiny_keyed += h_ctr->tiny_keyed;
+        stats.small_fresh += h_ctr->small_fresh;
+        stats.small_keyed += h_ctr->small_keyed;
+        stats.equal_moved += h_ctr->equal_moved;
+        stats.equal_final += h_ctr->equal_final;
+        stats.boundaries += nB;
+        n_cur = h_ctr->n_next;
+        live = h_ctr->live_next;
+        std::swap(cur, nxt);
+        ++round;
+    }
+    stats.rounds = round;
+    return SSORT_OK;
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+
+int validate_common(ssort_ctx *ctx, int off_width, uint64_t n) {
+    if (!ctx) return fail(SSORT_EINVAL, "null context");
+    if (off_width != 4 && off_width != 8) return fail(SSORT_EINVAL, "off_width must be 4 or 8");
+    if (n > SSORT_MAX_N) return fail(SSORT_EINVAL, "n exceeds SSORT_MAX_N");
+    return SSORT_OK;
+}
+
+int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                     const void *d_offs, int off_width, uint64_t n, uint32_t *d_perm,
+                     uint32_t *d_lcp) {
+    ctx->stats = ssort_stats{};
+    ctx->stats.n = n;
+    SS_CUDA(cudaEventRecord(ctx->ev_start, ctx->st));
+    int rc = ctx->run(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, d_perm, d_lcp);
+    if (rc != SSORT_OK) {
+        cudaStreamSynchronize(ctx->st);
+        ctx->recs.clear();
+        ctx->ev_used = 0;
+        return rc;
+    }
+    SS_CUDA(cudaEventRecord(ctx->ev_stop, ctx->st));
+    SS_CUDA(cudaStreamSynchronize(ctx->st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+    ctx->stats.device_ms = ms;
+    if (ctx->prof) ctx->prof_collect();
+    size_t held = 0;
+    for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->T,
+                    &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
+                    &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
+                    &ctx->cm, &ctx->partials, &ctx->arena, &ctx->offs, &ctx->perm})
+        held += b->cap;
+    ctx->stats.device_bytes = held;
+    return SSORT_OK;
+}
+
+// Run fn with the context's device current, restoring the caller's device.
+template <class F>
+int with_device(ssort_ctx *ctx, F fn) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ctx->device) cudaSetDevice(ctx->device);
+    int rc = fn();
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    return rc;
+}
+
+// Readable mappings of this process, for the drop-in's one-span fast path.
+bool span_is_readable(uintptr_t lo, uintptr_t hi) {
+    FILE *f = std::fopen("/proc/self/maps", "r");
+    if (!f) return false;
+    std::vector<std::pair<uintptr_t, uintptr_t>> rd;
+    char line[512];
+    while (std::fgets(line, sizeof line, f)) {
+        unsigned long a, b;
+        char perm[8] = {0};
+        if (std::sscanf(line, "%lx-%lx %7s", &a, &b, perm) == 3 && perm[0] == 'r')
+            rd.emplace_back((uintptr_t)a, (uintptr_t)b);
+    }
+    std::fclose(f);
+    std::sort(rd.begin(), rd.end());
+    uintptr_t cur = lo;
+    for (auto &m : rd) {
+        if (m.second <= cur) continue;
+        if (m.first > cur) return false;
+        cur = m.second;
+        if (cur >= hi) return true;
+    }
+    return cur >= hi;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ssort_strerror(int status) {
+    switch (status) {
+        case SSORT_OK: return "ok";
+        case SSORT_EINVAL: return "invalid argument";
+        case SSORT_ENOMEM: return "out of memory";
+        case SSORT_ECUDA: return "CUDA error";
+        case SSORT_ENODEV: return "no CUDA device";
+        case SSORT_EINTERNAL: return "internal error";
+        default: return "unknown status";
+    }
+}
+
+const char *ssort_last_error(void) { return g_last_error.c_str(); }
+
+int ssort_ctx_create(int device, ssort_ctx **out) {
+    if (!out) return fail(SSORT_EINVAL, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SSORT_ENODEV, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(SSORT_EINVAL, "device index out of range");
+    ssort_ctx *ctx = new ssort_ctx();
+    ctx->device = device;
+    int rc = with_device(ctx, [&]() -> int {
+        SS_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+        SS_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+        SS_CUDA(cudaEventCreate(&ctx->ev_start));
+        SS_CUDA(cudaEventCreate(&ctx->ev_stop));
+        ctx->st = ctx->own_stream;
+        return SSORT_OK;
+    });
+    if (rc != SSORT_OK) {
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return SSORT_OK;
+}
+
+void ssort_ctx_destroy(ssort_ctx *ctx) {
+    if (!ctx) return;
+    with_device(ctx, [&]() -> int {
+        if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+        for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->T,
+                        &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
+                        &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
+                        &ctx->cm, &ctx->partials, &ctx->ctr, &ctx->arena, &ctx->offs,
+                        &ctx->perm})
+            if (b->p) cudaFree(b->p);
+        for (HBuf *b : {&ctx->h_offs, &ctx->h_arena, &ctx->h_perm})
+            if (b->p) cudaFreeHost(b->p);
+        if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
+        for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+        if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+        if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        return SSORT_OK;
+    });
+    delete ctx;
+}
+
+int ssort_sort_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                      const void *d_offs, int off_width, uint64_t n, uint32_t *d_perm,
+                      uint32_t *d_lcp, void *stream) {
+    SS_TRY(validate_common(ctx, off_width, n));
+    if (n == 0) return SSORT_OK;
+    if (!d_arena || !d_offs || !d_perm) return fail(SSORT_EINVAL, "null device buffer");
+    if (((uintptr_t)d_arena & 7) != 0) return fail(SSORT_EINVAL, "arena must be 8-byte aligned");
+    return with_device(ctx, [&]() -> int {
+        ctx->st = stream ? (cudaStream_t)stream : ctx->own_stream;
+        int rc = sort_device_impl(ctx, d_arena, arena_bytes, d_offs, off_width, n, d_perm, d_lcp);
+        ctx->st = ctx->own_stream;
+        return rc;
+    });
+}
+
+int ssort_sort_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes, const void *offs,
+                    int off_width, uint64_t n, uint32_t *perm, uint32_t *lcp) {
+    SS_TRY(validate_common(ctx, off_width, n));
+    if (n == 0) return SSORT_OK;
+    if (!arena || !offs || !perm) return fail(SSORT_EINVAL, "null host buffer");
+    return with_device(ctx, [&]() -> int {
+        ctx->st = ctx->own_stream;
+        // Device arena: the bytes plus 16 zero bytes of padding.
+        SS_TRY(ctx->ensure(ctx->arena, arena_bytes + 16));
+        SS_TRY(ctx->ensure(ctx->offs, n * off_width));
+        SS_TRY(ctx->ensure(ctx->perm, n * 4 * (lcp ? 2 : 1)));
+        uint8_t *d_arena = (uint8_t *)ctx->arena.p;
+        uint32_t *d_perm = (uint32_t *)ctx->perm.p;
+        uint32_t *d_lcp = lcp ? d_perm + n : nullptr;
+        SS_CUDA(cudaMemcpyAsync(d_arena, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->st));
+        SS_CUDA(cudaMemsetAsync(d_arena + arena_bytes, 0, 16, ctx->st));
+        SS_CUDA(cudaMemcpyAsync(ctx->offs.p, offs, n * off_width, cudaMemcpyHostToDevice, ctx->st));
+        SS_TRY(sort_device_impl(ctx, d_arena, arena_bytes + 16, ctx->offs.p, off_width, n, d_perm,
+                                d_lcp));
+        SS_CUDA(cudaMemcpyAsync(perm, d_perm, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        if (lcp) SS_CUDA(cudaMemcpyAsync(lcp, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        SS_CUDA(cudaStreamSynchronize(ctx->st));
+        return SSORT_OK;
+    });
+}
+
+int ssort_sort_strings(ssort_ctx *ctx, unsigned char **strings, size_t n, uint32_t *lcp_out) {
+    if (!ctx) return fail(SSORT_EINVAL, "null context");
+    if (n > SSORT_MAX_N) return fail(SSORT_EINVAL, "n exceeds SSORT_MAX_N");
+    if (n == 0) return SSORT_OK;
+    if (!strings) return fail(SSORT_EINVAL, "null string array");
+    for (size_t i = 0; i < n; ++i)
+        if (!strings[i]) return fail(SSORT_EINVAL, "null string pointer at index " + std::to_string(i));
+    if (n == 1) {
+        if (lcp_out) lcp_out[0] = 0;
+        return SSORT_OK;
+    }
+    return with_device(ctx, [&]() -> int {
+        ctx->st = ctx->own_stream;
+        const int64_t nn = (int64_t)n;
+        // One readable span holding every string (sortstring's single text
+        // buffer, src/sortstring.c:310-335): ship the span as is.  Otherwise
+        // (e.g. separately strdup'd strings, unit-test/main.cpp:220-270) pack
+        // the strings into a pinned staging arena.
+        uintptr_t lo = UINTPTR_MAX, hi_start = 0;
+#pragma omp parallel for reduction(min : lo) reduction(max : hi_start) if (nn > 100000)
+        for (int64_t i = 0; i < nn; ++i) {
+            const uintptr_t p = (uintptr_t)strings[i];
+            lo = std::min(lo, p);
+            hi_start = std::max(hi_start, p);
+        }
+        const uintptr_t hi = hi_start + std::strlen((const char *)hi_start) + 1;
+        const uint64_t span = hi - lo;
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const bool use_span = span <= (uint64_t)free_b / 4 && span_is_readable(lo, hi);
+        const uint8_t *src;
+        uint64_t bytes;
+        int ow;
+        if (use_span) {
+            ow = span < 0xFFFFFFF0ull ? 4 : 8;
+            SS_TRY(ctx->ensure_host(ctx->h_offs, n * ow));
+            if (ow == 4) {
+                uint32_t *o = (uint32_t *)ctx->h_offs.p;
+#pragma omp parallel for if (nn > 100000)
+                for (int64_t i = 0; i < nn; ++i) o[i] = (uint32_t)((uintptr_t)strings[i] - lo);
+            } else {
+                uint64_t *o = (uint64_t *)ctx->h_offs.p;
+#pragma omp parallel for if (nn > 100000)
+                for (int64_t i = 0; i < nn; ++i) o[i] = (uint64_t)((uintptr_t)strings[i] - lo);
+            }
+            src = (const uint8_t *)lo;
+            bytes = span;
+        } else {
+            std::vector<uint64_t> len(n);
+#pragma omp parallel for if (nn > 100000)
+            for (int64_t i = 0; i < nn; ++i) len[i] = std::strlen((const char *)strings[i]) + 1;
+            uint64_t total = 0;
+            for (size_t i = 0; i < n; ++i) {
+                const uint64_t l = len[i];
+                len[i] = total;
+                total += l;
+            }
+            ow = total < 0xFFFFFFF0ull ? 4 : 8;
+            SS_TRY(ctx->ensure_host(ctx->h_offs, n * ow));
+            SS_TRY(ctx->ensure_host(ctx->h_arena, total));
+            uint8_t *dst = (uint8_t *)ctx->h_arena.p;
+#pragma omp parallel for if (nn > 100000)
+            for (int64_t i = 0; i < nn; ++i) {
+                const uint64_t o = len[i];
+                const uint64_t l = (i + 1 < nn ? len[i + 1] : total) - o;
+                std::memcpy(dst + o, strings[i], l);
+                if (ow == 4)
+                    ((uint32_t *)ctx->h_offs.p)[i] = (uint32_t)o;
+                else
+                    ((uint64_t *)ctx->h_offs.p)[i] = o;
+            }
+            src = dst;
+            bytes = total;
+        }
+        SS_TRY(ctx->ensure_host(ctx->h_perm, n * 4));
+        uint32_t *perm = (uint32_t *)ctx->h_perm.p;
+        // Device copies of the arena, offsets and results.
+        SS_TRY(ctx->ensure(ctx->arena, bytes + 16));
+        SS_TRY(ctx->ensure(ctx->offs, n * ow));
+        SS_TRY(ctx->ensure(ctx->perm, n * 4 * (lcp_out ? 2 : 1)));
+        uint8_t *d_arena = (uint8_t *)ctx->arena.p;
+        uint32_t *d_perm = (uint32_t *)ctx->perm.p;
+        uint32_t *d_lcp = lcp_out ? d_perm + n : nullptr;
+        SS_CUDA(cudaMemcpyAsync(d_arena, src, bytes, cudaMemcpyHostToDevice, ctx->st));
+        SS_CUDA(cudaMemsetAsync(d_arena + bytes, 0, 16, ctx->st));
+        SS_CUDA(cudaMemcpyAsync(ctx->offs.p, ctx->h_offs.p, n * ow, cudaMemcpyHostToDevice,
+                                ctx->st));
+        SS_TRY(sort_device_impl(ctx, d_arena, bytes + 16, ctx->offs.p, ow, n, d_perm, d_lcp));
+        SS_CUDA(cudaMemcpyAsync(perm, d_perm, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        if (lcp_out)
+            SS_CUDA(cudaMemcpyAsync(lcp_out, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        SS_CUDA(cudaStreamSynchronize(ctx->st));
+        std::vector<unsigned char *> orig(strings, strings + n);
+#pragma omp parallel for if (nn > 100000)
+        for (int64_t i = 0; i < nn; ++i) strings[i] = orig[perm[i]];
+        return SSORT_OK;
+    });
+}
+
+int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out) {
+    if (!ctx || !out) return fail(SSORT_EINVAL, "null argument");
+    *out = ctx->stats;
+    return SSORT_OK;
+}
+
+int ssort_set_profiling(ssort_ctx *ctx, int enabled) {
+    if (!ctx) return fail(SSORT_EINVAL, "null context");
+    ctx->prof = enabled != 0;
+    if (!ctx->prof) ctx->ktimes.clear();
+    return SSORT_OK;
+}
+
+int ssort_get_kernel_times(const ssort_ctx *ctx, const char **names, double *total_ms,
+                           uint64_t *launches, int max) {
+    if (!ctx) return fail(SSORT_EINVAL, "null context");
+    int i = 0;
+    for (auto &kv : ctx->ktimes) {
+        if (i < max) {
+            if (names) names[i] = kv.first.c_str();
+            if (total_ms) total_ms[i] = kv.second.first;
+            if (launches) launches[i] = kv.second.second;
+        }
+        ++i;
+    }
+    return i;
+}
+
+// The drop-in routine (struct routine::f, src/routine.h:33).
+void msd_gpu(unsigned char **strings, size_t n) {
+    static std::mutex mu;
+    static ssort_ctx *ctx = nullptr;
+    if (n < 2) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ctx) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int rc = ssort_ctx_create(dev, &ctx);
+        if (rc != SSORT_OK) {
+            std::fprintf(stderr, "msd_gpu: %s: %s\n", ssort_strerror(rc), ssort_last_error());
+            std::abort();
+        }
+    }
+    int rc = ssort_sort_strings(ctx, strings, n, nullptr);
+    if (rc != SSORT_OK) {
+        std::fprintf(stderr, "msd_gpu: %s: %s\n", ssort_strerror(rc), ssort_last_error());
+        std::abort();
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,292 @@
+"""ctypes binding of libssort_b200.so (the C ABI in include/ssort_b200.h) and of
+the synthetic workload generators in libssort_workloads.so.
+
+This is the Python face of the product path used by the tests and the
+benchmark.  It never falls back to a CPU implementation: if the CUDA library is
+missing or no GPU is present, every sort raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libssort_b200.so")
+WLIB_PATH = os.path.join(_HERE, "libssort_workloads.so")
+
+SSORT_OK = 0
+SSORT_MAX_ROUNDS = 64
+
+# Every symbol include/ssort_b200.h declares.
+EXPORTS = (
+    "msd_gpu", "ssort_strerror", "ssort_last_error", "ssort_ctx_create", "ssort_ctx_destroy",
+    "ssort_sort_device", "ssort_sort_host", "ssort_sort_strings", "ssort_get_stats",
+    "ssort_set_profiling", "ssort_get_kernel_times",
+)
+
+
+class SsortError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"ssort status {status}: {msg}")
+        self.status = status
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint32),
+        ("partition_levels", ctypes.c_uint32),
+        ("live", ctypes.c_uint64 * SSORT_MAX_ROUNDS),
+        ("partitioned", ctypes.c_uint64),
+        ("small_segments", ctypes.c_uint64),
+        ("device_bytes", ctypes.c_uint64),
+        ("device_ms", ctypes.c_double),
+        ("gather_elems", ctypes.c_uint64),
+        ("tiny_fresh", ctypes.c_uint64),
+        ("tiny_keyed", ctypes.c_uint64),
+        ("small_fresh", ctypes.c_uint64),
+        ("small_keyed", ctypes.c_uint64),
+        ("equal_moved", ctypes.c_uint64),
+        ("equal_final", ctypes.c_uint64),
+        ("boundaries", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "live"}
+        d["live"] = [int(self.live[i]) for i in range(min(self.rounds, SSORT_MAX_ROUNDS))]
+        return d
+
+
+_lib = None
+_wlib = None
+
+
+def lib():
+    """Load libssort_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with string-sorting_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+        L.ssort_strerror.restype = ctypes.c_char_p
+        L.ssort_strerror.argtypes = [i32]
+        L.ssort_last_error.restype = ctypes.c_char_p
+        L.ssort_last_error.argtypes = []
+        L.ssort_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
+        L.ssort_ctx_destroy.argtypes = [vp]
+        L.ssort_ctx_destroy.restype = None
+        L.ssort_sort_device.argtypes = [vp, vp, u64, vp, i32, u64, vp, vp, vp]
+        L.ssort_sort_host.argtypes = [vp, vp, u64, vp, i32, u64, vp, vp]
+        L.ssort_sort_strings.argtypes = [vp, vp, ctypes.c_size_t, vp]
+        L.ssort_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.ssort_set_profiling.argtypes = [vp, i32]
+        L.ssort_get_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p),
+                                             ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_uint64), i32]
+        L.msd_gpu.argtypes = [vp, ctypes.c_size_t]
+        L.msd_gpu.restype = None
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != SSORT_OK:
+        L = lib()
+        raise SsortError(status, f"{L.ssort_strerror(status).decode()}: "
+                                 f"{L.ssort_last_error().decode()}")
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+class Sorter:
+    """One sort context (a CUDA stream plus a reusable device workspace)."""
+
+    def __init__(self, device=0):
+        self._ctx = ctypes.c_void_p()
+        _check(lib().ssort_ctx_create(int(device), ctypes.byref(self._ctx)))
+
+    def close(self):
+        if self._ctx:
+            lib().ssort_ctx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- entry points ---------------------------------------------------------
+    def sort_host(self, arena, offs, with_lcp=True, perm=None, lcp=None):
+        """Sort from host buffers (numpy): arena uint8, offs uint32/uint64."""
+        arena = np.ascontiguousarray(arena, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs)
+        if offs.dtype not in (np.uint32, np.uint64):
+            raise TypeError("offsets must be uint32 or uint64")
+        n = offs.shape[0]
+        if perm is None:
+            perm = np.empty(n, dtype=np.uint32)
+        if with_lcp and lcp is None:
+            lcp = np.empty(n, dtype=np.uint32)
+        _check(lib().ssort_sort_host(self._ctx, _ptr(arena), arena.nbytes, _ptr(offs),
+                                     offs.dtype.itemsize, n, _ptr(perm),
+                                     _ptr(lcp) if with_lcp else None))
+        return perm, (lcp if with_lcp else None)
+
+    def sort_device(self, d_arena, arena_bytes, d_offs, off_width, n, d_perm, d_lcp=None,
+                    stream=None):
+        """Sort device-resident buffers (torch CUDA tensors or raw pointers)."""
+        def p(x):
+            return x if isinstance(x, int) or x is None else x.data_ptr()
+        _check(lib().ssort_sort_device(self._ctx, p(d_arena), int(arena_bytes), p(d_offs),
+                                       int(off_width), int(n), p(d_perm), p(d_lcp),
+                                       stream))
+
+    def sort_strings(self, strings, with_lcp=False):
+        """Pointer-array form: strings is a list of bytes objects (no NULs).
+        Returns the sorted list (and the LCP array)."""
+        n = len(strings)
+        bufs = [ctypes.create_string_buffer(s) for s in strings]
+        arr = (ctypes.c_void_p * max(n, 1))(*[ctypes.addressof(b) for b in bufs])
+        lcp = np.empty(n, dtype=np.uint32) if with_lcp else None
+        _check(lib().ssort_sort_strings(self._ctx, arr, n, _ptr(lcp)))
+        addr = {ctypes.addressof(b): i for i, b in enumerate(bufs)}
+        order = [addr[arr[i]] for i in range(n)]
+        out = [strings[i] for i in order]
+        return (out, lcp) if with_lcp else out
+
+    def stats(self):
+        s = Stats()
+        _check(lib().ssort_get_stats(self._ctx, ctypes.byref(s)))
+        return s
+
+    def set_profiling(self, on):
+        _check(lib().ssort_set_profiling(self._ctx, 1 if on else 0))
+
+    def kernel_times(self):
+        L = lib()
+        k = L.ssort_get_kernel_times(self._ctx, None, None, None, 0)
+        names = (ctypes.c_char_p * max(k, 1))()
+        ms = (ctypes.c_double * max(k, 1))()
+        cnt = (ctypes.c_uint64 * max(k, 1))()
+        L.ssort_get_kernel_times(self._ctx, names, ms, cnt, k)
+        return {names[i].decode(): (ms[i], cnt[i]) for i in range(k)}
+
+
+# ---- synthetic workloads ------------------------------------------------------
+class StringSet:
+    """An arena of NUL-terminated strings plus uint64 offsets, owned by the
+    workload library (freed on garbage collection)."""
+
+    def __init__(self, arena_ptr, arena_bytes, offs_ptr, n):
+        self._arena_ptr = arena_ptr
+        self._offs_ptr = offs_ptr
+        self.n = int(n)
+        self.text_bytes = int(arena_bytes)  # without the 16 padding bytes
+        ab = arena_bytes + 16
+        self.arena = np.ctypeslib.as_array(
+            ctypes.cast(arena_ptr, ctypes.POINTER(ctypes.c_uint8)), shape=(ab,))
+        self.offs = np.ctypeslib.as_array(
+            ctypes.cast(offs_ptr, ctypes.POINTER(ctypes.c_uint64)), shape=(max(self.n, 1),))[:self.n]
+
+    def __del__(self):
+        try:
+            if self._arena_ptr:
+                wlib().ssw_free(self._arena_ptr)
+                wlib().ssw_free(self._offs_ptr)
+                self._arena_ptr = None
+        except Exception:
+            pass
+
+    def string(self, i):
+        o = int(self.offs[i])
+        e = o
+        while self.arena[e] != 0:
+            e += 1
+        return bytes(self.arena[o:e])
+
+    def key_bytes(self):
+        """Sum of (length + 1) over all strings: the bytes the sort keys on."""
+        return self.text_bytes
+
+
+def wlib():
+    global _wlib
+    if _wlib is None:
+        if not os.path.exists(WLIB_PATH):
+            raise FileNotFoundError(f"{WLIB_PATH} is missing: build string-sorting_b200/build.py")
+        W = ctypes.CDLL(WLIB_PATH)
+        pp8 = ctypes.POINTER(ctypes.c_void_p)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        W.ssw_gen_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                      ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                      pp8, u64p, pp8]
+        W.ssw_gen_urls.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double,
+                                   ctypes.c_uint64, pp8, u64p, pp8]
+        W.ssw_gen_zipf_words.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double,
+                                         ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64,
+                                         pp8, u64p, pp8]
+        W.ssw_free.argtypes = [ctypes.c_void_p]
+        W.ssw_free.restype = None
+        W.ssw_uniform_doubles.argtypes = [ctypes.c_uint64, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_double)]
+        W.ssw_uniform_doubles.restype = None
+        _wlib = W
+    return _wlib
+
+
+def _gen(fn, *args):
+    a = ctypes.c_void_p()
+    o = ctypes.c_void_p()
+    nb = ctypes.c_uint64()
+    rc = fn(*args, ctypes.byref(a), ctypes.byref(nb), ctypes.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"workload generator failed ({rc})")
+    return a.value, nb.value, o.value
+
+
+def gen_uniform(n, min_len=1, max_len=20, alpha_lo=ord("a"), alpha_size=26, seed=1):
+    a, nb, o = _gen(wlib().ssw_gen_uniform, n, min_len, max_len, alpha_lo, alpha_size, seed)
+    return StringSet(a, nb, o, n)
+
+
+def gen_urls(n, n_hosts=4096, zipf_s=1.1, seed=2):
+    a, nb, o = _gen(wlib().ssw_gen_urls, n, n_hosts, zipf_s, seed)
+    return StringSet(a, nb, o, n)
+
+
+def gen_zipf_words(n, vocab=1_000_000, p_geom=0.15, max_len=24, zipf_s=1.0, seed=3):
+    a, nb, o = _gen(wlib().ssw_gen_zipf_words, n, vocab, p_geom, max_len, zipf_s, seed)
+    return StringSet(a, nb, o, n)
+
+
+def uniform_doubles(n, seed):
+    out = np.empty(n, dtype=np.float64)
+    wlib().ssw_uniform_doubles(n, seed, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return out
+
+
+# The workloads the benchmark and the parity tests use, by name.
+WORKLOADS = {
+    # 1,000,000 strings, length U[1,20], bytes U{'a'..'z'}, seed 1
+    "uniform_1m": lambda scale=1.0: gen_uniform(int(1_000_000 * scale), 1, 20, ord("a"), 26, 1),
+    # 50,000,000 URLs: "http://" + Zipf(1.1) host of 4096 + 1..6 path segments
+    "urls_50m": lambda scale=1.0: gen_urls(int(50_000_000 * scale), 4096, 1.1, 2),
+    # 100,000,000 copies of Zipf(1.0) words from a 1,000,000-word vocabulary
+    "zipf_words_100m": lambda scale=1.0: gen_zipf_words(int(100_000_000 * scale), 1_000_000,
+                                                        0.15, 24, 1.0, 3),
+}

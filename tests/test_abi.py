@@ -1,0 +1,63 @@
+"""CPU tests of the C ABI: the library loads, exports every entry point the
+public header declares, and validates arguments without touching a GPU."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import pyssort
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "ssort_b200.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    names = re.findall(r"^[A-Za-z_][\w\s\*]*?\b(\w+)\s*\([^;{]*\)\s*;", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_parses():
+    fns = header_functions()
+    assert "msd_gpu" in fns and "ssort_sort_device" in fns
+    assert set(fns) == set(pyssort.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(pyssort.LIB_PATH)
+    for name in header_functions():
+        assert hasattr(lib, name), name
+
+
+def test_routine_signature_symbol():
+    """msd_gpu has the struct routine::f signature: void(unsigned char**, size_t)."""
+    lib = pyssort.lib()
+    fn = lib.msd_gpu
+    assert fn.restype is None
+    assert len(fn.argtypes) == 2
+
+
+def test_status_strings():
+    L = pyssort.lib()
+    assert L.ssort_strerror(0) == b"ok"
+    assert L.ssort_strerror(-1) == b"invalid argument"
+    assert L.ssort_strerror(-4) == b"no CUDA device"
+
+
+def test_no_device_is_reported_not_faked():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pyssort.SsortError) as e:
+        pyssort.Sorter(0)
+    assert e.value.status == -4
+
+
+def test_null_context_is_rejected():
+    L = pyssort.lib()
+    assert L.ssort_sort_host(None, None, 0, None, 8, 0, None, None) == -1
+    assert L.ssort_sort_device(None, None, 0, None, 8, 0, None, None, None) == -1
+    assert L.ssort_set_profiling(None, 1) == -1

@@ -1,0 +1,113 @@
+"""GPU parity: the CUDA sort (through the C ABI) against the reference's own
+outputs (golden fixtures from msd_CE6) and against the C oracle on seeded
+workloads; full-size workloads are checked through size-independent properties
+(permutation, byte order, stability, LCP) by the independent checker."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import cases
+import pyoracle
+import pyssort
+
+pytestmark = pytest.mark.gpu
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<u4").tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", list(cases.CASES))
+def test_golden_cases_host_api(name, golden, sorter):
+    strings = cases.CASES[name]()
+    arena, offs = cases.arena_of(strings)
+    perm, lcp = sorter.sort_host(arena, offs)
+    g = golden[name]
+    if "perm" in g:
+        assert perm.tolist() == g["perm"]
+        assert lcp.tolist() == g["lcp"]
+    assert digest(perm) == g["perm_sha256"]
+    assert digest(lcp) == g["lcp_sha256"]
+
+
+@pytest.mark.parametrize("name", ["ut_runs30_8001", "dup_heavy_100000", "shared8_65537",
+                                  "high_bytes_5000", "desc_numbers_200000"])
+def test_golden_cases_u32_offsets(name, golden, sorter):
+    strings = cases.CASES[name]()
+    arena, offs = cases.arena_of(strings)
+    perm, lcp = sorter.sort_host(arena, offs.astype(np.uint32))
+    assert digest(perm) == golden[name]["perm_sha256"]
+    assert digest(lcp) == golden[name]["lcp_sha256"]
+
+
+def test_unpadded_arena_tail(sorter):
+    """Strings ending at the very end of the arena (no padding bytes)."""
+    strings = cases.uniform(5000, 31, 0, 30)
+    arena, offs = cases.arena_of(strings)
+    arena = arena[: len(arena) - 16].copy()
+    perm, lcp = sorter.sort_host(arena, offs)
+    ref_perm, ref_lcp = pyoracle.oracle_sort(np.concatenate([arena, np.zeros(16, np.uint8)]), offs)
+    assert np.array_equal(perm, ref_perm) and np.array_equal(lcp, ref_lcp)
+
+
+def test_device_api_with_torch_stream(sorter):
+    torch = pytest.importorskip("torch")
+    strings = cases.dup_heavy(50000, 32)
+    arena, offs = cases.arena_of(strings)
+    d_arena = torch.from_numpy(arena).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    n = len(strings)
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_lcp = torch.empty(n, dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        sorter.sort_device(d_arena, arena.nbytes, d_offs, 8, n, d_perm, d_lcp,
+                           stream=s.cuda_stream)
+    torch.cuda.synchronize()
+    perm = d_perm.cpu().numpy().view(np.uint32)
+    lcp = d_lcp.cpu().numpy().view(np.uint32)
+    ref_perm, ref_lcp = pyoracle.oracle_sort(arena, offs)
+    assert np.array_equal(perm, ref_perm) and np.array_equal(lcp, ref_lcp)
+
+
+def test_pointer_array_form(sorter):
+    strings = cases.high_bytes(3000, 33) + cases.ut_bb_a_bbb(50)
+    out, lcp = sorter.sort_strings(strings, with_lcp=True)
+    order, ref_lcp = pyoracle.python_sort(strings)
+    assert out == [strings[i] for i in order]
+    assert lcp.tolist() == ref_lcp
+
+
+@pytest.mark.parametrize("wl,n", [("uniform_1m", 1_000_000), ("urls", 2_000_000),
+                                  ("zipf", 5_000_000), ("alpha4", 1_000_000),
+                                  ("alpha95_long", 500_000)])
+def test_workloads_against_oracle(wl, n, sorter):
+    ss = {
+        "uniform_1m": lambda: pyssort.gen_uniform(n, 1, 20, ord("a"), 26, 1),
+        "urls": lambda: pyssort.gen_urls(n, 4096, 1.1, 2),
+        "zipf": lambda: pyssort.gen_zipf_words(n, 1_000_000, 0.15, 24, 1.0, 3),
+        "alpha4": lambda: pyssort.gen_uniform(n, 1, 32, ord("A"), 4, 41),
+        "alpha95_long": lambda: pyssort.gen_uniform(n, 1, 128, ord(" "), 95, 42),
+    }[wl]()
+    perm, lcp = sorter.sort_host(ss.arena, ss.offs)
+    ref_perm, ref_lcp = pyoracle.oracle_sort(ss.arena, ss.offs)
+    assert np.array_equal(perm, ref_perm)
+    assert np.array_equal(lcp, ref_lcp)
+
+
+def test_repeatable(sorter):
+    ss = pyssort.gen_urls(500_000, seed=44)
+    p1, l1 = sorter.sort_host(ss.arena, ss.offs)
+    p2, l2 = sorter.sort_host(ss.arena, ss.offs)
+    assert np.array_equal(p1, p2) and np.array_equal(l1, l2)
+
+
+@pytest.mark.parametrize("wl", ["urls_50m", "zipf_words_100m"])
+def test_full_size_properties(wl, sorter):
+    """The full-size plain workloads: the checker verifies permutation, byte
+    order, stability and every LCP entry independently of the oracle sort."""
+    ss = pyssort.WORKLOADS[wl]()
+    perm, lcp = sorter.sort_host(ss.arena, ss.offs)
+    bad, first = pyoracle.oracle_check(ss.arena, ss.offs, perm, lcp)
+    assert bad == 0, f"{bad} violations, first at {first}"
