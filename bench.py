@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(pyssort.WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="fraction of the workload's string count (profiling runs only; "
+                         "the reported workload is the full one at 1.0)")
     return ap.parse_args()
 
 
@@ -137,40 +140,58 @@ class Clocks:
 
 
 # ---- algorithmic bytes -----------------------------------------------------------
+KB = 16  # key bytes per round
+
+
 def kernel_bytes(st, w):
     """Algorithmic bytes each kernel must move for one sort, from the per-kernel
-    string counts: gather reads idx (4) + offset (w) + 8 key bytes and writes the
-    key (8); count reads keys (8); scatter reads and writes key+idx (2x12);
-    on-chip sorts read idx (4) + offset (w) + 8 key bytes when they gather
-    themselves, or key+idx (12) otherwise, and write idx + lcp (8); equality
-    buckets copy idx (8) and/or write lcp (4)."""
-    fresh = st.tiny_fresh + st.small_fresh
-    keyed = st.tiny_keyed + st.small_keyed
+    string counts: gather reads idx (4) + offset (w) + the key bytes and writes
+    the key (16); count reads keys (16); scatter reads and writes key+idx
+    (2x20); on-chip sorts read idx (4) + offset (w) + key bytes when they
+    gather themselves, or key+idx (20) otherwise, and write idx + lcp (8);
+    equality buckets copy idx (8) and/or write lcp (4)."""
+    def sort_bytes(fresh, keyed):
+        return fresh * (4 + w + KB) + keyed * (KB + 4) + (fresh + keyed) * 8
     return {
-        "gather": st.gather_elems * (4 + w + 8 + 8),
-        "count": st.partitioned * 8,
-        "scatter": st.partitioned * 24,
-        "small": (st.small_fresh * (4 + w + 8) + st.small_keyed * 12
-                  + (st.small_fresh + st.small_keyed) * 8),
-        "tiny": (st.tiny_fresh * (4 + w + 8) + st.tiny_keyed * 12
-                 + (st.tiny_fresh + st.tiny_keyed) * 8),
+        "gather": st.gather_elems * (4 + w + KB + KB),
+        "count": st.partitioned * KB,
+        "scatter": st.partitioned * 2 * (KB + 4),
+        "warp1": sort_bytes(st.warp1_fresh, st.warp1_keyed),
+        "warp8": sort_bytes(st.warp8_fresh, st.warp8_keyed),
+        "block": sort_bytes(st.block_fresh, st.block_keyed),
         "equal": st.equal_moved * 8 + st.equal_final * 4,
-        "_sorts_total_elems": fresh + keyed,
     }
 
 
-def sort_algorithmic_bytes(st, w):
-    """Bytes each round must touch: per live string idx (4) + offset (w) + key
-    (8) + one read and one write of (key, idx) (2x12); plus perm + lcp writes."""
-    live = [int(st.live[i]) for i in range(min(st.rounds, pyssort.SSORT_MAX_ROUNDS))]
-    return sum(m * (4 + w + 8 + 24) for m in live) + st.n * 8
+def intrinsic_live(lcp, n):
+    """Strings live entering each 8-byte round of a plain MSD radix sort,
+    derived from the final LCP array (independent of this implementation's
+    round width): string i is live at depth 8r when it shares >= 8r bytes
+    with a neighbour, i.e. max(lcp[i], lcp[i+1]) >= 8r."""
+    import numpy as np
+    l = np.asarray(lcp, dtype=np.int64)
+    m = np.maximum(l, np.append(l[1:], 0))
+    top = int(m.max()) if n else 0
+    live = [n]
+    d = 8
+    while d <= top:
+        live.append(int(np.count_nonzero(m >= d)))
+        d += 8
+    return live
+
+
+def sort_algorithmic_bytes(live8, n, w):
+    """Bytes a plain 8-byte-per-round MSD radix sort must touch: per live
+    string per round idx (4) + offset (w) + 8 key bytes + one read and one
+    write of (key, idx) (2x12); plus the perm and lcp writes (8 per string)."""
+    return sum(m * (4 + w + 8 + 24) for m in live8) + n * 8
 
 
 # ---- our arm ---------------------------------------------------------------------
 def run_ours(args, rank, world, local_rank, dist):
     import torch
     torch.cuda.set_device(local_rank)
-    ss = pyssort.WORKLOADS[args.workload]()
+    ss = pyssort.WORKLOADS[args.workload](args.scale)
     n = ss.n
     w = ss.offs.dtype.itemsize
     arena_t = torch.from_numpy(ss.arena)
@@ -269,13 +290,15 @@ def run_ours(args, rank, world, local_rank, dist):
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
                     "traffic": None, "algorithmic_bytes_per_launch": int(per_launch_bytes),
                     "launch_ms": round(per_launch_s * 1e3, 4)}
-    sort_bytes = sort_algorithmic_bytes(st, w)
+    live8 = intrinsic_live(d_lcp.cpu().numpy().view(np.uint32), n)
+    sort_bytes = sort_algorithmic_bytes(live8, n, w)
     sort_s = ms / 1e3 / args.steps
     sort_roof = {"bound": "hbm", "algorithmic_bytes_per_sort": int(sort_bytes),
                  "achieved": round(sort_bytes / sort_s / 1e9, 1), "peak": peak,
                  "frac": round(sort_bytes / sort_s / 1e9 / peak, 4),
                  "frac_of_8tbs": round(sort_bytes / sort_s / 1e9 / 8000, 4),
-                 "formula": "sum_r m_r*(4+W+8+24) + n*8"}
+                 "live_per_8byte_round": live8,
+                 "formula": "sum_r m_r*(4+W+8+24) + n*8, m_r from the LCP array"}
     launches = sum(v["launches"] * (3 if k == "scan" else 1) for k, v in per_kernel.items())
 
     cpu = None
@@ -354,7 +377,7 @@ def cpu_baseline(workload, ss, reps=3):
 def run_reference(args, rank):
     if rank != 0:
         return None
-    ss = pyssort.WORKLOADS[args.workload]()
+    ss = pyssort.WORKLOADS[args.workload](args.scale)
     m = min(ss.n, CPU_SAMPLE.get(args.workload, 2_000_000))
     for _ in range(args.warmup):
         time_cpu_sort(ss, m)

@@ -64,7 +64,7 @@ int ssort_ctx_create(int device, ssort_ctx **out);
 void ssort_ctx_destroy(ssort_ctx *ctx);
 
 /*
- * Device-resident sort: d_arena holds the strings (8-byte aligned base
+ * Device-resident sort: d_arena holds the strings (16-byte aligned base
  * address, arena_bytes long), d_offs holds n offsets of width off_width
  * (4 or 8 bytes; string i starts at d_arena + d_offs[i] and is NUL-terminated
  * inside the arena).  Writes d_perm[n] and, if d_lcp is not NULL, d_lcp[n].
@@ -90,7 +90,7 @@ int ssort_sort_strings(ssort_ctx *ctx, unsigned char **strings, size_t n, uint32
 /* Per-call statistics of the last sort on this context. */
 typedef struct {
     uint64_t n;                              /* strings sorted */
-    uint32_t rounds;                         /* 8-byte refinement rounds run */
+    uint32_t rounds;                         /* 16-byte refinement rounds run */
     uint32_t partition_levels;               /* sample-partition passes run */
     uint64_t live[SSORT_MAX_ROUNDS];         /* strings live entering each round */
     uint64_t partitioned;                    /* elements moved by partition scatters */
@@ -98,11 +98,12 @@ typedef struct {
     uint64_t device_bytes;                   /* device workspace currently held */
     double device_ms;                        /* device time of the sort (events) */
     /* strings handled per kernel, summed over rounds: keys gathered for large
-     * segments; strings sorted by warps / CTAs with keys loaded in the kernel
-     * ("fresh") or taken from the key buffer ("keyed"); equality-bucket
+     * segments; strings sorted by the one-per-lane warp sort, the
+     * eight-per-lane warp sort and the CTA sort, with keys loaded in the
+     * kernel ("fresh") or taken from the key buffer ("keyed"); equality-bucket
      * strings moved between buffers / finalised; partition boundaries. */
     uint64_t gather_elems;
-    uint64_t tiny_fresh, tiny_keyed, small_fresh, small_keyed;
+    uint64_t warp1_fresh, warp1_keyed, warp8_fresh, warp8_keyed, block_fresh, block_keyed;
     uint64_t equal_moved, equal_final;
     uint64_t boundaries;
 } ssort_stats;

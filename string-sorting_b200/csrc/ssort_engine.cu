@@ -62,8 +62,9 @@ struct ssort_ctx {
     cudaStream_t st = nullptr;
 
     // workspace
-    DBuf idx1, key0, key1, lcp, R, N, T, S, E, B, L, L2, spl, nspl, ntiles, cm_size, tile_base,
-        cm_base, tmp, cm, partials, ctr;
+    DBuf idx1, key0, key1, lcp, R, N, W1, W8, S, E, B, L, L2, spl, nspl, ntiles, cm_size,
+        tile_base, cm_base, tmp, cm, partials, ctr;
+    size_t cm_cap = 0;
     DBuf arena, offs, perm;  // staging for the host-buffer entry points
     HBuf h_offs, h_arena, h_perm;
     Counters *h_ctr = nullptr;
@@ -159,7 +160,7 @@ struct ssort_ctx {
     int grid_for(int per_sm) const { return num_sms * per_sm; }
 
     int reserve(uint32_t n, bool need_lcp);
-    int scan(const uint32_t *in, uint32_t *out, uint32_t n);
+    int scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev);
     int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
             uint32_t n, uint32_t *d_perm, uint32_t *d_lcp);
 };
@@ -176,25 +177,30 @@ int ssort_ctx::reserve(uint32_t n, bool need_internal_lcp) {
     const size_t half = (size_t)n / 2 + 2;
     const size_t nlarge = (size_t)n / (SMALL_CAP + 1) + 2;
     SS_TRY(ensure(idx1, (size_t)n * 4));
-    SS_TRY(ensure(key0, (size_t)n * 8));
-    SS_TRY(ensure(key1, (size_t)n * 8));
+    SS_TRY(ensure(key0, (size_t)n * 16));
+    SS_TRY(ensure(key1, (size_t)n * 16));
     if (need_internal_lcp) SS_TRY(ensure(lcp, (size_t)n * 4));
     SS_TRY(ensure(R, half * sizeof(Seg)));
     SS_TRY(ensure(N, half * sizeof(Seg)));
-    SS_TRY(ensure(T, half * sizeof(Seg)));
-    SS_TRY(ensure(S, half * sizeof(Seg)));
-    SS_TRY(ensure(E, half * sizeof(Seg)));
+    SS_TRY(ensure(W1, half * sizeof(Seg)));
+    SS_TRY(ensure(W8, (n / (WARP1_CAP + 1) + 2) * sizeof(Seg)));
+    SS_TRY(ensure(S, (n / (WARP8_CAP + 1) + 2) * sizeof(Seg)));
+    // equality work items: buckets of >= 2 strings, one item per EQ_TILE
+    SS_TRY(ensure(E, (half + (size_t)n / EQ_TILE + 2) * sizeof(Seg)));
     SS_TRY(ensure(B, ((size_t)n + 2) * sizeof(uint2)));
     SS_TRY(ensure(L, nlarge * sizeof(Seg)));
     SS_TRY(ensure(L2, nlarge * sizeof(Seg)));
-    SS_TRY(ensure(spl, nlarge * SPL_STRIDE * sizeof(uint64_t)));
+    SS_TRY(ensure(spl, nlarge * SPL_STRIDE * sizeof(ulonglong2)));
     SS_TRY(ensure(nspl, nlarge * 4));
     SS_TRY(ensure(ntiles, nlarge * 4));
     SS_TRY(ensure(cm_size, nlarge * 4));
     SS_TRY(ensure(cm_base, (nlarge + 1) * 4));
-    SS_TRY(ensure(tile_base, (half + 1) * 4));
-    SS_TRY(ensure(tmp, (half + 1) * 4));
-    SS_TRY(ensure(partials, (size_t)scan_partials_needed((uint32_t)half) * 4));
+    SS_TRY(ensure(tile_base, (nlarge + 1) * 4));
+    SS_TRY(ensure(tmp, (nlarge + 1) * 4));
+    // bucket-count matrix: at most NB_MAX buckets per tile of each segment
+    cm_cap = (size_t)NB_MAX * ((size_t)n / PART_TILE + nlarge + 1) + 1;
+    SS_TRY(ensure(cm, cm_cap * 4));
+    SS_TRY(ensure(partials, (size_t)scan_partials_needed((uint32_t)std::min<size_t>(cm_cap, 0xFFFFFFFFull)) * 4));
     SS_TRY(ensure(ctr, sizeof(Counters)));
     if (!h_ctr) {
         SS_CUDA(cudaHostAlloc((void **)&h_ctr, sizeof(Counters), cudaHostAllocDefault));
@@ -202,16 +208,17 @@ int ssort_ctx::reserve(uint32_t n, bool need_internal_lcp) {
     return SSORT_OK;
 }
 
-int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n) {
-    SS_TRY(ensure(partials, (size_t)scan_partials_needed(n) * 4));
-    LAUNCH(this, "scan", launch_scan(in, out, n, (uint32_t *)partials.p, st));
+int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev) {
+    LAUNCH(this, "scan", launch_scan(in, out, n_host, n_dev, (uint32_t *)partials.p, st));
     return SSORT_OK;
 }
 
 // The round loop.  Every position's final index lands in d_perm (= idx[0]);
-// every lcp entry is written exactly once: inside a small/tiny sort or an
+// every lcp entry is written exactly once: inside an on-chip sort or an
 // equality bucket for pairs in the same leaf, by the boundary pass for pairs
-// split by a partition, and lcp[0] = 0 up front.
+// split by a partition, and lcp[0] = 0 up front.  The host waits for the
+// device twice per round (segment counts after classification, and the
+// next round's count) plus once per partition level.
 int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
                    int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp) {
     SS_TRY(reserve(n, d_lcp == nullptr));
@@ -223,8 +230,8 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
     a.n = n;
     a.idx[0] = d_perm;
     a.idx[1] = (uint32_t *)idx1.p;
-    a.key[0] = (uint64_t *)key0.p;
-    a.key[1] = (uint64_t *)key1.p;
+    a.key[0] = (ulonglong2 *)key0.p;
+    a.key[1] = (ulonglong2 *)key1.p;
     a.lcp = d_lcp ? d_lcp : (uint32_t *)lcp.p;
 
     Seg *cur = (Seg *)R.p, *nxt = (Seg *)N.p;
@@ -238,27 +245,25 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
     uint32_t n_cur = 1;
     uint64_t live = n;
     uint32_t round = 0;
+    const int g8 = grid_for(8), g4 = grid_for(4);
 
     while (n_cur) {
-        if (round < SSORT_MAX_ROUNDS) stats.live[round] = live;
         SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
         LAUNCH(this, "classify",
-               launch_classify(cur, n_cur, (Seg *)T.p, (Seg *)S.p, (Seg *)L.p, dc, st));
+               launch_classify(cur, n_cur, (Seg *)W1.p, (Seg *)W8.p, (Seg *)S.p, (Seg *)L.p, dc,
+                               st));
         SS_TRY(sync_counters());
+        live = h_ctr->live_next;  // strings in this round's segments
+        if (round < SSORT_MAX_ROUNDS) stats.live[round] = live;
         uint32_t n_large = h_ctr->n_large;
         Seg *lcur = (Seg *)L.p, *lnext = (Seg *)L2.p;
         if (n_large) {
             // Keys of the large segments at this depth.
             LAUNCH(this, "tile_counts",
                    launch_tile_counts(lcur, n_large, GATHER_TILE, (uint32_t *)tmp.p, st));
-            SS_TRY(scan((uint32_t *)tmp.p, (uint32_t *)tile_base.p, n_large));
-            uint32_t total_tiles = 0;
-            SS_CUDA(cudaMemcpyAsync(&total_tiles, (uint32_t *)tile_base.p + n_large, 4,
-                                    cudaMemcpyDeviceToHost, st));
-            SS_CUDA(cudaStreamSynchronize(st));
+            SS_TRY(scan((uint32_t *)tmp.p, (uint32_t *)tile_base.p, n_large, nullptr));
             LAUNCH(this, "gather",
-                   launch_gather(a, lcur, n_large, (const uint32_t *)tile_base.p, total_tiles,
-                                 std::min<uint32_t>(total_tiles, grid_for(8)), st));
+                   launch_gather(a, lcur, n_large, (const uint32_t *)tile_base.p, g8, st));
         }
         uint32_t levels_this_round = 0;
         while (n_large) {
@@ -269,68 +274,49 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
                 return fail(SSORT_EINTERNAL, "partition levels exceeded 4096");
             stats.partition_levels++;
             LAUNCH(this, "sample",
-                   launch_sample(a, lcur, n_large, (uint64_t *)spl.p, (uint32_t *)nspl.p,
+                   launch_sample(a, lcur, n_large, (ulonglong2 *)spl.p, (uint32_t *)nspl.p,
                                  (uint32_t *)ntiles.p, (uint32_t *)cm_size.p, st));
-            SS_TRY(scan((const uint32_t *)ntiles.p, (uint32_t *)tile_base.p, n_large));
-            SS_TRY(scan((const uint32_t *)cm_size.p, (uint32_t *)cm_base.p, n_large));
-            uint32_t totals[2] = {0, 0};
-            SS_CUDA(cudaMemcpyAsync(&totals[0], (uint32_t *)tile_base.p + n_large, 4,
-                                    cudaMemcpyDeviceToHost, st));
-            SS_CUDA(cudaMemcpyAsync(&totals[1], (uint32_t *)cm_base.p + n_large, 4,
-                                    cudaMemcpyDeviceToHost, st));
-            SS_CUDA(cudaStreamSynchronize(st));
-            const uint32_t total_tiles = totals[0], cm_total = totals[1];
-            SS_TRY(ensure(cm, ((size_t)cm_total + 1) * 4));
-            const int pg = std::min<uint32_t>(total_tiles, grid_for(4));
+            SS_TRY(scan((const uint32_t *)ntiles.p, (uint32_t *)tile_base.p, n_large, nullptr));
+            SS_TRY(scan((const uint32_t *)cm_size.p, (uint32_t *)cm_base.p, n_large, nullptr));
             LAUNCH(this, "count",
-                   launch_count(a, lcur, n_large, (const uint32_t *)tile_base.p, total_tiles,
-                                (const uint64_t *)spl.p, (const uint32_t *)nspl.p,
-                                (const uint32_t *)cm_base.p, (uint32_t *)cm.p, pg, st));
-            SS_TRY(scan((const uint32_t *)cm.p, (uint32_t *)cm.p, cm_total));
+                   launch_count(a, lcur, n_large, (const uint32_t *)tile_base.p,
+                                (const ulonglong2 *)spl.p, (const uint32_t *)nspl.p,
+                                (const uint32_t *)cm_base.p, (uint32_t *)cm.p, g4, st));
+            SS_TRY(scan((const uint32_t *)cm.p, (uint32_t *)cm.p, (uint32_t)(cm_cap - 1),
+                        (const uint32_t *)cm_base.p + n_large));
             LAUNCH(this, "scatter",
-                   launch_scatter(a, lcur, n_large, (const uint32_t *)tile_base.p, total_tiles,
-                                  (const uint64_t *)spl.p, (const uint32_t *)nspl.p,
-                                  (const uint32_t *)cm_base.p, (const uint32_t *)cm.p, pg, st));
+                   launch_scatter(a, lcur, n_large, (const uint32_t *)tile_base.p,
+                                  (const ulonglong2 *)spl.p, (const uint32_t *)nspl.p,
+                                  (const uint32_t *)cm_base.p, (const uint32_t *)cm.p, g4, st));
             LAUNCH(this, "emit",
                    launch_emit(a, lcur, n_large, (const uint32_t *)tile_base.p,
                                (const uint32_t *)nspl.p, (const uint32_t *)cm_base.p,
-                               (const uint32_t *)cm.p, (Seg *)T.p, (Seg *)S.p, lnext, (Seg *)E.p,
-                               (uint2 *)B.p, dc, st));
+                               (const uint32_t *)cm.p, (Seg *)W1.p, (Seg *)W8.p, (Seg *)S.p, lnext,
+                               (Seg *)E.p, (uint2 *)B.p, nxt, dc, st));
             SS_TRY(sync_counters());
             n_large = h_ctr->n_large_next;
             SS_CUDA(cudaMemsetAsync(&dc->n_large_next, 0, 4, st));
             std::swap(lcur, lnext);
         }
-        const uint32_t nT = h_ctr->n_tiny, nS = h_ctr->n_small, nE = h_ctr->n_equal,
-                       nB = h_ctr->n_bound;
-        stats.small_segments += nT + nS;
-        LAUNCH(this, "tiny", launch_tiny(a, (Seg *)T.p, nT, nxt, dc, grid_for(8), st));
-        LAUNCH(this, "small", launch_small(a, (Seg *)S.p, nS, nxt, dc, grid_for(8), st));
-        if (nE) {
-            LAUNCH(this, "tile_counts",
-                   launch_tile_counts((Seg *)E.p, nE, EQ_TILE, (uint32_t *)tmp.p, st));
-            SS_TRY(scan((uint32_t *)tmp.p, (uint32_t *)tile_base.p, nE));
-            uint32_t total_tiles = 0;
-            SS_CUDA(cudaMemcpyAsync(&total_tiles, (uint32_t *)tile_base.p + nE, 4,
-                                    cudaMemcpyDeviceToHost, st));
-            SS_CUDA(cudaStreamSynchronize(st));
-            LAUNCH(this, "equal",
-                   launch_equal(a, (Seg *)E.p, nE, (const uint32_t *)tile_base.p, total_tiles,
-                                nxt, dc, grid_for(8), st));
-        }
-        LAUNCH(this, "boundary", launch_boundary(a, (uint2 *)B.p, nB, st));
+        LAUNCH(this, "warp1", launch_warp1(a, (Seg *)W1.p, nxt, dc, g8, st));
+        LAUNCH(this, "warp8", launch_warp8(a, (Seg *)W8.p, nxt, dc, g8, st));
+        LAUNCH(this, "block", launch_block(a, (Seg *)S.p, nxt, dc, g8, st));
+        LAUNCH(this, "equal", launch_equal(a, (Seg *)E.p, nxt, dc, g8, st));
+        LAUNCH(this, "boundary", launch_boundary(a, (uint2 *)B.p, dc, g4, st));
         SS_TRY(sync_counters());
+        stats.small_segments += h_ctr->n_w1 + h_ctr->n_w8 + h_ctr->n_small;
         stats.partitioned += h_ctr->partitioned;
         stats.gather_elems += h_ctr->gather_elems;
-        stats.tiny_fresh += h_ctr->tiny_fresh;
-        stats.tiny_keyed += h_ctr->tiny_keyed;
-        stats.small_fresh += h_ctr->small_fresh;
-        stats.small_keyed += h_ctr->small_keyed;
+        stats.warp1_fresh += h_ctr->warp1_fresh;
+        stats.warp1_keyed += h_ctr->warp1_keyed;
+        stats.warp8_fresh += h_ctr->warp8_fresh;
+        stats.warp8_keyed += h_ctr->warp8_keyed;
+        stats.block_fresh += h_ctr->block_fresh;
+        stats.block_keyed += h_ctr->block_keyed;
         stats.equal_moved += h_ctr->equal_moved;
         stats.equal_final += h_ctr->equal_final;
-        stats.boundaries += nB;
+        stats.boundaries += h_ctr->n_bound;
         n_cur = h_ctr->n_next;
-        live = h_ctr->live_next;
         std::swap(cur, nxt);
         ++round;
     }
@@ -368,8 +354,8 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
     ctx->stats.device_ms = ms;
     if (ctx->prof) ctx->prof_collect();
     size_t held = 0;
-    for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->T,
-                    &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
+    for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->W1,
+                    &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
                     &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
                     &ctx->cm, &ctx->partials, &ctx->arena, &ctx->offs, &ctx->perm})
         held += b->cap;
@@ -462,8 +448,8 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
     if (!ctx) return;
     with_device(ctx, [&]() -> int {
         if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
-        for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->T,
-                        &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
+        for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->W1,
+                        &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
                         &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
                         &ctx->cm, &ctx->partials, &ctx->ctr, &ctx->arena, &ctx->offs,
                         &ctx->perm})
@@ -486,7 +472,8 @@ int ssort_sort_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byt
     SS_TRY(validate_common(ctx, off_width, n));
     if (n == 0) return SSORT_OK;
     if (!d_arena || !d_offs || !d_perm) return fail(SSORT_EINVAL, "null device buffer");
-    if (((uintptr_t)d_arena & 7) != 0) return fail(SSORT_EINVAL, "arena must be 8-byte aligned");
+    if (((uintptr_t)d_arena & 15) != 0)
+        return fail(SSORT_EINVAL, "arena must be 16-byte aligned");
     return with_device(ctx, [&]() -> int {
         ctx->st = stream ? (cudaStream_t)stream : ctx->own_stream;
         int rc = sort_device_impl(ctx, d_arena, arena_bytes, d_offs, off_width, n, d_perm, d_lcp);

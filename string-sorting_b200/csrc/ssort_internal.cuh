@@ -2,12 +2,15 @@
 // the device code (ssort_kernels.cu) and the host engine (ssort_engine.cu).
 //
 // Data layout in HBM for one sort of n strings:
-//   arena            the string bytes (read-only), NUL-terminated strings
+//   arena            the string bytes (read-only), NUL-terminated strings,
+//                    16-byte aligned base
 //   offs[n]          uint32 or uint64 offset of string i in the arena
 //   idx[0], idx[1]   uint32 string indices in sorted-position order (ping-pong);
 //                    idx[0] is the caller's perm buffer and holds the result
-//   key[0], key[1]   uint64 big-endian 8-byte key of each live position at the
-//                    depth of its segment (ping-pong with idx)
+//   key[0], key[1]   16-byte big-endian key (two uint64 words, most
+//                    significant first) of each live position at the depth of
+//                    its segment, every byte after the first NUL zeroed
+//                    (ping-pong with idx)
 //   lcp[n]           uint32 LCP array (the caller's buffer or an internal one)
 //   segment lists    Seg records; every live segment is a contiguous range of
 //                    positions whose strings agree on their first `depth` bytes
@@ -19,50 +22,59 @@
 
 namespace ssort {
 
+// Bytes of string consumed per refinement round.
+constexpr uint32_t KEY_BYTES = 16;
+
 // Seg.flags
 constexpr uint32_t SEG_BUF1 = 1u;   // idx/keys of this segment live in buffer 1
 constexpr uint32_t SEG_KEYS = 2u;   // key[buf] already holds this depth's keys
-constexpr uint32_t SEG_EQUAL = 4u;  // every key in the segment is equal
+constexpr uint32_t SEG_CHUNK_SHIFT = 8;  // equality work items: chunk index << 8
 
 struct Seg {
     uint32_t start, len, depth, flags;
 };
 
-// Segments of at most TINY_CAP strings are sorted by one warp in registers,
-// at most SMALL_CAP by one CTA in shared memory; larger ones are split by
-// sample partitioning first.
-constexpr int TINY_CAP = 32;
+// Segments of at most WARP1_CAP strings are sorted by one warp with one string
+// per lane, at most WARP8_CAP by one warp with 8 strings per lane, at most
+// SMALL_CAP by one CTA; larger ones are split by sample partitioning first.
+constexpr int WARP1_CAP = 32;
+constexpr int WARP8_CAP = 256;
 constexpr int SMALL_CAP = 2048;
 constexpr int SMALL_THREADS = 256;
+constexpr int SMALL_ITEMS = SMALL_CAP / SMALL_THREADS;  // 8
 
 // Sample partitioning of large segments.
 constexpr int KMAX = 511;               // splitters per segment and pass
 constexpr int SPL_STRIDE = 512;         // splitter slots per segment (pow2)
 constexpr int NB_MAX = 2 * KMAX + 1;    // range + equality buckets
-constexpr int SAMPLES = 4096;           // keys sampled per large segment
-constexpr int PART_THREADS = 256;
+constexpr int SAMPLES_MAX = 4096;       // keys sampled per large segment
+constexpr int TARGET_BUCKET = 512;      // wanted strings per range bucket
+constexpr int PART_THREADS = 512;
 constexpr int PART_WARPS = PART_THREADS / 32;
-constexpr int PART_ITEMS = 16;
+constexpr int PART_ITEMS = 8;
 constexpr int PART_TILE = PART_THREADS * PART_ITEMS;  // 4096 keys per tile
 
 constexpr int GATHER_TILE = 4096;
 constexpr int GATHER_THREADS = 256;
+constexpr int GATHER_ITEMS = 8;
 constexpr int EQ_TILE = 8192;
 
 struct Counters {
-    uint32_t n_tiny, n_small, n_large, n_equal;
-    uint32_t n_bound, n_next, n_large_next, error;
+    uint32_t n_w1, n_w8, n_small, n_large;
+    uint32_t n_equal, n_bound, n_next, n_large_next;
+    uint32_t gather_tiles, part_tiles, cm_total, error;
     unsigned long long live_next;    // strings in next-round segments
     unsigned long long partitioned;  // strings moved by partition scatters
     // element counts per kernel (for the algorithmic-bytes roofline)
     unsigned long long gather_elems;  // keys gathered by k_gather
-    unsigned long long tiny_fresh, tiny_keyed, small_fresh, small_keyed;
+    unsigned long long warp1_fresh, warp1_keyed, warp8_fresh, warp8_keyed, block_fresh,
+        block_keyed;
     unsigned long long equal_moved, equal_final;  // equality-bucket copies / lcp fills
 };
 
 struct SortArgs {
     __device__ __forceinline__ uint32_t *idxb(int b) const { return b ? idx[1] : idx[0]; }
-    __device__ __forceinline__ uint64_t *keyb(int b) const { return b ? key[1] : key[0]; }
+    __device__ __forceinline__ ulonglong2 *keyb(int b) const { return b ? key[1] : key[0]; }
 
     const uint8_t *arena;
     uint64_t arena_bytes;
@@ -70,40 +82,44 @@ struct SortArgs {
     int off_width;
     uint32_t n;
     uint32_t *idx[2];
-    uint64_t *key[2];
+    ulonglong2 *key[2];
     uint32_t *lcp;
 };
 
 // ---- launchers (ssort_kernels.cu) ----------------------------------------
 void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st);
-void launch_classify(const Seg *R, uint32_t nR, Seg *T, Seg *S, Seg *L, Counters *c,
+void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L, Counters *c,
                      cudaStream_t st);
 void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
                         cudaStream_t st);
-// exclusive scan of in[0..n) into out[0..n); out[n] = total (out has n+1 slots)
-void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *partials,
-                 cudaStream_t st);
+// exclusive scan of in[0..n) into out[0..n); out[n] = total (out has n+1 slots).
+// n is read from *n_dev when n_dev is not null (n_host is then an upper bound).
+void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
+                 uint32_t *partials, cudaStream_t st);
 uint32_t scan_partials_needed(uint32_t n);
 void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                   uint32_t total_tiles, int grid, cudaStream_t st);
-void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, uint64_t *spl,
+                   int grid, cudaStream_t st);
+void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl,
                    uint32_t *nspl, uint32_t *ntiles, uint32_t *cm_size, cudaStream_t st);
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                  uint32_t total_tiles, const uint64_t *spl, const uint32_t *nspl,
-                  const uint32_t *cm_base, uint32_t *cm, int grid, cudaStream_t st);
+                  const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
+                  uint32_t *cm, int grid, cudaStream_t st);
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                    uint32_t total_tiles, const uint64_t *spl, const uint32_t *nspl,
-                    const uint32_t *cm_base, const uint32_t *cm_scan, int grid,
-                    cudaStream_t st);
+                    const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
+                    const uint32_t *cm_scan, int grid, cudaStream_t st);
 void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                  const uint32_t *nspl, const uint32_t *cm_base, const uint32_t *cm_scan,
-                 Seg *T, Seg *S, Seg *L2, Seg *E, uint2 *B, Counters *c, cudaStream_t st);
-void launch_tiny(const SortArgs &a, const Seg *T, uint32_t nT, Seg *N, Counters *c, int grid,
+                 Seg *W1, Seg *W8, Seg *S, Seg *L2, Seg *E, uint2 *B, Seg *N, Counters *c,
                  cudaStream_t st);
-void launch_small(const SortArgs &a, const Seg *S, uint32_t nS, Seg *N, Counters *c, int grid,
+// On-chip segment sorts; list lengths are read from the counters on the device.
+void launch_warp1(const SortArgs &a, const Seg *W1, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
-void launch_equal(const SortArgs &a, const Seg *E, uint32_t nE, const uint32_t *tile_base,
-                  uint32_t total_tiles, Seg *N, Counters *c, int grid, cudaStream_t st);
-void launch_boundary(const SortArgs &a, const uint2 *B, uint32_t nB, cudaStream_t st);
+void launch_warp8(const SortArgs &a, const Seg *W8, Seg *N, Counters *c, int grid,
+                  cudaStream_t st);
+void launch_block(const SortArgs &a, const Seg *S, Seg *N, Counters *c, int grid,
+                  cudaStream_t st);
+void launch_equal(const SortArgs &a, const Seg *E, Seg *N, Counters *c, int grid,
+                  cudaStream_t st);
+void launch_boundary(const SortArgs &a, const uint2 *B, Counters *c, int grid, cudaStream_t st);
 
 }  // namespace ssort

@@ -1,89 +1,142 @@
 // ssort_kernels.cu -- sm_100a kernels of the MSD radix string sort.
 //
 // One refinement round works on the live segments at one depth (a multiple of
-// 8 bytes).  For every live string it gathers the 8 bytes at arena[off+depth]
-// as a big-endian key with every byte after the first NUL zeroed (the uint64
-// form of the reference's get_char, src/util/get_char.h:68-89, but built with
-// unsigned shifts; the reference's int-promoted shifts sign-extend bytes >= 0x80
-// and are not reproduced).  Each segment is then sorted by (key, index):
-// segments of <= 32 strings by one warp in registers, <= SMALL_CAP by one CTA
-// in shared memory, larger ones are first split by sample partitioning into
-// range buckets and equality buckets with a stable scatter.  Equal runs whose
-// key holds no NUL (the reference's is_end test, src/util/get_char.h:162-175,
-// and its bucket-skip rule, src/msd_ce.cpp:402) become the next round's
-// segments at depth+8; every other adjacent pair gets its LCP here.
+// 16 bytes).  For every live string it gathers the 16 bytes at arena[off+depth]
+// as a big-endian key with every byte after the first NUL zeroed (the
+// multi-byte form of the reference's get_char, src/util/get_char.h:42-89, built
+// with unsigned shifts; the reference's int-promoted 64-bit form sign-extends
+// bytes >= 0x80, :82, and is not reproduced).  Each segment is then sorted by
+// (key, index): segments of <= 32 strings by one warp in registers, <= 256 by
+// one warp with 8 strings per lane, <= SMALL_CAP by one CTA, larger ones are
+// first split by sample partitioning into range buckets and equality buckets
+// with a stable scatter.  Equal runs whose key holds no NUL (the reference's
+// is_end test, src/util/get_char.h:162-175, and its bucket-skip rule,
+// src/msd_ce.cpp:402) become the next round's segments at depth+16; every
+// other adjacent pair gets its LCP here.
 #include "ssort_internal.cuh"
 
 namespace ssort {
 
 namespace {
 
-constexpr uint64_t KEY_MAX = ~0ull;
+constexpr uint64_t W_MAX = ~0ull;
 constexpr uint32_t IDX_MAX = ~0u;
+
+// ---- 16-byte keys -----------------------------------------------------------
+struct Key {
+    uint64_t hi, lo;
+};
+
+__device__ __forceinline__ Key key_max() { return Key{W_MAX, W_MAX}; }
+__device__ __forceinline__ Key to_key(ulonglong2 v) { return Key{v.x, v.y}; }
+__device__ __forceinline__ ulonglong2 from_key(Key k) { return make_ulonglong2(k.hi, k.lo); }
+__device__ __forceinline__ bool key_lt(const Key &a, const Key &b) {
+    return a.hi < b.hi || (a.hi == b.hi && a.lo < b.lo);
+}
+__device__ __forceinline__ bool key_eq(const Key &a, const Key &b) {
+    return a.hi == b.hi && a.lo == b.lo;
+}
+__device__ __forceinline__ bool pair_lt(const Key &a, uint32_t ia, const Key &b, uint32_t ib) {
+    return a.hi < b.hi || (a.hi == b.hi && (a.lo < b.lo || (a.lo == b.lo && ia < ib)));
+}
 
 __device__ __forceinline__ uint64_t bswap64(uint64_t x) {
     const uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
     return ((uint64_t)__byte_perm(lo, 0, 0x0123) << 32) | __byte_perm(hi, 0, 0x0123);
 }
 
-// 8 bytes of the string at arena[pos..], big-endian, zero after the first NUL.
-__device__ __forceinline__ uint64_t load_key(const uint8_t *__restrict__ arena,
-                                             uint64_t arena_bytes, uint64_t pos) {
-    uint64_t w;
-    const uint64_t a = pos & ~7ull;
-    const uint32_t sh = (uint32_t)(pos & 7) * 8;
-    if (a + 16 <= arena_bytes) {
-        const uint64_t *p = reinterpret_cast<const uint64_t *>(arena + a);
-        const uint64_t lo = __ldg(p);
-        if (sh) {
-            const uint64_t hi = __ldg(p + 1);
-            w = (lo >> sh) | (hi << (64 - sh));
+// Classic zero-byte test on a little-endian word: the lowest flagged byte is
+// the first NUL (no false positives below it).  Returns the word with that
+// byte and everything after it cleared, and whether a NUL was found.
+__device__ __forceinline__ uint64_t cut_at_nul(uint64_t w, bool &found) {
+    const uint64_t z = (w - 0x0101010101010101ull) & ~w & 0x8080808080808080ull;
+    found = z != 0;
+    if (!found) return w;
+    const uint32_t jb = (uint32_t)(__ffsll((long long)z) - 1) >> 3;
+    return jb ? (w & ((1ull << (8 * jb)) - 1)) : 0ull;
+}
+
+// The 16 bytes of the string at arena[pos..], big-endian, zero after the
+// first NUL.  The arena base is 16-byte aligned; bytes at or beyond
+// arena_bytes read as NUL.
+__device__ __forceinline__ Key load_key(const uint8_t *__restrict__ arena, uint64_t arena_bytes,
+                                        uint64_t pos) {
+    uint64_t w0, w1;  // little-endian: byte 0 of w0 is arena[pos]
+    const uint64_t a = pos & ~15ull;
+    const uint32_t off = (uint32_t)(pos & 15);
+    if (a + 32 <= arena_bytes) {
+        const ulonglong2 v0 = __ldg(reinterpret_cast<const ulonglong2 *>(arena + a));
+        if (off == 0) {
+            w0 = v0.x;
+            w1 = v0.y;
         } else {
-            w = lo;
+            const ulonglong2 v1 = __ldg(reinterpret_cast<const ulonglong2 *>(arena + a + 16));
+            uint64_t q0, q1, q2;
+            if (off < 8) {
+                q0 = v0.x;
+                q1 = v0.y;
+                q2 = v1.x;
+            } else {
+                q0 = v0.y;
+                q1 = v1.x;
+                q2 = v1.y;
+            }
+            const uint32_t sh = (off & 7) * 8;
+            if (sh) {
+                w0 = (q0 >> sh) | (q1 << (64 - sh));
+                w1 = (q1 >> sh) | (q2 << (64 - sh));
+            } else {
+                w0 = q0;
+                w1 = q1;
+            }
         }
     } else {
-        // Within 16 bytes of the arena end: byte loads, never past the end
-        // (bytes past the end read as NUL).
-        w = 0;
-        for (int i = 0; i < 8; ++i) {
+        w0 = 0;
+        w1 = 0;
+        for (int i = 0; i < 16; ++i) {
             const uint64_t q = pos + i;
             if (q >= arena_bytes) break;
-            const uint8_t c = arena[q];
-            w |= (uint64_t)c << (8 * i);
+            const uint64_t c = arena[q];
+            if (i < 8)
+                w0 |= c << (8 * i);
+            else
+                w1 |= c << (8 * (i - 8));
             if (!c) break;
         }
     }
-    // Little-endian word: byte 0 is arena[pos].  The lowest flagged byte of
-    // the classic zero-byte test is the first NUL (no false positives below it).
-    const uint64_t z = (w - 0x0101010101010101ull) & ~w & 0x8080808080808080ull;
-    if (z) {
-        const uint32_t jb = (uint32_t)(__ffsll((long long)z) - 1) >> 3;
-        w &= jb ? ((1ull << (8 * jb)) - 1) : 0ull;
-    }
-    return bswap64(w);
+    bool nul;
+    w0 = cut_at_nul(w0, nul);
+    if (nul)
+        w1 = 0;
+    else
+        w1 = cut_at_nul(w1, nul);
+    return Key{bswap64(w0), bswap64(w1)};
 }
 
-// The key holds the end of its string (low byte NUL).
-__device__ __forceinline__ bool key_is_end(uint64_t k) { return (k & 0xFF) == 0; }
+// The key holds the end of its string (last byte NUL).
+__device__ __forceinline__ bool key_is_end(const Key &k) { return (k.lo & 0xFF) == 0; }
+
+__device__ __forceinline__ uint32_t len8(uint64_t w) {
+    return w ? 8u - ((uint32_t)(__ffsll((long long)w) - 1) >> 3) : 0u;
+}
 
 // Number of string bytes in a key that contains the NUL.
-__device__ __forceinline__ uint32_t key_len(uint64_t k) {
-    return k ? 8u - ((uint32_t)(__ffsll((long long)k) - 1) >> 3) : 0u;
+__device__ __forceinline__ uint32_t key_len(const Key &k) {
+    return (k.hi & 0xFF) ? 8u + len8(k.lo) : len8(k.hi);
 }
 
 // LCP contribution of two keys at the same depth (reference lcp(),
 // src/mergesort_lcp.cpp:88-100: stop at the first difference or the NUL).
-__device__ __forceinline__ uint32_t key_lcp(uint64_t a, uint64_t b) {
-    return a == b ? key_len(a) : ((uint32_t)__clzll((long long)(a ^ b)) >> 3);
+__device__ __forceinline__ uint32_t key_lcp(const Key &a, const Key &b) {
+    if (a.hi != b.hi) return (uint32_t)__clzll((long long)(a.hi ^ b.hi)) >> 3;
+    if ((a.hi & 0xFF) == 0) return len8(a.hi);
+    if (a.lo != b.lo) return 8u + ((uint32_t)__clzll((long long)(a.lo ^ b.lo)) >> 3);
+    return 8u + len8(a.lo);
 }
 
 __device__ __forceinline__ uint64_t string_offset(const void *offs, int off_width, uint32_t i) {
     return off_width == 8 ? __ldg(reinterpret_cast<const unsigned long long *>(offs) + i)
                           : (uint64_t)__ldg(reinterpret_cast<const uint32_t *>(offs) + i);
-}
-
-__device__ __forceinline__ bool pair_less(uint64_t ka, uint32_t ia, uint64_t kb, uint32_t ib) {
-    return ka < kb || (ka == kb && ia < ib);
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -109,22 +162,301 @@ __device__ __forceinline__ uint32_t find_seg(const uint32_t *base, uint32_t n, u
     return lo;
 }
 
+// Warp-aggregated append to a list counter: all 32 lanes call it together;
+// each lane with `want` gets its own slot, at the cost of one atomic per warp
+// (appends from millions of small segments would otherwise serialise on one
+// address).
+__device__ __forceinline__ uint32_t warp_append(uint32_t *ctr, bool want) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, want);
+    if (!mask) return 0;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(mask & lanemask_lt());
+}
+
+// Append a next-round segment; warp-collective like warp_append.
+__device__ __forceinline__ void emit_next_warp(Seg *N, Counters *c, bool want, uint32_t start,
+                                               uint32_t len, uint32_t depth) {
+    const uint32_t slot = warp_append(&c->n_next, want);
+    if (want) N[slot] = Seg{start, len, depth, 0u};
+}
+
+// Single-thread append (rare paths only).
 __device__ __forceinline__ void emit_next(Seg *N, Counters *c, uint32_t start, uint32_t len,
                                           uint32_t depth) {
     const uint32_t slot = atomicAdd(&c->n_next, 1u);
     N[slot] = Seg{start, len, depth, 0u};
-    atomicAdd(&c->live_next, (unsigned long long)len);
 }
 
-// Bucket of `key` among u sorted distinct splitters s[0..u) padded with
-// KEY_MAX to kp2-1 entries: range bucket 2j holds s[j-1] < key < s[j],
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    return v;
+}
+
+// Bucket of `key` among u sorted distinct splitters s[0..u) padded with the
+// all-ones key to kp2-1 entries: range bucket 2j holds s[j-1] < key < s[j],
 // equality bucket 2j+1 holds key == s[j].
-__device__ __forceinline__ uint32_t classify(const uint64_t *s, uint32_t kp2, uint32_t u,
-                                             uint64_t key) {
+__device__ __forceinline__ uint32_t classify(const ulonglong2 *s, uint32_t kp2, uint32_t u,
+                                             const Key &key) {
     uint32_t lo = 0;
     for (uint32_t step = kp2 >> 1; step > 0; step >>= 1)
-        if (s[lo + step - 1] < key) lo += step;
-    return (lo < u && s[lo] == key) ? 2 * lo + 1 : 2 * lo;
+        if (key_lt(to_key(s[lo + step - 1]), key)) lo += step;
+    return (lo < u && key_eq(to_key(s[lo]), key)) ? 2 * lo + 1 : 2 * lo;
+}
+
+// Padded shared-memory index: one spare slot per 8 keeps both the blocked
+// (stride 8) and the striped (stride 1) access patterns free of bank conflicts.
+__device__ __forceinline__ uint32_t pad(uint32_t e) { return e + (e >> 3); }
+
+// ---- bitonic sort of (key, index) pairs held in registers -------------------
+// Element e = tid * ITEMS + i of a group of THREADS threads (blocked layout).
+// Strides below ITEMS run inside a thread, below 32 * ITEMS across lanes with
+// shuffles, larger ones through shared memory (groups of several warps).
+template <int ITEMS, int J>
+__device__ __forceinline__ void stage_local(Key (&k)[ITEMS], uint32_t (&x)[ITEMS], uint32_t kk,
+                                            uint32_t tid) {
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        if ((i & J) == 0) {
+            const int l = i | J;
+            const bool asc = (((tid * ITEMS + i) & kk) == 0);
+            if (pair_lt(k[l], x[l], k[i], x[i]) == asc) {
+                const Key tk = k[i];
+                k[i] = k[l];
+                k[l] = tk;
+                const uint32_t tx = x[i];
+                x[i] = x[l];
+                x[l] = tx;
+            }
+        }
+    }
+}
+
+// Bitonic sort of 32 * ITEMS pairs held by one warp (ITEMS = 2, 4 or 8):
+// lane l holds elements l * ITEMS .. l * ITEMS + ITEMS - 1.
+template <int ITEMS>
+__device__ __forceinline__ void warp_bitonic(Key (&k)[ITEMS], uint32_t (&x)[ITEMS],
+                                             uint32_t lane) {
+    constexpr uint32_t P = 32 * ITEMS;
+#pragma unroll
+    for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+#pragma unroll
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            if (j >= (uint32_t)ITEMS) {
+                const uint32_t lm = j / ITEMS;
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    Key ko;
+                    ko.hi = __shfl_xor_sync(0xffffffffu, k[i].hi, lm);
+                    ko.lo = __shfl_xor_sync(0xffffffffu, k[i].lo, lm);
+                    const uint32_t xo = __shfl_xor_sync(0xffffffffu, x[i], lm);
+                    const uint32_t e = lane * ITEMS + i;
+                    const bool keep_min = ((lane & lm) == 0) == ((e & kk) == 0);
+                    const bool take = keep_min ? pair_lt(ko, xo, k[i], x[i])
+                                               : pair_lt(k[i], x[i], ko, xo);
+                    if (take) {
+                        k[i] = ko;
+                        x[i] = xo;
+                    }
+                }
+            } else {
+                if constexpr (ITEMS > 4) {
+                    if (j == 4) {
+                        stage_local<ITEMS, 4>(k, x, kk, lane);
+                        continue;
+                    }
+                }
+                if constexpr (ITEMS > 2) {
+                    if (j == 2) {
+                        stage_local<ITEMS, 2>(k, x, kk, lane);
+                        continue;
+                    }
+                }
+                if constexpr (ITEMS > 1) stage_local<ITEMS, 1>(k, x, kk, lane);
+            }
+        }
+    }
+}
+
+// One warp sorts the 32 * ITEMS pairs at padded shared-memory positions
+// base .. base + 32 * ITEMS - 1 in place.
+template <int ITEMS>
+__device__ __noinline__ void warp_sort_run(ulonglong2 *sk, uint32_t *sx, uint32_t base,
+                                              uint32_t lane) {
+    Key k[ITEMS];
+    uint32_t x[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t e = base + lane * ITEMS + i;
+        k[i] = to_key(sk[pad(e)]);
+        x[i] = sx[pad(e)];
+    }
+    warp_bitonic<ITEMS>(k, x, lane);
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t e = base + lane * ITEMS + i;
+        sk[pad(e)] = from_key(k[i]);
+        sx[pad(e)] = x[i];
+    }
+}
+
+// ---- packed 64-bit sort keys -------------------------------------------------
+// Within one segment every key shares its first f bits (f = leading zeros of
+// the OR of key ^ key0 over the segment).  The 53 bits after them, with the
+// string's local position (< 2048) in the low 11 bits, form a unique 64-bit
+// sort key whose order agrees with (key, index) order except between keys
+// whose windows are equal; those pairs are checked afterwards (check_sorted)
+// and a segment with any disagreement is re-sorted with the full comparator.
+constexpr uint32_t POS_BITS = 11;
+constexpr uint64_t POS_MASK = (1ull << POS_BITS) - 1;
+
+__device__ __forceinline__ uint32_t clz128(uint64_t hi, uint64_t lo) {
+    return hi ? (uint32_t)__clzll((long long)hi)
+              : 64u + (lo ? (uint32_t)__clzll((long long)lo) : 64u);
+}
+
+// Top 64 bits of the 128-bit key shifted left by f (0 <= f < 128).
+__device__ __forceinline__ uint64_t window64(const Key &k, uint32_t f) {
+    if (f == 0) return k.hi;
+    if (f < 64) return (k.hi << f) | (k.lo >> (64 - f));
+    return k.lo << (f - 64);
+}
+
+__device__ __forceinline__ uint64_t sort_key(const Key &k, uint32_t f, uint32_t pos) {
+    return (window64(k, f) & ~POS_MASK) | pos;
+}
+
+template <int ITEMS, int J>
+__device__ __forceinline__ void stage_local64(uint64_t (&v)[ITEMS], uint32_t kk, uint32_t lane) {
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        if ((i & J) == 0) {
+            const int l = i | J;
+            const bool asc = (((lane * ITEMS + i) & kk) == 0);
+            const uint64_t a = v[i], b = v[l];
+            const bool sw = (b < a) == asc;
+            v[i] = sw ? b : a;
+            v[l] = sw ? a : b;
+        }
+    }
+}
+
+// Bitonic sort of 32 * ITEMS distinct uint64 values held by one warp (lane l
+// holds elements l * ITEMS ..), ITEMS = 1, 2, 4 or 8.
+template <int ITEMS>
+__device__ __forceinline__ void warp_bitonic64(uint64_t (&v)[ITEMS], uint32_t lane) {
+    constexpr uint32_t P = 32 * ITEMS;
+#pragma unroll
+    for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+#pragma unroll
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            if (j >= (uint32_t)ITEMS) {
+                const uint32_t lm = j / ITEMS;
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    const uint64_t o = __shfl_xor_sync(0xffffffffu, v[i], lm);
+                    const uint32_t e = lane * ITEMS + i;
+                    const bool keep_min = ((lane & lm) == 0) == ((e & kk) == 0);
+                    v[i] = keep_min ? (o < v[i] ? o : v[i]) : (o > v[i] ? o : v[i]);
+                }
+            } else {
+                if constexpr (ITEMS > 4) {
+                    if (j == 4) {
+                        stage_local64<ITEMS, 4>(v, kk, lane);
+                        continue;
+                    }
+                }
+                if constexpr (ITEMS > 2) {
+                    if (j == 2) {
+                        stage_local64<ITEMS, 2>(v, kk, lane);
+                        continue;
+                    }
+                }
+                if constexpr (ITEMS > 1) stage_local64<ITEMS, 1>(v, kk, lane);
+            }
+        }
+    }
+}
+
+// Merge-path split over two sorted uint64 runs (values distinct).
+__device__ __forceinline__ uint32_t merge_split64(const uint64_t *s, uint32_t a0, uint32_t la,
+                                                  uint32_t b0, uint32_t lb, uint32_t d) {
+    uint32_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s[pad(a0 + mid)] < s[pad(b0 + d - 1 - mid)])
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Merge-path split: number of elements of run A (length la, at a0) among the
+// first d outputs of merging A with run B (length lb, at b0); ties go to A.
+__device__ __forceinline__ uint32_t merge_split(const ulonglong2 *sk, const uint32_t *sx,
+                                                uint32_t a0, uint32_t la, uint32_t b0,
+                                                uint32_t lb, uint32_t d) {
+    uint32_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t pa = pad(a0 + mid), pb = pad(b0 + d - 1 - mid);
+        // A[mid] <= B[d-1-mid]: A[mid] is among the first d outputs.
+        if (!pair_lt(to_key(sk[pb]), sx[pb], to_key(sk[pa]), sx[pa]))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// After a segment of `len` strings is sorted into shared memory (padded
+// layout), write its indices, LCPs and first/last keys, and emit the runs of
+// equal non-final keys as next-round segments.  Called by `threads` threads
+// numbered t = 0..threads-1.
+__device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
+                                               const ulonglong2 *sk, const uint32_t *sx,
+                                               uint32_t t, uint32_t threads, Seg *N,
+                                               Counters *c) {
+    // Uniform trip count so that every warp reaches the collective append.
+    for (uint32_t e0 = 0; e0 < s.len; e0 += threads) {
+        const uint32_t e = e0 + t;
+        bool want = false;
+        uint32_t run_lo = 0;
+        if (e < s.len) {
+            const uint32_t p = s.start + e;
+            const Key k = to_key(sk[pad(e)]);
+            a.idx[0][p] = sx[pad(e)];
+            if (e == 0 || e == s.len - 1) a.key[0][p] = from_key(k);
+            bool same_prev = false;
+            if (e > 0) {
+                const Key kp = to_key(sk[pad(e - 1)]);
+                same_prev = key_eq(kp, k);
+                if (!same_prev)
+                    a.lcp[p] = s.depth + key_lcp(kp, k);
+                else if (key_is_end(k))
+                    a.lcp[p] = s.depth + key_len(k);
+            }
+            if (same_prev && !key_is_end(k) &&
+                (e == s.len - 1 || !key_eq(to_key(sk[pad(e + 1)]), k))) {
+                uint32_t lo = 0, hi = e;  // first position of this run
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (key_lt(to_key(sk[pad(mid)]), k))
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                want = true;
+                run_lo = lo;
+            }
+        }
+        emit_next_warp(N, c, want, s.start + run_lo, e - run_lo + 1, s.depth + KEY_BYTES);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -133,18 +465,28 @@ __global__ void k_iota(uint32_t *idx, uint32_t n) {
         idx[i] = i;
 }
 
-__global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *T, Seg *S, Seg *L,
-                           Counters *c) {
+__global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *W1, Seg *W8, Seg *S,
+                           Seg *L, Counters *c) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nR) return;
-    const Seg s = R[i];
-    if (s.len <= (uint32_t)TINY_CAP)
-        T[atomicAdd(&c->n_tiny, 1u)] = s;
-    else if (s.len <= (uint32_t)SMALL_CAP)
-        S[atomicAdd(&c->n_small, 1u)] = s;
-    else {
-        L[atomicAdd(&c->n_large, 1u)] = s;
-        atomicAdd(&c->gather_elems, (unsigned long long)s.len);
+    const bool v = i < nR;
+    const Seg s = v ? R[i] : Seg{0, 0, 0, 0};
+    const bool w1 = v && s.len <= (uint32_t)WARP1_CAP;
+    const bool w8 = v && !w1 && s.len <= (uint32_t)WARP8_CAP;
+    const bool sm = v && !w1 && !w8 && s.len <= (uint32_t)SMALL_CAP;
+    const bool lg = v && !w1 && !w8 && !sm;
+    uint32_t slot = warp_append(&c->n_w1, w1);
+    if (w1) W1[slot] = s;
+    slot = warp_append(&c->n_w8, w8);
+    if (w8) W8[slot] = s;
+    slot = warp_append(&c->n_small, sm);
+    if (sm) S[slot] = s;
+    slot = warp_append(&c->n_large, lg);
+    if (lg) L[slot] = s;
+    const unsigned long long live = warp_sum(v ? s.len : 0);
+    const unsigned long long big = warp_sum(lg ? s.len : 0);
+    if ((threadIdx.x & 31) == 0) {
+        if (live) atomicAdd(&c->live_next, live);
+        if (big) atomicAdd(&c->gather_elems, big);
     }
 }
 
@@ -182,13 +524,22 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &e
     return total;
 }
 
+__device__ __forceinline__ uint32_t scan_n(uint32_t n_host, const uint32_t *n_dev) {
+    return n_dev ? *n_dev : n_host;
+}
+
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t *__restrict__ in,
-                                                              uint32_t n, uint32_t *partials) {
+                                                              uint32_t n_host,
+                                                              const uint32_t *n_dev,
+                                                              uint32_t *partials) {
+    const uint32_t n = scan_n(n_host, n_dev);
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_CHUNK;
     uint32_t s = 0;
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        const uint64_t i = base + (uint64_t)k * SCAN_THREADS + threadIdx.x;
-        if (i < n) s += in[i];
+    if (base < n) {
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            const uint64_t i = base + (uint64_t)k * SCAN_THREADS + threadIdx.x;
+            if (i < n) s += in[i];
+        }
     }
     uint32_t excl;
     const uint32_t tot = block_exclusive_scan(s, excl);
@@ -210,11 +561,14 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_partials(uint32_t *partia
 }
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t *in, uint32_t *out,
-                                                            uint32_t n,
+                                                            uint32_t n_host, const uint32_t *n_dev,
                                                             const uint32_t *__restrict__ partials,
                                                             uint32_t nparts) {
     __shared__ uint32_t buf[SCAN_CHUNK];
+    const uint32_t n = scan_n(n_host, n_dev);
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_CHUNK;
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = partials[nparts];
+    if (base >= n) return;
     for (int k = 0; k < SCAN_ITEMS; ++k) {
         const int j = k * SCAN_THREADS + threadIdx.x;
         const uint64_t i = base + j;
@@ -238,19 +592,22 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t *in, 
         const uint64_t i = base + j;
         if (i < n) out[i] = buf[j];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = partials[nparts];
 }
 
 // ---- key gather for large segments ----------------------------------------
 __global__ void __launch_bounds__(GATHER_THREADS) k_gather(SortArgs a, const Seg *__restrict__ L,
                                                           uint32_t nL,
-                                                          const uint32_t *__restrict__ tile_base,
-                                                          uint32_t total_tiles) {
-    constexpr int U = GATHER_TILE / GATHER_THREADS;
-    for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+                                                          const uint32_t *__restrict__ tile_base) {
+    constexpr int U = GATHER_ITEMS;
+    static_assert(GATHER_TILE % (GATHER_THREADS * GATHER_ITEMS) == 0, "tile shape");
+    const uint32_t total_tiles = tile_base[nL] * (GATHER_TILE / (GATHER_THREADS * U));
+    constexpr uint32_t SUBT = GATHER_TILE / (GATHER_THREADS * U);
+    for (uint32_t t2 = blockIdx.x; t2 < total_tiles; t2 += gridDim.x) {
+        const uint32_t t = t2 / SUBT;
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
-        const uint32_t lo = (t - tile_base[si]) * GATHER_TILE;
+        const uint32_t lo = (t - tile_base[si]) * GATHER_TILE + (t2 % SUBT) * GATHER_THREADS * U;
+        if (lo >= s.len) continue;
         const uint32_t *I = a.idx[0];
         uint32_t id[U];
         uint64_t off[U];
@@ -266,7 +623,8 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(SortArgs a, const Seg
         for (int u = 0; u < U; ++u) {
             const uint32_t i = lo + u * GATHER_THREADS + threadIdx.x;
             if (id[u] != IDX_MAX)
-                a.key[0][s.start + i] = load_key(a.arena, a.arena_bytes, off[u] + s.depth);
+                a.key[0][s.start + i] =
+                    from_key(load_key(a.arena, a.arena_bytes, off[u] + s.depth));
         }
     }
 }
@@ -284,64 +642,67 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
 }
 
 __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg *__restrict__ L,
-                                                           uint64_t *spl, uint32_t *nspl,
+                                                           ulonglong2 *spl, uint32_t *nspl,
                                                            uint32_t *ntiles, uint32_t *cm_size) {
-    __shared__ uint64_t smp[SAMPLES];
-    __shared__ uint32_t keep[SAMPLE_THREADS + 1];
+    extern __shared__ ulonglong2 smp[];  // SAMPLES_MAX keys
+    __shared__ uint32_t warp_cnt[SAMPLE_THREADS / 32 + 1];
     const Seg s = L[blockIdx.x];
-    const uint64_t *K = a.keyb(s.flags & SEG_BUF1);
-    for (int i = threadIdx.x; i < SAMPLES; i += SAMPLE_THREADS) {
-        const uint32_t r = hash32(s.start * 0x9E3779B1u + (uint32_t)i * 0x85EBCA77u + s.len);
-        const uint32_t p = (uint32_t)(((uint64_t)r * s.len) >> 32);
-        smp[i] = K[s.start + p];
+    const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
+    uint32_t k = (s.len + TARGET_BUCKET - 1) / TARGET_BUCKET;
+    if (k > (uint32_t)KMAX) k = KMAX;
+    if (k < 1) k = 1;
+    uint32_t S = next_pow2(8 * (k + 1));
+    if (S < 128) S = 128;
+    if (S > (uint32_t)SAMPLES_MAX) S = SAMPLES_MAX;
+    for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
+        const uint32_t r = hash32(s.start * 0x9E3779B1u + i * 0x85EBCA77u + s.len);
+        smp[i] = K[(uint32_t)(((uint64_t)r * s.len) >> 32)];
     }
     __syncthreads();
-    for (int k = 2; k <= SAMPLES; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < SAMPLES; i += SAMPLE_THREADS) {
-                const int l = i ^ j;
+    for (uint32_t kk = 2; kk <= S; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
+                const uint32_t l = i ^ j;
                 if (l > i) {
-                    const uint64_t x = smp[i], y = smp[l];
-                    const bool asc = (i & k) == 0;
-                    if ((x > y) == asc) {
-                        smp[i] = y;
-                        smp[l] = x;
+                    const Key x = to_key(smp[i]), y = to_key(smp[l]);
+                    if (key_lt(y, x) == ((i & kk) == 0)) {
+                        smp[i] = from_key(y);
+                        smp[l] = from_key(x);
                     }
                 }
             }
             __syncthreads();
         }
     }
-    // k candidate splitters at evenly spaced sample ranks, deduplicated.
-    uint32_t k = (s.len + SMALL_CAP / 4 - 1) / (SMALL_CAP / 4);
-    if (k > (uint32_t)KMAX) k = KMAX;
-    if (k < 1) k = 1;
-    uint64_t *out = spl + (uint64_t)blockIdx.x * SPL_STRIDE;
-    // Thread j < k owns candidate j; it survives if it differs from j-1.
-    // Compact survivors with a block scan over SAMPLE_THREADS >= KMAX slots.
+    // Candidate j < k sits at sample rank (j+1)*S/(k+1); it survives if it
+    // differs from candidate j-1.  Survivors are compacted in order.
     const uint32_t j = threadIdx.x;
-    uint64_t cand = 0;
-    uint32_t flag = 0;
+    Key cand{0, 0};
+    bool keep = false;
     if (j < k) {
-        cand = smp[((uint64_t)(j + 1) * SAMPLES) / (k + 1)];
-        flag = (j == 0) || smp[((uint64_t)j * SAMPLES) / (k + 1)] != cand;
+        cand = to_key(smp[((j + 1) * S) / (k + 1)]);
+        keep = j == 0 || !key_eq(to_key(smp[(j * S) / (k + 1)]), cand);
     }
-    keep[j] = flag;
+    const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) warp_cnt[w] = __popc(bal);
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t run = 0;
-        for (uint32_t q = 0; q < (uint32_t)SAMPLE_THREADS; ++q) {
-            const uint32_t f = keep[q];
-            keep[q] = run;
-            run += f;
+        for (int q = 0; q < SAMPLE_THREADS / 32; ++q) {
+            const uint32_t v = warp_cnt[q];
+            warp_cnt[q] = run;
+            run += v;
         }
-        keep[SAMPLE_THREADS] = run;
+        warp_cnt[SAMPLE_THREADS / 32] = run;
     }
     __syncthreads();
-    const uint32_t u = keep[SAMPLE_THREADS];
-    if (flag) out[keep[j]] = cand;
+    const uint32_t u = warp_cnt[SAMPLE_THREADS / 32];
+    ulonglong2 *out = spl + (uint64_t)blockIdx.x * SPL_STRIDE;
+    if (keep) out[warp_cnt[w] + __popc(bal & lanemask_lt())] = from_key(cand);
     const uint32_t kp2 = next_pow2(u + 1);
-    for (uint32_t q = u + threadIdx.x; q < kp2 - 1; q += SAMPLE_THREADS) out[q] = KEY_MAX;
+    for (uint32_t q = u + threadIdx.x; q + 1 < kp2; q += SAMPLE_THREADS)
+        out[q] = from_key(key_max());
     if (threadIdx.x == 0) {
         nspl[blockIdx.x] = u;
         const uint32_t nt = (s.len + PART_TILE - 1) / PART_TILE;
@@ -351,115 +712,141 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
 }
 
 // ---- partition count: per-tile bucket histograms ---------------------------
-__global__ void __launch_bounds__(PART_THREADS) k_count(SortArgs a, const Seg *__restrict__ L,
+// Each warp counts its own 512 consecutive keys into a private row, one
+// shared-memory update per distinct bucket per 32 keys (__match_any_sync).
+__global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg *__restrict__ L,
                                                         uint32_t nL,
                                                         const uint32_t *__restrict__ tile_base,
-                                                        uint32_t total_tiles,
-                                                        const uint64_t *__restrict__ spl,
+                                                        const ulonglong2 *__restrict__ spl,
                                                         const uint32_t *__restrict__ nspl,
                                                         const uint32_t *__restrict__ cm_base,
                                                         uint32_t *cm) {
-    __shared__ uint64_t sspl[SPL_STRIDE];
-    __shared__ uint32_t hist[NB_MAX + 1];
+    __shared__ ulonglong2 sspl[SPL_STRIDE];
+    __shared__ __align__(16) uint16_t hist[PART_WARPS][NB_MAX + 1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr int SUB = PART_TILE / PART_WARPS;
+    const uint32_t total_tiles = tile_base[nL];
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
         const uint32_t u = nspl[si], kp2 = next_pow2(u + 1), nb = 2 * u + 1;
         for (uint32_t q = threadIdx.x; q + 1 < kp2; q += PART_THREADS)
             sspl[q] = spl[(uint64_t)si * SPL_STRIDE + q];
-        for (uint32_t q = threadIdx.x; q < nb; q += PART_THREADS) hist[q] = 0;
+        {
+            uint32_t *h32 = reinterpret_cast<uint32_t *>(&hist[0][0]);
+            for (uint32_t q = threadIdx.x; q < PART_WARPS * (NB_MAX + 1) / 2; q += PART_THREADS)
+                h32[q] = 0;
+        }
         __syncthreads();
         const uint32_t tl = t - tile_base[si];
         const uint32_t nt = tile_base[si + 1] - tile_base[si];
-        const uint32_t lo = tl * PART_TILE;
-        const uint64_t *K = a.keyb(s.flags & SEG_BUF1) + s.start;
-#pragma unroll 4
-        for (int it = 0; it < PART_ITEMS; ++it) {
-            const uint32_t i = lo + it * PART_THREADS + threadIdx.x;
-            if (i < s.len) atomicAdd(&hist[classify(sspl, kp2, u, K[i])], 1u);
+        const uint32_t lo = tl * PART_TILE + w * SUB;
+        const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
+        Key kk[PART_ITEMS];
+#pragma unroll
+        for (int c = 0; c < PART_ITEMS; ++c) {
+            const uint32_t e = lo + c * 32 + lane;
+            kk[c] = e < s.len ? to_key(K[e]) : key_max();
+        }
+#pragma unroll
+        for (int c = 0; c < PART_ITEMS; ++c) {
+            const uint32_t e = lo + c * 32 + lane;
+            const uint32_t b = e < s.len ? classify(sspl, kp2, u, kk[c]) : nb;
+            const uint32_t peers = __match_any_sync(0xffffffffu, b);
+            if ((peers & lanemask_lt()) == 0) hist[w][b] += (uint16_t)__popc(peers);
+            __syncwarp();
         }
         __syncthreads();
-        for (uint32_t q = threadIdx.x; q < nb; q += PART_THREADS)
-            cm[cm_base[si] + (uint64_t)q * nt + tl] = hist[q];
+        for (uint32_t q = threadIdx.x; q < nb; q += PART_THREADS) {
+            uint32_t sum = 0;
+#pragma unroll
+            for (int ww = 0; ww < PART_WARPS; ++ww) sum += hist[ww][q];
+            cm[cm_base[si] + (uint64_t)q * nt + tl] = sum;
+        }
         __syncthreads();
     }
 }
 
 // ---- partition scatter: stable within and across tiles ---------------------
-__global__ void __launch_bounds__(PART_THREADS) k_scatter(SortArgs a, const Seg *__restrict__ L,
+__global__ void __launch_bounds__(PART_THREADS, 2) k_scatter(SortArgs a, const Seg *__restrict__ L,
                                                           uint32_t nL,
                                                           const uint32_t *__restrict__ tile_base,
-                                                          uint32_t total_tiles,
-                                                          const uint64_t *__restrict__ spl,
+                                                          const ulonglong2 *__restrict__ spl,
                                                           const uint32_t *__restrict__ nspl,
                                                           const uint32_t *__restrict__ cm_base,
                                                           const uint32_t *__restrict__ cm_scan) {
-    __shared__ uint64_t sspl[SPL_STRIDE];
-    __shared__ uint32_t wcnt[PART_WARPS][NB_MAX + 1];
+    __shared__ ulonglong2 sspl[SPL_STRIDE];
+    __shared__ __align__(16) uint16_t wcnt[PART_WARPS][NB_MAX + 1];
+    __shared__ uint32_t gbase[NB_MAX + 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr int SUB = PART_TILE / PART_WARPS;  // consecutive keys per warp
+    const uint32_t total_tiles = tile_base[nL];
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
         const uint32_t u = nspl[si], kp2 = next_pow2(u + 1), nb = 2 * u + 1;
         const uint32_t tl = t - tile_base[si];
         const uint32_t nt = tile_base[si + 1] - tile_base[si];
-        const uint32_t lo = tl * PART_TILE;
+        const uint32_t lo = tl * PART_TILE + w * SUB;
         for (uint32_t q = threadIdx.x; q + 1 < kp2; q += PART_THREADS)
             sspl[q] = spl[(uint64_t)si * SPL_STRIDE + q];
-        for (uint32_t q = threadIdx.x; q <= nb; q += PART_THREADS)
-#pragma unroll
-            for (int ww = 0; ww < PART_WARPS; ++ww) wcnt[ww][q] = 0;
+        {
+            uint32_t *w32 = reinterpret_cast<uint32_t *>(&wcnt[0][0]);
+            for (uint32_t q = threadIdx.x; q < PART_WARPS * (NB_MAX + 1) / 2; q += PART_THREADS)
+                w32[q] = 0;
+        }
         const int ib = s.flags & SEG_BUF1;
-        const uint64_t *Kin = a.keyb(ib) + s.start;
+        const ulonglong2 *Kin = a.keyb(ib) + s.start;
         const uint32_t *Iin = a.idxb(ib) + s.start;
-        uint64_t *Kout = a.keyb(ib ^ 1) + s.start;
+        ulonglong2 *Kout = a.keyb(ib ^ 1) + s.start;
         uint32_t *Iout = a.idxb(ib ^ 1) + s.start;
-        uint64_t kk[PART_ITEMS];
+        Key kk[PART_ITEMS];
         uint32_t ii[PART_ITEMS];
         uint32_t br[PART_ITEMS];
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t e = lo + w * SUB + c * 32 + lane;
+            const uint32_t e = lo + c * 32 + lane;
             const bool v = e < s.len;
-            kk[c] = v ? Kin[e] : 0;
+            kk[c] = v ? to_key(Kin[e]) : key_max();
             ii[c] = v ? Iin[e] : 0;
         }
         __syncthreads();
         const uint32_t lt = lanemask_lt();
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t e = lo + w * SUB + c * 32 + lane;
+            const uint32_t e = lo + c * 32 + lane;
             const uint32_t b = e < s.len ? classify(sspl, kp2, u, kk[c]) : nb;
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
             const uint32_t r = __popc(peers & lt);
             const uint32_t base = wcnt[w][b];
             __syncwarp();
-            if (r == 0) wcnt[w][b] = base + __popc(peers);
+            if (r == 0) wcnt[w][b] = (uint16_t)(base + __popc(peers));
             __syncwarp();
             br[c] = (b << 16) | (base + r);
         }
         __syncthreads();
-        // Exclusive scan over warps per bucket, plus the tile's global base.
+        // Exclusive scan over warps per bucket (tile-local, < PART_TILE) and
+        // the tile's global base per bucket.
         const uint32_t cmb = cm_base[si];
         const uint32_t seg0 = cm_scan[cmb];
         for (uint32_t q = threadIdx.x; q < nb; q += PART_THREADS) {
-            uint32_t run = cm_scan[cmb + (uint64_t)q * nt + tl] - seg0;
+            gbase[q] = cm_scan[cmb + (uint64_t)q * nt + tl] - seg0;
+            uint32_t run = 0;
 #pragma unroll
             for (int ww = 0; ww < PART_WARPS; ++ww) {
                 const uint32_t x = wcnt[ww][q];
-                wcnt[ww][q] = run;
+                wcnt[ww][q] = (uint16_t)run;
                 run += x;
             }
         }
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t e = lo + w * SUB + c * 32 + lane;
+            const uint32_t e = lo + c * 32 + lane;
             if (e < s.len) {
                 const uint32_t b = br[c] >> 16;
-                const uint32_t o = wcnt[w][b] + (br[c] & 0xFFFF);
-                Kout[o] = kk[c];
+                const uint32_t o = gbase[b] + wcnt[w][b] + (br[c] & 0xFFFF);
+                Kout[o] = from_key(kk[c]);
                 Iout[o] = ii[c];
             }
         }
@@ -470,8 +857,8 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(SortArgs a, const Seg 
 // ---- bucket emission: one CTA per partitioned segment ----------------------
 __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__restrict__ tile_base,
                        const uint32_t *__restrict__ nspl, const uint32_t *__restrict__ cm_base,
-                       const uint32_t *__restrict__ cm_scan, Seg *T, Seg *S, Seg *L2, Seg *E,
-                       uint2 *B, Counters *c) {
+                       const uint32_t *__restrict__ cm_scan, Seg *W1, Seg *W8, Seg *S, Seg *L2,
+                       Seg *E, uint2 *B, Seg *N, Counters *c) {
     const uint32_t si = blockIdx.x;
     const Seg s = L[si];
     const uint32_t u = nspl[si], nb = 2 * u + 1;
@@ -480,203 +867,517 @@ __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__
     const uint32_t seg0 = cm_scan[cmb];
     const uint32_t ob = (s.flags & SEG_BUF1) ^ 1u;
     const uint32_t flags = ob | SEG_KEYS;
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
-        const uint32_t off = cm_scan[cmb + (uint64_t)b * nt] - seg0;
-        const uint32_t end = b + 1 < nb ? cm_scan[cmb + (uint64_t)(b + 1) * nt] - seg0 : s.len;
-        const uint32_t len = end - off;
-        if (len == 0) continue;
+    // Uniform trip count: every warp reaches the collective appends.
+    for (uint32_t b0 = 0; b0 < nb; b0 += blockDim.x) {
+        const uint32_t b = b0 + threadIdx.x;
+        uint32_t off = 0, len = 0;
+        if (b < nb) {
+            off = cm_scan[cmb + (uint64_t)b * nt] - seg0;
+            const uint32_t end =
+                b + 1 < nb ? cm_scan[cmb + (uint64_t)(b + 1) * nt] - seg0 : s.len;
+            len = end - off;
+        }
         const uint32_t p = s.start + off;
-        if (off > 0) B[atomicAdd(&c->n_bound, 1u)] = make_uint2(p, s.depth);
-        if (len == 1) {
-            if (ob) {
-                a.idx[0][p] = a.idx[1][p];
-                a.key[0][p] = a.key[1][p];
+        uint32_t slot = warp_append(&c->n_bound, len > 0 && off > 0);
+        if (len > 0 && off > 0) B[slot] = make_uint2(p, s.depth);
+        if (len == 1 && ob) {
+            a.idx[0][p] = a.idx[1][p];
+            a.key[0][p] = a.key[1][p];
+        }
+        const bool multi = len > 1;
+        const bool eq = multi && (b & 1);
+        bool direct = false;
+        uint32_t nch = 0;
+        if (eq) {
+            const Key k = to_key(a.keyb(ob)[p]);
+            // In buffer 0 with its keys and not final: straight to the next round.
+            direct = !ob && !key_is_end(k);
+            if (!direct) nch = (len + EQ_TILE - 1) / EQ_TILE;
+        }
+        emit_next_warp(N, c, direct, p, len, s.depth + KEY_BYTES);
+        {
+            // nch equality work items per bucket: warp-level exclusive sum.
+            uint32_t incl = nch;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+                if ((threadIdx.x & 31) >= (uint32_t)d) incl += y;
             }
-            continue;
+            const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+            uint32_t base = 0;
+            if ((threadIdx.x & 31) == 31 && tot) base = atomicAdd(&c->n_equal, tot);
+            base = __shfl_sync(0xffffffffu, base, 31) + incl - nch;
+            for (uint32_t ch = 0; ch < nch; ++ch)
+                E[base + ch] = Seg{p, len, s.depth, ob | (ch << SEG_CHUNK_SHIFT)};
         }
         const Seg o{p, len, s.depth, flags};
-        if (b & 1) {
-            E[atomicAdd(&c->n_equal, 1u)] = Seg{p, len, s.depth, flags | SEG_EQUAL};
-        } else if (len <= (uint32_t)TINY_CAP) {
-            T[atomicAdd(&c->n_tiny, 1u)] = o;
-        } else if (len <= (uint32_t)SMALL_CAP) {
-            S[atomicAdd(&c->n_small, 1u)] = o;
-        } else {
-            L2[atomicAdd(&c->n_large_next, 1u)] = o;
-        }
+        const bool rng = multi && !(b & 1);
+        const bool w1 = rng && len <= (uint32_t)WARP1_CAP;
+        const bool w8 = rng && !w1 && len <= (uint32_t)WARP8_CAP;
+        const bool sm = rng && !w1 && !w8 && len <= (uint32_t)SMALL_CAP;
+        const bool lg = rng && !w1 && !w8 && !sm;
+        slot = warp_append(&c->n_w1, w1);
+        if (w1) W1[slot] = o;
+        slot = warp_append(&c->n_w8, w8);
+        if (w8) W8[slot] = o;
+        slot = warp_append(&c->n_small, sm);
+        if (sm) S[slot] = o;
+        slot = warp_append(&c->n_large_next, lg);
+        if (lg) L2[slot] = o;
     }
     if (threadIdx.x == 0) atomicAdd(&c->partitioned, (unsigned long long)s.len);
 }
 
-// ---- tiny segments: one warp, bitonic sort in registers --------------------
-constexpr int TINY_THREADS = 256;
+// ---- segments of <= 32 strings: one warp, one string per lane -------------
+constexpr int WARP_THREADS = 256;
 
-__global__ void __launch_bounds__(TINY_THREADS) k_tiny(SortArgs a, const Seg *__restrict__ T,
-                                                       uint32_t nT, Seg *N, Counters *c) {
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void load_elem(const SortArgs &a, const Seg &s, uint32_t e, Key &k,
+                                          uint32_t &id) {
+    const int b = s.flags & SEG_BUF1;
+    id = a.idxb(b)[s.start + e];
+    k = (s.flags & SEG_KEYS)
+            ? to_key(a.keyb(b)[s.start + e])
+            : load_key(a.arena, a.arena_bytes, string_offset(a.offs, a.off_width, id) + s.depth);
+}
+
+__global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *__restrict__ T,
+                                                        Seg *N, Counters *c) {
+    const uint32_t nT = c->n_w1;
+    const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long fresh = 0, keyed = 0;
     for (uint32_t g = warp0; g < nT; g += nwarps) {
         const Seg s = T[g];
-        const int b = s.flags & SEG_BUF1;
-        const bool v = (uint32_t)lane < s.len;
+        const bool v = lane < s.len;
         if (s.flags & SEG_KEYS)
             keyed += s.len;
         else
             fresh += s.len;
         uint32_t id = IDX_MAX;
-        uint64_t k = KEY_MAX;
-        if (v) {
-            id = a.idxb(b)[s.start + lane];
-            k = (s.flags & SEG_KEYS)
-                    ? a.keyb(b)[s.start + lane]
-                    : load_key(a.arena, a.arena_bytes,
-                               string_offset(a.offs, a.off_width, id) + s.depth);
+        Key k = key_max();
+        if (v) load_elem(a, s, lane, k, id);
+        // Bits in which the segment's keys differ.
+        Key k0;
+        k0.hi = __shfl_sync(0xffffffffu, k.hi, 0);
+        k0.lo = __shfl_sync(0xffffffffu, k.lo, 0);
+        uint64_t dh = v ? (k.hi ^ k0.hi) : 0, dl = v ? (k.lo ^ k0.lo) : 0;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            dh |= __shfl_xor_sync(0xffffffffu, dh, d);
+            dl |= __shfl_xor_sync(0xffffffffu, dl, d);
         }
+        if (dh | dl) {
+            // Packed 64-bit keys, then move each record to its rank.
+            const uint32_t f = clz128(dh, dl);
+            uint64_t sv[1] = {v ? sort_key(k, f, lane) : ~0ull};
+            warp_bitonic64<1>(sv, lane);
+            const uint32_t src = v ? (uint32_t)(sv[0] & 31) : lane;
+            Key kn;
+            kn.hi = __shfl_sync(0xffffffffu, k.hi, src);
+            kn.lo = __shfl_sync(0xffffffffu, k.lo, src);
+            const uint32_t idn = __shfl_sync(0xffffffffu, id, src);
+            k = kn;
+            id = idn;
+            // Pairs with equal windows must also be in full-key order.
+            Key kp;
+            kp.hi = __shfl_up_sync(0xffffffffu, k.hi, 1);
+            kp.lo = __shfl_up_sync(0xffffffffu, k.lo, 1);
+            const bool bad = v && lane > 0 &&
+                             (window64(kp, f) >> POS_BITS) == (window64(k, f) >> POS_BITS) &&
+                             key_lt(k, kp);
+            if (__any_sync(0xffffffffu, bad)) {
 #pragma unroll
-        for (int kk = 2; kk <= 32; kk <<= 1) {
+                for (int kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
-            for (int j = kk >> 1; j > 0; j >>= 1) {
-                const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, j);
-                const uint32_t oi = __shfl_xor_sync(0xffffffffu, id, j);
-                const bool want_min = ((lane & j) == 0) == ((lane & kk) == 0);
-                const bool other_less = pair_less(ok, oi, k, id);
-                const bool other_more = pair_less(k, id, ok, oi);
-                if (want_min ? other_less : other_more) {
-                    k = ok;
-                    id = oi;
+                    for (int j = kk >> 1; j > 0; j >>= 1) {
+                        Key ok;
+                        ok.hi = __shfl_xor_sync(0xffffffffu, k.hi, j);
+                        ok.lo = __shfl_xor_sync(0xffffffffu, k.lo, j);
+                        const uint32_t oi = __shfl_xor_sync(0xffffffffu, id, j);
+                        const bool keep_min = ((lane & j) == 0) == ((lane & kk) == 0);
+                        const bool take =
+                            keep_min ? pair_lt(ok, oi, k, id) : pair_lt(k, id, ok, oi);
+                        if (take) {
+                            k = ok;
+                            id = oi;
+                        }
+                    }
                 }
             }
         }
-        const uint64_t prev = __shfl_up_sync(0xffffffffu, k, 1);
-        const uint64_t next = __shfl_down_sync(0xffffffffu, k, 1);
-        const bool head = v && (lane == 0 || prev != k);
+        Key prev, next;
+        prev.hi = __shfl_up_sync(0xffffffffu, k.hi, 1);
+        prev.lo = __shfl_up_sync(0xffffffffu, k.lo, 1);
+        next.hi = __shfl_down_sync(0xffffffffu, k.hi, 1);
+        next.lo = __shfl_down_sync(0xffffffffu, k.lo, 1);
+        const bool head = v && (lane == 0 || !key_eq(prev, k));
         const uint32_t heads = __ballot_sync(0xffffffffu, head);
+        bool want = false;
+        uint32_t h = 0;
         if (v) {
             const uint32_t p = s.start + lane;
             a.idx[0][p] = id;
-            if (lane == 0 || (uint32_t)lane == s.len - 1) a.key[0][p] = k;
+            if (lane == 0 || lane == s.len - 1) a.key[0][p] = from_key(k);
             if (lane > 0) {
-                if (prev != k)
+                if (!key_eq(prev, k))
                     a.lcp[p] = s.depth + key_lcp(prev, k);
                 else if (key_is_end(k))
                     a.lcp[p] = s.depth + key_len(k);
             }
-            const bool tail = (uint32_t)lane == s.len - 1 || next != k;
+            const bool tail = lane == s.len - 1 || !key_eq(next, k);
             if (tail && !head && !key_is_end(k)) {
                 const uint32_t m = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
-                const uint32_t h = 31 - __clz(heads & m);
-                emit_next(N, c, s.start + h, lane - h + 1, s.depth + 8);
+                h = 31 - __clz(heads & m);
+                want = true;
             }
         }
+        emit_next_warp(N, c, want, s.start + h, lane - h + 1, s.depth + KEY_BYTES);
     }
     if (lane == 0 && (fresh | keyed)) {
-        atomicAdd(&c->tiny_fresh, fresh);
-        atomicAdd(&c->tiny_keyed, keyed);
+        atomicAdd(&c->warp1_fresh, fresh);
+        atomicAdd(&c->warp1_keyed, keyed);
     }
 }
 
-// ---- small segments: one CTA, bitonic sort in shared memory -----------------
-__global__ void __launch_bounds__(SMALL_THREADS) k_small(SortArgs a, const Seg *__restrict__ S,
-                                                         uint32_t nS, Seg *N, Counters *c) {
-    __shared__ uint64_t sk[SMALL_CAP];
-    __shared__ uint32_t sx[SMALL_CAP];
+// True when the records at padded positions 0..len-1 are in (key, index)
+// order wherever the packed keys could not tell them apart (equal windows).
+// Called by `threads` threads numbered t; returns a per-thread verdict that
+// the caller combines.
+__device__ __forceinline__ bool window_pairs_ok(const ulonglong2 *sk, uint32_t len, uint32_t f,
+                                                uint32_t t, uint32_t threads) {
+    bool ok = true;
+    for (uint32_t e = t + 1; e < len; e += threads) {
+        const Key kp = to_key(sk[pad(e - 1)]), k = to_key(sk[pad(e)]);
+        if ((window64(kp, f) >> POS_BITS) == (window64(k, f) >> POS_BITS) && key_lt(k, kp))
+            ok = false;
+    }
+    return ok;
+}
+
+// Warp-wide OR of key ^ key0 over the records at padded positions 0..len-1.
+__device__ __forceinline__ uint32_t warp_diff_bit(const ulonglong2 *sk, uint32_t len,
+                                                  uint32_t lane) {
+    const Key k0 = to_key(sk[pad(0)]);
+    uint64_t dh = 0, dl = 0;
+    for (uint32_t e = lane; e < len; e += 32) {
+        const Key k = to_key(sk[pad(e)]);
+        dh |= k.hi ^ k0.hi;
+        dl |= k.lo ^ k0.lo;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        dh |= __shfl_xor_sync(0xffffffffu, dh, d);
+        dl |= __shfl_xor_sync(0xffffffffu, dl, d);
+    }
+    return (dh | dl) ? clz128(dh, dl) : 128u;
+}
+
+// One warp sorts the len (<= 32 * ITEMS) records at padded positions
+// 0..len-1 of sk/sx by packed keys; returns false if the window check fails.
+template <int ITEMS>
+__device__ __forceinline__ bool warp_sort_packed(ulonglong2 *sk, uint32_t *sx, uint32_t len,
+                                                 uint32_t f, uint32_t lane) {
+    uint64_t v[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t e = lane * ITEMS + i;
+        v[i] = e < len ? sort_key(to_key(sk[pad(e)]), f, e) : ~0ull;
+    }
+    warp_bitonic64<ITEMS>(v, lane);
+    Key k[ITEMS];
+    uint32_t x[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t e = lane * ITEMS + i;
+        if (e < len) {
+            const uint32_t src = (uint32_t)(v[i] & POS_MASK);
+            k[i] = to_key(sk[pad(src)]);
+            x[i] = sx[pad(src)];
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t e = lane * ITEMS + i;
+        if (e < len) {
+            sk[pad(e)] = from_key(k[i]);
+            sx[pad(e)] = x[i];
+        }
+    }
+    __syncwarp();
+    return __all_sync(0xffffffffu, window_pairs_ok(sk, len, f, lane, 32));
+}
+
+// ---- segments of 33..256 strings: one warp, 2/4/8 strings per lane ----------
+constexpr int W8_PAD = WARP8_CAP + WARP8_CAP / 8;
+
+__global__ void __launch_bounds__(WARP_THREADS, 2) k_warp8(SortArgs a, const Seg *__restrict__ T,
+                                                           Seg *N, Counters *c) {
+    __shared__ ulonglong2 sk_all[WARP_THREADS / 32][W8_PAD];
+    __shared__ uint32_t sx_all[WARP_THREADS / 32][W8_PAD];
+    const uint32_t nT = c->n_w8;
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    ulonglong2 *sk = sk_all[w];
+    uint32_t *sx = sx_all[w];
+    const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long fresh = 0, keyed = 0;
-    for (uint32_t g = blockIdx.x; g < nS; g += gridDim.x) {
-        const Seg s = S[g];
-        const int b = s.flags & SEG_BUF1;
-        const uint32_t P = next_pow2(s.len);
+    for (uint32_t g = warp0; g < nT; g += nwarps) {
+        const Seg s = T[g];
         if (s.flags & SEG_KEYS)
             keyed += s.len;
         else
             fresh += s.len;
-        for (uint32_t i = threadIdx.x; i < P; i += SMALL_THREADS) {
-            if (i < s.len) {
-                const uint32_t id = a.idxb(b)[s.start + i];
-                sx[i] = id;
-                sk[i] = (s.flags & SEG_KEYS)
-                            ? a.keyb(b)[s.start + i]
-                            : load_key(a.arena, a.arena_bytes,
-                                       string_offset(a.offs, a.off_width, id) + s.depth);
-            } else {
-                sx[i] = IDX_MAX;
-                sk[i] = KEY_MAX;
+        const uint32_t P = next_pow2(s.len);
+        for (uint32_t e = lane; e < P; e += 32) {
+            Key k = key_max();
+            uint32_t id = IDX_MAX;
+            if (e < s.len) load_elem(a, s, e, k, id);
+            sk[pad(e)] = from_key(k);
+            sx[pad(e)] = id;
+        }
+        __syncwarp();
+        const uint32_t f = warp_diff_bit(sk, s.len, lane);
+        if (f < 128) {
+            bool ok;
+            if (P <= 64)
+                ok = warp_sort_packed<2>(sk, sx, s.len, f, lane);
+            else if (P <= 128)
+                ok = warp_sort_packed<4>(sk, sx, s.len, f, lane);
+            else
+                ok = warp_sort_packed<8>(sk, sx, s.len, f, lane);
+            if (!ok) {
+                if (P <= 64)
+                    warp_sort_run<2>(sk, sx, 0, lane);
+                else if (P <= 128)
+                    warp_sort_run<4>(sk, sx, 0, lane);
+                else
+                    warp_sort_run<8>(sk, sx, 0, lane);
             }
         }
-        __syncthreads();
-        for (uint32_t k = 2; k <= P; k <<= 1) {
-            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t i = threadIdx.x; i < P; i += SMALL_THREADS) {
-                    const uint32_t l = i ^ j;
-                    if (l > i) {
-                        const uint64_t ki = sk[i], kl = sk[l];
-                        const uint32_t xi = sx[i], xl = sx[l];
-                        const bool asc = (i & k) == 0;
-                        if (pair_less(kl, xl, ki, xi) == asc) {
-                            sk[i] = kl;
-                            sk[l] = ki;
-                            sx[i] = xl;
-                            sx[l] = xi;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
-        }
-        for (uint32_t i = threadIdx.x; i < s.len; i += SMALL_THREADS) {
-            const uint32_t p = s.start + i;
-            const uint64_t k = sk[i];
-            a.idx[0][p] = sx[i];
-            if (i == 0 || i == s.len - 1) a.key[0][p] = k;
-            const bool same_prev = i > 0 && sk[i - 1] == k;
-            if (i > 0) {
-                if (!same_prev)
-                    a.lcp[p] = s.depth + key_lcp(sk[i - 1], k);
-                else if (key_is_end(k))
-                    a.lcp[p] = s.depth + key_len(k);
-            }
-            const bool tail = i == s.len - 1 || sk[i + 1] != k;
-            if (tail && same_prev && !key_is_end(k)) {
-                // First position of this run: lower bound of k in sk[0..i].
-                uint32_t lo = 0, hi = i;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (sk[mid] < k)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
-                }
-                emit_next(N, c, s.start + lo, i - lo + 1, s.depth + 8);
-            }
-        }
-        __syncthreads();
+        __syncwarp();
+        finish_segment(a, s, sk, sx, lane, 32, N, c);
+        __syncwarp();
     }
-    if (threadIdx.x == 0 && (fresh | keyed)) {
-        atomicAdd(&c->small_fresh, fresh);
-        atomicAdd(&c->small_keyed, keyed);
+    if (lane == 0 && (fresh | keyed)) {
+        atomicAdd(&c->warp8_fresh, fresh);
+        atomicAdd(&c->warp8_keyed, keyed);
     }
 }
 
-// ---- equality buckets ------------------------------------------------------
-__global__ void k_equal(SortArgs a, const Seg *__restrict__ E, uint32_t nE,
-                        const uint32_t *__restrict__ tile_base, uint32_t total_tiles, Seg *N,
-                        Counters *c) {
-    unsigned long long moved = 0, fin = 0;
-    for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-        const uint32_t si = find_seg(tile_base, nE, t);
-        const Seg s = E[si];
-        const int b = s.flags & SEG_BUF1;
-        const uint64_t k = a.keyb(b)[s.start];
-        const bool end = key_is_end(k);
-        const uint32_t tl = t - tile_base[si];
-        if (tl == 0 && threadIdx.x == 0) {
-            a.key[0][s.start] = k;
-            a.key[0][s.start + s.len - 1] = k;
-            if (!end) emit_next(N, c, s.start, s.len, s.depth + 8);
+// ---- segments of 257..SMALL_CAP strings: one CTA ---------------------------
+constexpr int SMALL_PAD = SMALL_CAP + SMALL_CAP / 8;
+constexpr size_t BLOCK_SMEM = SMALL_PAD * (sizeof(ulonglong2) + sizeof(uint32_t) + sizeof(uint64_t));
+
+// Full-comparator sort of the span (multiple of RUN) records at padded
+// positions 0..span-1: warp runs of RUN, then pairwise merge-path merges.
+__device__ __noinline__ void block_sort_full(ulonglong2 *sk, uint32_t *sx, uint32_t span) {
+    constexpr uint32_t RUN = 32 * SMALL_ITEMS;
+    const uint32_t nruns = span / RUN;
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (w < nruns) warp_sort_run<SMALL_ITEMS>(sk, sx, w * RUN, lane);
+    __syncthreads();
+    for (uint32_t run = RUN; run < span; run <<= 1) {
+        const uint32_t o = threadIdx.x * SMALL_ITEMS;
+        Key ok[SMALL_ITEMS];
+        uint32_t ox[SMALL_ITEMS];
+        const bool active = o < span;
+        if (active) {
+            const uint32_t a0 = o / (2 * run) * (2 * run);
+            const uint32_t b0 = a0 + run;
+            const uint32_t la = min(run, span - a0);
+            const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
+            const uint32_t d = o - a0;
+            uint32_t ia = merge_split(sk, sx, a0, la, b0, lb, d);
+            uint32_t ib = d - ia;
+#pragma unroll
+            for (int i = 0; i < SMALL_ITEMS; ++i) {
+                bool take_a = ib >= lb;
+                Key ka, kb;
+                uint32_t xa = 0, xb = 0;
+                if (ia < la) {
+                    ka = to_key(sk[pad(a0 + ia)]);
+                    xa = sx[pad(a0 + ia)];
+                }
+                if (ib < lb) {
+                    kb = to_key(sk[pad(b0 + ib)]);
+                    xb = sx[pad(b0 + ib)];
+                    if (ia < la) take_a = !pair_lt(kb, xb, ka, xa);
+                }
+                if (take_a) {
+                    ok[i] = ka;
+                    ox[i] = xa;
+                    ++ia;
+                } else {
+                    ok[i] = kb;
+                    ox[i] = xb;
+                    ++ib;
+                }
+            }
         }
-        if (!b && !end) continue;
-        const uint32_t lo = tl * EQ_TILE;
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < SMALL_ITEMS; ++i) {
+                sk[pad(o + i)] = from_key(ok[i]);
+                sx[pad(o + i)] = ox[i];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(SMALL_THREADS, 2) k_block(SortArgs a, const Seg *__restrict__ S,
+                                                            Seg *N, Counters *c) {
+    extern __shared__ __align__(16) unsigned char block_smem[];
+    ulonglong2 *sk = reinterpret_cast<ulonglong2 *>(block_smem);
+    uint64_t *sv = reinterpret_cast<uint64_t *>(sk + SMALL_PAD);
+    uint32_t *sx = reinterpret_cast<uint32_t *>(sv + SMALL_PAD);
+    __shared__ uint64_t red[2][SMALL_THREADS / 32];
+    constexpr uint32_t RUN = 32 * SMALL_ITEMS;
+    const uint32_t nS = c->n_small;
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long fresh = 0, keyed = 0;
+    for (uint32_t g = blockIdx.x; g < nS; g += gridDim.x) {
+        const Seg s = S[g];
+        if (s.flags & SEG_KEYS)
+            keyed += s.len;
+        else
+            fresh += s.len;
+        const uint32_t nruns = (s.len + RUN - 1) / RUN;
+        const uint32_t span = nruns * RUN;
+        for (uint32_t e = threadIdx.x; e < span; e += SMALL_THREADS) {
+            Key k = key_max();
+            uint32_t id = IDX_MAX;
+            if (e < s.len) load_elem(a, s, e, k, id);
+            sk[pad(e)] = from_key(k);
+            sx[pad(e)] = id;
+        }
+        __syncthreads();
+        // f: first bit in which the keys differ.
+        {
+            const Key k0 = to_key(sk[pad(0)]);
+            uint64_t dh = 0, dl = 0;
+            for (uint32_t e = threadIdx.x; e < s.len; e += SMALL_THREADS) {
+                const Key k = to_key(sk[pad(e)]);
+                dh |= k.hi ^ k0.hi;
+                dl |= k.lo ^ k0.lo;
+            }
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                dh |= __shfl_xor_sync(0xffffffffu, dh, d);
+                dl |= __shfl_xor_sync(0xffffffffu, dl, d);
+            }
+            if (lane == 0) {
+                red[0][w] = dh;
+                red[1][w] = dl;
+            }
+        }
+        __syncthreads();
+        uint64_t dh = 0, dl = 0;
+#pragma unroll
+        for (int q = 0; q < SMALL_THREADS / 32; ++q) {
+            dh |= red[0][q];
+            dl |= red[1][q];
+        }
+        if (dh | dl) {
+            const uint32_t f = clz128(dh, dl);
+            // Packed keys: warp runs of RUN, then merges, all on uint64.
+            if (w < nruns) {
+                uint64_t v[SMALL_ITEMS];
+#pragma unroll
+                for (int i = 0; i < SMALL_ITEMS; ++i) {
+                    const uint32_t e = w * RUN + lane * SMALL_ITEMS + i;
+                    v[i] = e < s.len ? sort_key(to_key(sk[pad(e)]), f, e) : ~0ull;
+                }
+                warp_bitonic64<SMALL_ITEMS>(v, lane);
+#pragma unroll
+                for (int i = 0; i < SMALL_ITEMS; ++i)
+                    sv[pad(w * RUN + lane * SMALL_ITEMS + i)] = v[i];
+            }
+            __syncthreads();
+            for (uint32_t run = RUN; run < span; run <<= 1) {
+                const uint32_t o = threadIdx.x * SMALL_ITEMS;
+                uint64_t ov[SMALL_ITEMS];
+                const bool active = o < span;
+                if (active) {
+                    const uint32_t a0 = o / (2 * run) * (2 * run);
+                    const uint32_t b0 = a0 + run;
+                    const uint32_t la = min(run, span - a0);
+                    const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
+                    const uint32_t d = o - a0;
+                    uint32_t ia = merge_split64(sv, a0, la, b0, lb, d);
+                    uint32_t ib = d - ia;
+#pragma unroll
+                    for (int i = 0; i < SMALL_ITEMS; ++i) {
+                        const uint64_t va = ia < la ? sv[pad(a0 + ia)] : ~0ull;
+                        const uint64_t vb = ib < lb ? sv[pad(b0 + ib)] : ~0ull;
+                        const bool take_a = ib >= lb || (ia < la && va < vb);
+                        ov[i] = take_a ? va : vb;
+                        ia += take_a;
+                        ib += !take_a;
+                    }
+                }
+                __syncthreads();
+                if (active) {
+#pragma unroll
+                    for (int i = 0; i < SMALL_ITEMS; ++i) sv[pad(o + i)] = ov[i];
+                }
+                __syncthreads();
+            }
+            // Move every record to its rank (through registers: in place).
+            Key k[SMALL_ITEMS];
+            uint32_t x[SMALL_ITEMS];
+#pragma unroll
+            for (int i = 0; i < SMALL_ITEMS; ++i) {
+                const uint32_t e = threadIdx.x + i * SMALL_THREADS;
+                if (e < s.len) {
+                    const uint32_t src = (uint32_t)(sv[pad(e)] & POS_MASK);
+                    k[i] = to_key(sk[pad(src)]);
+                    x[i] = sx[pad(src)];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < SMALL_ITEMS; ++i) {
+                const uint32_t e = threadIdx.x + i * SMALL_THREADS;
+                if (e < s.len) {
+                    sk[pad(e)] = from_key(k[i]);
+                    sx[pad(e)] = x[i];
+                }
+            }
+            __syncthreads();
+            const bool ok =
+                __syncthreads_and(window_pairs_ok(sk, s.len, f, threadIdx.x, SMALL_THREADS));
+            if (!ok) block_sort_full(sk, sx, span);
+        }
+        __syncthreads();
+        finish_segment(a, s, sk, sx, threadIdx.x, SMALL_THREADS, N, c);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && (fresh | keyed)) {
+        atomicAdd(&c->block_fresh, fresh);
+        atomicAdd(&c->block_keyed, keyed);
+    }
+}
+
+// ---- equality buckets: work items of up to EQ_TILE strings ------------------
+__global__ void k_equal(SortArgs a, const Seg *__restrict__ E, Seg *N, Counters *c) {
+    const uint32_t nE = c->n_equal;
+    unsigned long long moved = 0, fin = 0;
+    for (uint32_t g = blockIdx.x; g < nE; g += gridDim.x) {
+        const Seg s = E[g];
+        const int b = s.flags & SEG_BUF1;
+        const uint32_t ch = s.flags >> SEG_CHUNK_SHIFT;
+        const Key k = to_key(a.keyb(b)[s.start]);
+        const bool end = key_is_end(k);
+        if (ch == 0 && threadIdx.x == 0) {
+            a.key[0][s.start] = from_key(k);
+            a.key[0][s.start + s.len - 1] = from_key(k);
+            if (!end) emit_next(N, c, s.start, s.len, s.depth + KEY_BYTES);
+        }
+        const uint32_t lo = ch * EQ_TILE;
         const uint32_t hi = min(lo + (uint32_t)EQ_TILE, s.len);
         if (threadIdx.x == 0) {
             if (b) moved += hi - lo;
@@ -695,11 +1396,12 @@ __global__ void k_equal(SortArgs a, const Seg *__restrict__ E, uint32_t nE,
     }
 }
 
-__global__ void k_boundary(SortArgs a, const uint2 *__restrict__ B, uint32_t nB) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nB) return;
-    const uint2 e = B[i];
-    a.lcp[e.x] = e.y + key_lcp(a.key[0][e.x - 1], a.key[0][e.x]);
+__global__ void k_boundary(SortArgs a, const uint2 *__restrict__ B, Counters *c) {
+    const uint32_t nB = c->n_bound;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nB; i += gridDim.x * blockDim.x) {
+        const uint2 e = B[i];
+        a.lcp[e.x] = e.y + key_lcp(to_key(a.key[0][e.x - 1]), to_key(a.key[0][e.x]));
+    }
 }
 
 }  // namespace
@@ -712,10 +1414,10 @@ void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st) {
     k_iota<<<g ? g : 1, 256, 0, st>>>(idx, n);
 }
 
-void launch_classify(const Seg *R, uint32_t nR, Seg *T, Seg *S, Seg *L, Counters *c,
+void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L, Counters *c,
                      cudaStream_t st) {
     if (!nR) return;
-    k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, T, S, L, c);
+    k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, W1, W8, S, L, c);
 }
 
 void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
@@ -726,73 +1428,83 @@ void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *ou
 
 uint32_t scan_partials_needed(uint32_t n) { return cdiv(n ? n : 1, SCAN_CHUNK) + 1; }
 
-void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *partials,
-                 cudaStream_t st) {
-    const uint32_t nb = cdiv(n ? n : 1, SCAN_CHUNK);
-    k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(in, n, partials);
+void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
+                 uint32_t *partials, cudaStream_t st) {
+    const uint32_t nb = cdiv(n_host ? n_host : 1, SCAN_CHUNK);
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(in, n_host, n_dev, partials);
     k_scan_partials<<<1, SCAN_THREADS, 0, st>>>(partials, nb);
-    k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(in, out, n, partials, nb);
+    k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(in, out, n_host, n_dev, partials, nb);
 }
 
 void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                   uint32_t total_tiles, int grid, cudaStream_t st) {
-    if (!total_tiles) return;
-    k_gather<<<grid, GATHER_THREADS, 0, st>>>(a, L, nL, tile_base, total_tiles);
+                   int grid, cudaStream_t st) {
+    if (!nL) return;
+    k_gather<<<grid, GATHER_THREADS, 0, st>>>(a, L, nL, tile_base);
 }
 
-void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, uint64_t *spl, uint32_t *nspl,
+void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl, uint32_t *nspl,
                    uint32_t *ntiles, uint32_t *cm_size, cudaStream_t st) {
     if (!nL) return;
-    k_sample<<<nL, SAMPLE_THREADS, 0, st>>>(a, L, spl, nspl, ntiles, cm_size);
+    static bool attr = false;
+    const int smem = SAMPLES_MAX * sizeof(ulonglong2);
+    if (!attr) {
+        cudaFuncSetAttribute(k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    k_sample<<<nL, SAMPLE_THREADS, smem, st>>>(a, L, spl, nspl, ntiles, cm_size);
 }
 
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                  uint32_t total_tiles, const uint64_t *spl, const uint32_t *nspl,
-                  const uint32_t *cm_base, uint32_t *cm, int grid, cudaStream_t st) {
-    if (!total_tiles) return;
-    k_count<<<grid, PART_THREADS, 0, st>>>(a, L, nL, tile_base, total_tiles, spl, nspl, cm_base,
-                                           cm);
+                  const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
+                  uint32_t *cm, int grid, cudaStream_t st) {
+    if (!nL) return;
+    k_count<<<grid, PART_THREADS, 0, st>>>(a, L, nL, tile_base, spl, nspl, cm_base, cm);
 }
 
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                    uint32_t total_tiles, const uint64_t *spl, const uint32_t *nspl,
-                    const uint32_t *cm_base, const uint32_t *cm_scan, int grid,
-                    cudaStream_t st) {
-    if (!total_tiles) return;
-    k_scatter<<<grid, PART_THREADS, 0, st>>>(a, L, nL, tile_base, total_tiles, spl, nspl,
-                                             cm_base, cm_scan);
+                    const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
+                    const uint32_t *cm_scan, int grid, cudaStream_t st) {
+    if (!nL) return;
+    k_scatter<<<grid, PART_THREADS, 0, st>>>(a, L, nL, tile_base, spl, nspl, cm_base, cm_scan);
 }
 
 void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                  const uint32_t *nspl, const uint32_t *cm_base, const uint32_t *cm_scan,
-                 Seg *T, Seg *S, Seg *L2, Seg *E, uint2 *B, Counters *c, cudaStream_t st) {
-    if (!nL) return;
-    k_emit<<<nL, 256, 0, st>>>(a, L, tile_base, nspl, cm_base, cm_scan, T, S, L2, E, B, c);
-}
-
-void launch_tiny(const SortArgs &a, const Seg *T, uint32_t nT, Seg *N, Counters *c, int grid,
+                 Seg *W1, Seg *W8, Seg *S, Seg *L2, Seg *E, uint2 *B, Seg *N, Counters *c,
                  cudaStream_t st) {
-    if (!nT) return;
-    const uint32_t need = cdiv(nT, TINY_THREADS / 32);
-    k_tiny<<<need < (uint32_t)grid ? need : (uint32_t)grid, TINY_THREADS, 0, st>>>(a, T, nT, N, c);
+    if (!nL) return;
+    k_emit<<<nL, 256, 0, st>>>(a, L, tile_base, nspl, cm_base, cm_scan, W1, W8, S, L2, E, B, N,
+                               c);
 }
 
-void launch_small(const SortArgs &a, const Seg *S, uint32_t nS, Seg *N, Counters *c, int grid,
+void launch_warp1(const SortArgs &a, const Seg *W1, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
-    if (!nS) return;
-    k_small<<<nS < (uint32_t)grid ? nS : (uint32_t)grid, SMALL_THREADS, 0, st>>>(a, S, nS, N, c);
+    k_warp1<<<grid, WARP_THREADS, 0, st>>>(a, W1, N, c);
 }
 
-void launch_equal(const SortArgs &a, const Seg *E, uint32_t nE, const uint32_t *tile_base,
-                  uint32_t total_tiles, Seg *N, Counters *c, int grid, cudaStream_t st) {
-    if (!total_tiles) return;
-    const uint32_t g = total_tiles < (uint32_t)grid ? total_tiles : (uint32_t)grid;
-    k_equal<<<g, 256, 0, st>>>(a, E, nE, tile_base, total_tiles, N, c);
+void launch_warp8(const SortArgs &a, const Seg *W8, Seg *N, Counters *c, int grid,
+                  cudaStream_t st) {
+    k_warp8<<<grid, WARP_THREADS, 0, st>>>(a, W8, N, c);
 }
 
-void launch_boundary(const SortArgs &a, const uint2 *B, uint32_t nB, cudaStream_t st) {
-    if (!nB) return;
-    k_boundary<<<cdiv(nB, 256), 256, 0, st>>>(a, B, nB);
+void launch_block(const SortArgs &a, const Seg *S, Seg *N, Counters *c, int grid,
+                  cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)BLOCK_SMEM);
+        attr = true;
+    }
+    k_block<<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, N, c);
+}
+
+void launch_equal(const SortArgs &a, const Seg *E, Seg *N, Counters *c, int grid,
+                  cudaStream_t st) {
+    k_equal<<<grid, 256, 0, st>>>(a, E, N, c);
+}
+
+void launch_boundary(const SortArgs &a, const uint2 *B, Counters *c, int grid, cudaStream_t st) {
+    k_boundary<<<grid, 256, 0, st>>>(a, B, c);
 }
 
 }  // namespace ssort

@@ -42,10 +42,12 @@ class Stats(ctypes.Structure):
         ("device_bytes", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
         ("gather_elems", ctypes.c_uint64),
-        ("tiny_fresh", ctypes.c_uint64),
-        ("tiny_keyed", ctypes.c_uint64),
-        ("small_fresh", ctypes.c_uint64),
-        ("small_keyed", ctypes.c_uint64),
+        ("warp1_fresh", ctypes.c_uint64),
+        ("warp1_keyed", ctypes.c_uint64),
+        ("warp8_fresh", ctypes.c_uint64),
+        ("warp8_keyed", ctypes.c_uint64),
+        ("block_fresh", ctypes.c_uint64),
+        ("block_keyed", ctypes.c_uint64),
         ("equal_moved", ctypes.c_uint64),
         ("equal_final", ctypes.c_uint64),
         ("boundaries", ctypes.c_uint64),
