@@ -62,7 +62,7 @@ struct ssort_ctx {
     cudaStream_t st = nullptr;
 
     // workspace
-    DBuf idx1, key0, key1, lcp, R, N, W1, W8, S, E, B, L, L2, spl, nspl, ntiles, cm_size,
+    DBuf idx1, key0, key1, lcp, R, N, W1, W8, S, E, B, L, L2, spl, nspl, tbl, ntiles, cm_size,
         tile_base, cm_base, tmp, cm, partials, ctr;
     size_t cm_cap = 0;
     DBuf arena, offs, perm;  // staging for the host-buffer entry points
@@ -192,6 +192,7 @@ int ssort_ctx::reserve(uint32_t n, bool need_internal_lcp) {
     SS_TRY(ensure(L2, nlarge * sizeof(Seg)));
     SS_TRY(ensure(spl, nlarge * SPL_STRIDE * sizeof(ulonglong2)));
     SS_TRY(ensure(nspl, nlarge * 4));
+    SS_TRY(ensure(tbl, nlarge * TBL_STRIDE * sizeof(uint16_t)));
     SS_TRY(ensure(ntiles, nlarge * 4));
     SS_TRY(ensure(cm_size, nlarge * 4));
     SS_TRY(ensure(cm_base, (nlarge + 1) * 4));
@@ -245,7 +246,7 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
     uint32_t n_cur = 1;
     uint64_t live = n;
     uint32_t round = 0;
-    const int g8 = grid_for(8), g4 = grid_for(4);
+    const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
 
     while (n_cur) {
         SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
@@ -275,19 +276,22 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
             stats.partition_levels++;
             LAUNCH(this, "sample",
                    launch_sample(a, lcur, n_large, (ulonglong2 *)spl.p, (uint32_t *)nspl.p,
-                                 (uint32_t *)ntiles.p, (uint32_t *)cm_size.p, st));
+                                 (uint16_t *)tbl.p, (uint32_t *)ntiles.p, (uint32_t *)cm_size.p,
+                                 st));
             SS_TRY(scan((const uint32_t *)ntiles.p, (uint32_t *)tile_base.p, n_large, nullptr));
             SS_TRY(scan((const uint32_t *)cm_size.p, (uint32_t *)cm_base.p, n_large, nullptr));
             LAUNCH(this, "count",
                    launch_count(a, lcur, n_large, (const uint32_t *)tile_base.p,
                                 (const ulonglong2 *)spl.p, (const uint32_t *)nspl.p,
-                                (const uint32_t *)cm_base.p, (uint32_t *)cm.p, g4, st));
+                                (const uint16_t *)tbl.p, (const uint32_t *)cm_base.p,
+                                (uint32_t *)cm.p, g2, st));
             SS_TRY(scan((const uint32_t *)cm.p, (uint32_t *)cm.p, (uint32_t)(cm_cap - 1),
                         (const uint32_t *)cm_base.p + n_large));
             LAUNCH(this, "scatter",
                    launch_scatter(a, lcur, n_large, (const uint32_t *)tile_base.p,
                                   (const ulonglong2 *)spl.p, (const uint32_t *)nspl.p,
-                                  (const uint32_t *)cm_base.p, (const uint32_t *)cm.p, g4, st));
+                                  (const uint16_t *)tbl.p, (const uint32_t *)cm_base.p,
+                                  (const uint32_t *)cm.p, g2, st));
             LAUNCH(this, "emit",
                    launch_emit(a, lcur, n_large, (const uint32_t *)tile_base.p,
                                (const uint32_t *)nspl.p, (const uint32_t *)cm_base.p,
@@ -355,7 +359,7 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
     if (ctx->prof) ctx->prof_collect();
     size_t held = 0;
     for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->W1,
-                    &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
+                    &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl, &ctx->tbl,
                     &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
                     &ctx->cm, &ctx->partials, &ctx->arena, &ctx->offs, &ctx->perm})
         held += b->cap;
@@ -449,7 +453,7 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
     with_device(ctx, [&]() -> int {
         if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
         for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->W1,
-                        &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl,
+                        &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl, &ctx->tbl,
                         &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
                         &ctx->cm, &ctx->partials, &ctx->ctr, &ctx->arena, &ctx->offs,
                         &ctx->perm})

@@ -46,6 +46,11 @@ constexpr int SMALL_ITEMS = SMALL_CAP / SMALL_THREADS;  // 8
 // Sample partitioning of large segments.
 constexpr int KMAX = 511;               // splitters per segment and pass
 constexpr int SPL_STRIDE = 512;         // splitter slots per segment (pow2)
+// Splitter lookup table: for the 12 key bits after the splitters' common
+// prefix, the index range of splitters carrying those bits.
+constexpr int TBL_BITS = 12;
+constexpr int TBL_N = 1 << TBL_BITS;
+constexpr int TBL_STRIDE = TBL_N + 64;  // uint16 entries per segment (TBL_N + 1 used)
 constexpr int NB_MAX = 2 * KMAX + 1;    // range + equality buckets
 constexpr int SAMPLES_MAX = 4096;       // keys sampled per large segment
 constexpr int TARGET_BUCKET = 512;      // wanted strings per range bucket
@@ -100,13 +105,15 @@ uint32_t scan_partials_needed(uint32_t n);
 void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                    int grid, cudaStream_t st);
 void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl,
-                   uint32_t *nspl, uint32_t *ntiles, uint32_t *cm_size, cudaStream_t st);
+                   uint32_t *nspl, uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size,
+                   cudaStream_t st);
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                  const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
-                  uint32_t *cm, int grid, cudaStream_t st);
+                  const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
+                  const uint32_t *cm_base, uint32_t *cm, int grid, cudaStream_t st);
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                    const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
-                    const uint32_t *cm_scan, int grid, cudaStream_t st);
+                    const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
+                    const uint32_t *cm_base, const uint32_t *cm_scan, int grid,
+                    cudaStream_t st);
 void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                  const uint32_t *nspl, const uint32_t *cm_base, const uint32_t *cm_scan,
                  Seg *W1, Seg *W8, Seg *S, Seg *L2, Seg *E, uint2 *B, Seg *N, Counters *c,

@@ -208,6 +208,35 @@ __device__ __forceinline__ uint32_t classify(const ulonglong2 *s, uint32_t kp2, 
     return (lo < u && key_eq(to_key(s[lo]), key)) ? 2 * lo + 1 : 2 * lo;
 }
 
+// The same bucket through the lookup table T: splitters share their first f
+// bits; T[w] counts the splitters whose next TBL_BITS bits are below w, so a
+// key strictly between the first and last splitter (and hence sharing those
+// f bits) only needs a search among the splitters with its own window.
+__device__ __forceinline__ uint64_t window64(const Key &k, uint32_t f);
+
+__device__ __forceinline__ uint32_t window_bits(const Key &k, uint32_t f) {
+    return (uint32_t)(window64(k, f) >> (64 - TBL_BITS));
+}
+
+__device__ __forceinline__ uint32_t classify_tbl(const ulonglong2 *s, const uint16_t *T,
+                                                 uint32_t u, uint32_t f, const Key &key) {
+    const Key s0 = to_key(s[0]), sl = to_key(s[u - 1]);
+    if (key_lt(key, s0)) return 0;
+    if (key_eq(key, s0)) return 1;
+    if (key_lt(sl, key)) return 2 * u;
+    if (key_eq(key, sl)) return 2 * u - 1;
+    const uint32_t w = window_bits(key, f);
+    uint32_t lo = T[w], hi = T[w + 1];
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (key_lt(to_key(s[mid]), key))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return (lo < u && key_eq(to_key(s[lo]), key)) ? 2 * lo + 1 : 2 * lo;
+}
+
 // Padded shared-memory index: one spare slot per 8 keeps both the blocked
 // (stride 8) and the striped (stride 1) access patterns free of bank conflicts.
 __device__ __forceinline__ uint32_t pad(uint32_t e) { return e + (e >> 3); }
@@ -643,7 +672,8 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
 
 __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg *__restrict__ L,
                                                            ulonglong2 *spl, uint32_t *nspl,
-                                                           uint32_t *ntiles, uint32_t *cm_size) {
+                                                           uint16_t *tbl, uint32_t *ntiles,
+                                                           uint32_t *cm_size) {
     extern __shared__ ulonglong2 smp[];  // SAMPLES_MAX keys
     __shared__ uint32_t warp_cnt[SAMPLE_THREADS / 32 + 1];
     const Seg s = L[blockIdx.x];
@@ -699,12 +729,34 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
     __syncthreads();
     const uint32_t u = warp_cnt[SAMPLE_THREADS / 32];
     ulonglong2 *out = spl + (uint64_t)blockIdx.x * SPL_STRIDE;
-    if (keep) out[warp_cnt[w] + __popc(bal & lanemask_lt())] = from_key(cand);
+    if (keep) {
+        const uint32_t pos = warp_cnt[w] + __popc(bal & lanemask_lt());
+        out[pos] = from_key(cand);
+        smp[pos] = from_key(cand);  // candidates were read before the barrier
+    }
     const uint32_t kp2 = next_pow2(u + 1);
     for (uint32_t q = u + threadIdx.x; q + 1 < kp2; q += SAMPLE_THREADS)
         out[q] = from_key(key_max());
+    __syncthreads();
+    // Lookup table over the TBL_BITS bits after the splitters' common prefix.
+    const Key s0 = to_key(smp[0]), sl = to_key(smp[u - 1]);
+    const uint32_t f = u >= 2 ? clz128(s0.hi ^ sl.hi, s0.lo ^ sl.lo) : 128u;
+    if (f < 128) {
+        uint16_t *T = tbl + (uint64_t)blockIdx.x * TBL_STRIDE;
+        for (uint32_t wv = threadIdx.x; wv <= (uint32_t)TBL_N; wv += SAMPLE_THREADS) {
+            uint32_t lo = 0, hi = u;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (window_bits(to_key(smp[mid]), f) < wv)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            T[wv] = (uint16_t)lo;
+        }
+    }
     if (threadIdx.x == 0) {
-        nspl[blockIdx.x] = u;
+        nspl[blockIdx.x] = u | (f << 16);
         const uint32_t nt = (s.len + PART_TILE - 1) / PART_TILE;
         ntiles[blockIdx.x] = nt;
         cm_size[blockIdx.x] = (2 * u + 1) * nt;
@@ -714,24 +766,50 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
 // ---- partition count: per-tile bucket histograms ---------------------------
 // Each warp counts its own 512 consecutive keys into a private row, one
 // shared-memory update per distinct bucket per 32 keys (__match_any_sync).
+// Shared memory of the partition kernels.
+struct PartSmem {
+    ulonglong2 spl[SPL_STRIDE];              // the segment's splitters
+    uint16_t tbl[TBL_N + 8];                 // splitter lookup table
+    uint16_t cnt[PART_WARPS][NB_MAX + 1];    // per-warp bucket counters
+    uint32_t gbase[NB_MAX + 1];              // tile's global base per bucket
+};
+
+// Splitters (and the lookup table when f < 128) of segment si into smem.
+__device__ __forceinline__ void load_splitters(PartSmem &sm, const ulonglong2 *__restrict__ spl,
+                                               const uint16_t *__restrict__ tbl, uint32_t si,
+                                               uint32_t u, uint32_t f) {
+    for (uint32_t q = threadIdx.x; q < u; q += PART_THREADS)
+        sm.spl[q] = spl[(uint64_t)si * SPL_STRIDE + q];
+    if (f < 128) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(tbl + (uint64_t)si * TBL_STRIDE);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(sm.tbl);
+        for (uint32_t q = threadIdx.x; q < (TBL_N + 2) / 2; q += PART_THREADS) dst[q] = src[q];
+    }
+}
+
 __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg *__restrict__ L,
                                                         uint32_t nL,
                                                         const uint32_t *__restrict__ tile_base,
                                                         const ulonglong2 *__restrict__ spl,
                                                         const uint32_t *__restrict__ nspl,
+                                                        const uint16_t *__restrict__ tbl,
                                                         const uint32_t *__restrict__ cm_base,
                                                         uint32_t *cm) {
-    __shared__ ulonglong2 sspl[SPL_STRIDE];
-    __shared__ __align__(16) uint16_t hist[PART_WARPS][NB_MAX + 1];
+    extern __shared__ __align__(16) unsigned char part_smem[];
+    PartSmem &sm = *reinterpret_cast<PartSmem *>(part_smem);
+    auto &hist = sm.cnt;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr int SUB = PART_TILE / PART_WARPS;
     const uint32_t total_tiles = tile_base[nL];
+    uint32_t loaded = ~0u;
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
-        const uint32_t u = nspl[si], kp2 = next_pow2(u + 1), nb = 2 * u + 1;
-        for (uint32_t q = threadIdx.x; q + 1 < kp2; q += PART_THREADS)
-            sspl[q] = spl[(uint64_t)si * SPL_STRIDE + q];
+        const uint32_t u = nspl[si] & 0xFFFF, f = nspl[si] >> 16, nb = 2 * u + 1;
+        if (si != loaded) {
+            load_splitters(sm, spl, tbl, si, u, f);
+            loaded = si;
+        }
         {
             uint32_t *h32 = reinterpret_cast<uint32_t *>(&hist[0][0]);
             for (uint32_t q = threadIdx.x; q < PART_WARPS * (NB_MAX + 1) / 2; q += PART_THREADS)
@@ -751,7 +829,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
             const uint32_t e = lo + c * 32 + lane;
-            const uint32_t b = e < s.len ? classify(sspl, kp2, u, kk[c]) : nb;
+            const uint32_t b = e < s.len ? classify_tbl(sm.spl, sm.tbl, u, f, kk[c]) : nb;
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
             if ((peers & lanemask_lt()) == 0) hist[w][b] += (uint16_t)__popc(peers);
             __syncwarp();
@@ -773,23 +851,28 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_scatter(SortArgs a, const S
                                                           const uint32_t *__restrict__ tile_base,
                                                           const ulonglong2 *__restrict__ spl,
                                                           const uint32_t *__restrict__ nspl,
+                                                          const uint16_t *__restrict__ tbl,
                                                           const uint32_t *__restrict__ cm_base,
                                                           const uint32_t *__restrict__ cm_scan) {
-    __shared__ ulonglong2 sspl[SPL_STRIDE];
-    __shared__ __align__(16) uint16_t wcnt[PART_WARPS][NB_MAX + 1];
-    __shared__ uint32_t gbase[NB_MAX + 1];
+    extern __shared__ __align__(16) unsigned char part_smem[];
+    PartSmem &sm = *reinterpret_cast<PartSmem *>(part_smem);
+    auto &wcnt = sm.cnt;
+    uint32_t *gbase = sm.gbase;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr int SUB = PART_TILE / PART_WARPS;  // consecutive keys per warp
     const uint32_t total_tiles = tile_base[nL];
+    uint32_t loaded = ~0u;
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
-        const uint32_t u = nspl[si], kp2 = next_pow2(u + 1), nb = 2 * u + 1;
+        const uint32_t u = nspl[si] & 0xFFFF, f = nspl[si] >> 16, nb = 2 * u + 1;
         const uint32_t tl = t - tile_base[si];
         const uint32_t nt = tile_base[si + 1] - tile_base[si];
         const uint32_t lo = tl * PART_TILE + w * SUB;
-        for (uint32_t q = threadIdx.x; q + 1 < kp2; q += PART_THREADS)
-            sspl[q] = spl[(uint64_t)si * SPL_STRIDE + q];
+        if (si != loaded) {
+            load_splitters(sm, spl, tbl, si, u, f);
+            loaded = si;
+        }
         {
             uint32_t *w32 = reinterpret_cast<uint32_t *>(&wcnt[0][0]);
             for (uint32_t q = threadIdx.x; q < PART_WARPS * (NB_MAX + 1) / 2; q += PART_THREADS)
@@ -815,7 +898,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_scatter(SortArgs a, const S
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
             const uint32_t e = lo + c * 32 + lane;
-            const uint32_t b = e < s.len ? classify(sspl, kp2, u, kk[c]) : nb;
+            const uint32_t b = e < s.len ? classify_tbl(sm.spl, sm.tbl, u, f, kk[c]) : nb;
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
             const uint32_t r = __popc(peers & lt);
             const uint32_t base = wcnt[w][b];
@@ -861,7 +944,7 @@ __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__
                        Seg *E, uint2 *B, Seg *N, Counters *c) {
     const uint32_t si = blockIdx.x;
     const Seg s = L[si];
-    const uint32_t u = nspl[si], nb = 2 * u + 1;
+    const uint32_t u = nspl[si] & 0xFFFF, nb = 2 * u + 1;
     const uint32_t nt = tile_base[si + 1] - tile_base[si];
     const uint32_t cmb = cm_base[si];
     const uint32_t seg0 = cm_scan[cmb];
@@ -1443,7 +1526,7 @@ void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t 
 }
 
 void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl, uint32_t *nspl,
-                   uint32_t *ntiles, uint32_t *cm_size, cudaStream_t st) {
+                   uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size, cudaStream_t st) {
     if (!nL) return;
     static bool attr = false;
     const int smem = SAMPLES_MAX * sizeof(ulonglong2);
@@ -1451,21 +1534,35 @@ void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl
         cudaFuncSetAttribute(k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    k_sample<<<nL, SAMPLE_THREADS, smem, st>>>(a, L, spl, nspl, ntiles, cm_size);
+    k_sample<<<nL, SAMPLE_THREADS, smem, st>>>(a, L, spl, nspl, tbl, ntiles, cm_size);
 }
 
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                  const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
-                  uint32_t *cm, int grid, cudaStream_t st) {
+                  const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
+                  const uint32_t *cm_base, uint32_t *cm, int grid, cudaStream_t st) {
     if (!nL) return;
-    k_count<<<grid, PART_THREADS, 0, st>>>(a, L, nL, tile_base, spl, nspl, cm_base, cm);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(PartSmem));
+        attr = true;
+    }
+    k_count<<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl, tbl,
+                                                          cm_base, cm);
 }
 
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                    const ulonglong2 *spl, const uint32_t *nspl, const uint32_t *cm_base,
-                    const uint32_t *cm_scan, int grid, cudaStream_t st) {
+                    const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
+                    const uint32_t *cm_base, const uint32_t *cm_scan, int grid, cudaStream_t st) {
     if (!nL) return;
-    k_scatter<<<grid, PART_THREADS, 0, st>>>(a, L, nL, tile_base, spl, nspl, cm_base, cm_scan);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(PartSmem));
+        attr = true;
+    }
+    k_scatter<<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl, tbl,
+                                                            cm_base, cm_scan);
 }
 
 void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
