@@ -11,4 +11,4 @@
 #include "ssort_b200.h"
 
 ROUTINE_REGISTER_SINGLECORE(msd_gpu,
-	"B200 GPU MSD radix sort: 8-byte keys per round, sample partition + on-chip segment sorts")
+	"B200 GPU MSD radix sort: 16-byte keys per round, sample partition + on-chip segment sorts")
