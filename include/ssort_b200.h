@@ -75,6 +75,29 @@ int ssort_sort_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byt
                       const void *d_offs, int off_width, uint64_t n, uint32_t *d_perm,
                       uint32_t *d_lcp, void *stream);
 
+/*
+ * ssort_sort_device without any device allocation.  This entry point has no
+ * counterpart in the reference; it exists for callers that cannot let a
+ * library allocate device memory: cudaMalloc/cudaFree synchronise the device
+ * and can fail when the application has already budgeted all memory to its
+ * own pool.  All scratch lives in one fixed device array inside the library
+ * (SSORT_NOALLOC_MAX_N strings' worth, about 24 MB), which every GPU that
+ * loads the library holds until the process exits; larger n is rejected with
+ * SSORT_EINVAL.  The caller still passes the inputs and the perm (and
+ * optional lcp) outputs, and a cudaStream_t (NULL = the legacy default
+ * stream); the call returns when the results are complete.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * it should come before any stream capture.  Every call uses the same array
+ * and leaves its contents behind (what must start at zero is cleared by each
+ * call).  Calls that overlapped on the GPU would race on the array; the
+ * library prevents that within one process by taking a lock for the whole
+ * call and returning only after the call's GPU work has finished.
+ */
+#define SSORT_NOALLOC_MAX_N 262144u
+int ssort_sort_device_noalloc(const uint8_t *d_arena, uint64_t arena_bytes, const void *d_offs,
+                              int off_width, uint64_t n, uint32_t *d_perm, uint32_t *d_lcp,
+                              void *stream);
+
 /* The same from host buffers: copies arena and offsets to the device, sorts,
  * and copies perm (and lcp when not NULL) back.  Pinned host buffers make the
  * copies faster but are not required. */

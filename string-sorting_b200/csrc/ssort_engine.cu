@@ -62,9 +62,9 @@ struct ssort_ctx {
     cudaStream_t st = nullptr;
 
     // workspace
-    DBuf idx1, key0, key1, lcp, R, N, W1, W8, S, E, B, L, L2, spl, nspl, tbl, ntiles, cm_size,
-        tile_base, cm_base, tmp, cm, partials, ctr;
-    size_t cm_cap = 0;
+    DBuf ws_buf;    // one block holding every scratch buffer (ws_layout)
+    Workspace ws{};
+    size_t ws_n = 0;  // string capacity ws is laid out for
     DBuf arena, offs, perm;  // staging for the host-buffer entry points
     HBuf h_offs, h_arena, h_perm;
     Counters *h_ctr = nullptr;
@@ -152,17 +152,19 @@ struct ssort_ctx {
     }
 
     int sync_counters() {
-        SS_CUDA(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        SS_CUDA(cudaMemcpyAsync(h_ctr, ws.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
         SS_CUDA(cudaStreamSynchronize(st));
         return SSORT_OK;
     }
 
     int grid_for(int per_sm) const { return num_sms * per_sm; }
 
-    int reserve(uint32_t n, bool need_lcp);
+    int reserve(uint32_t n);
     int scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev);
     int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
             uint32_t n, uint32_t *d_perm, uint32_t *d_lcp);
+    int run_ws(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
+               uint32_t n, uint32_t *d_perm, uint32_t *d_lcp);
 };
 
 #define LAUNCH(ctx, name, call)                 \
@@ -173,36 +175,12 @@ struct ssort_ctx {
         SS_TRY((ctx)->check_launch(name));      \
     } while (0)
 
-int ssort_ctx::reserve(uint32_t n, bool need_internal_lcp) {
-    const size_t half = (size_t)n / 2 + 2;
-    const size_t nlarge = (size_t)n / (SMALL_CAP + 1) + 2;
-    SS_TRY(ensure(idx1, (size_t)n * 4));
-    SS_TRY(ensure(key0, (size_t)n * 16));
-    SS_TRY(ensure(key1, (size_t)n * 16));
-    if (need_internal_lcp) SS_TRY(ensure(lcp, (size_t)n * 4));
-    SS_TRY(ensure(R, half * sizeof(Seg)));
-    SS_TRY(ensure(N, half * sizeof(Seg)));
-    SS_TRY(ensure(W1, half * sizeof(Seg)));
-    SS_TRY(ensure(W8, (n / (WARP1_CAP + 1) + 2) * sizeof(Seg)));
-    SS_TRY(ensure(S, (n / (WARP8_CAP + 1) + 2) * sizeof(Seg)));
-    // equality work items: buckets of >= 2 strings, one item per EQ_TILE
-    SS_TRY(ensure(E, (half + (size_t)n / EQ_TILE + 2) * sizeof(Seg)));
-    SS_TRY(ensure(B, ((size_t)n + 2) * sizeof(uint2)));
-    SS_TRY(ensure(L, nlarge * sizeof(Seg)));
-    SS_TRY(ensure(L2, nlarge * sizeof(Seg)));
-    SS_TRY(ensure(spl, nlarge * SPL_STRIDE * sizeof(ulonglong2)));
-    SS_TRY(ensure(nspl, nlarge * 4));
-    SS_TRY(ensure(tbl, nlarge * TBL_STRIDE * sizeof(uint16_t)));
-    SS_TRY(ensure(ntiles, nlarge * 4));
-    SS_TRY(ensure(cm_size, nlarge * 4));
-    SS_TRY(ensure(cm_base, (nlarge + 1) * 4));
-    SS_TRY(ensure(tile_base, (nlarge + 1) * 4));
-    SS_TRY(ensure(tmp, (nlarge + 1) * 4));
-    // bucket-count matrix: at most NB_MAX buckets per tile of each segment
-    cm_cap = (size_t)NB_MAX * ((size_t)n / PART_TILE + nlarge + 1) + 1;
-    SS_TRY(ensure(cm, cm_cap * 4));
-    SS_TRY(ensure(partials, (size_t)scan_partials_needed((uint32_t)std::min<size_t>(cm_cap, 0xFFFFFFFFull)) * 4));
-    SS_TRY(ensure(ctr, sizeof(Counters)));
+int ssort_ctx::reserve(uint32_t n) {
+    if (ws_buf.p && n <= ws_n) return SSORT_OK;
+    const WsLayout lay = ws_layout(n);
+    SS_TRY(ensure(ws_buf, lay.total));
+    ws = ws_bind(lay, (unsigned char *)ws_buf.p);
+    ws_n = n;
     if (!h_ctr) {
         SS_CUDA(cudaHostAlloc((void **)&h_ctr, sizeof(Counters), cudaHostAllocDefault));
     }
@@ -210,7 +188,7 @@ int ssort_ctx::reserve(uint32_t n, bool need_internal_lcp) {
 }
 
 int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev) {
-    LAUNCH(this, "scan", launch_scan(in, out, n_host, n_dev, (uint32_t *)partials.p, st));
+    LAUNCH(this, "scan", launch_scan(in, out, n_host, n_dev, ws.partials, st));
     return SSORT_OK;
 }
 
@@ -222,7 +200,13 @@ int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const ui
 // next round's count) plus once per partition level.
 int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
                    int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp) {
-    SS_TRY(reserve(n, d_lcp == nullptr));
+    SS_TRY(reserve(n));
+    return run_ws(arena_p, arena_bytes, offs_p, off_width, n, d_perm, d_lcp);
+}
+
+// The round loop over an already laid-out workspace `ws`.
+int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
+                      int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp) {
     SortArgs a{};
     a.arena = arena_p;
     a.arena_bytes = arena_bytes;
@@ -230,13 +214,13 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
     a.off_width = off_width;
     a.n = n;
     a.idx[0] = d_perm;
-    a.idx[1] = (uint32_t *)idx1.p;
-    a.key[0] = (ulonglong2 *)key0.p;
-    a.key[1] = (ulonglong2 *)key1.p;
-    a.lcp = d_lcp ? d_lcp : (uint32_t *)lcp.p;
+    a.idx[1] = ws.idx1;
+    a.key[0] = ws.key0;
+    a.key[1] = ws.key1;
+    a.lcp = d_lcp ? d_lcp : ws.lcp;
 
-    Seg *cur = (Seg *)R.p, *nxt = (Seg *)N.p;
-    Counters *dc = (Counters *)ctr.p;
+    Seg *cur = ws.R, *nxt = ws.N;
+    Counters *dc = ws.ctr;
 
     LAUNCH(this, "iota", launch_iota(d_perm, n, st));
     SS_CUDA(cudaMemsetAsync(a.lcp, 0, 4, st));
@@ -251,20 +235,20 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
     while (n_cur) {
         SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
         LAUNCH(this, "classify",
-               launch_classify(cur, n_cur, (Seg *)W1.p, (Seg *)W8.p, (Seg *)S.p, (Seg *)L.p, dc,
+               launch_classify(cur, n_cur, ws.W1, ws.W8, ws.S, ws.L, dc,
                                st));
         SS_TRY(sync_counters());
         live = h_ctr->live_next;  // strings in this round's segments
         if (round < SSORT_MAX_ROUNDS) stats.live[round] = live;
         uint32_t n_large = h_ctr->n_large;
-        Seg *lcur = (Seg *)L.p, *lnext = (Seg *)L2.p;
+        Seg *lcur = ws.L, *lnext = ws.L2;
         if (n_large) {
             // Keys of the large segments at this depth.
             LAUNCH(this, "tile_counts",
-                   launch_tile_counts(lcur, n_large, GATHER_TILE, (uint32_t *)tmp.p, st));
-            SS_TRY(scan((uint32_t *)tmp.p, (uint32_t *)tile_base.p, n_large, nullptr));
+                   launch_tile_counts(lcur, n_large, GATHER_TILE, ws.tmp, st));
+            SS_TRY(scan(ws.tmp, ws.tile_base, n_large, nullptr));
             LAUNCH(this, "gather",
-                   launch_gather(a, lcur, n_large, (const uint32_t *)tile_base.p, g8, st));
+                   launch_gather(a, lcur, n_large, ws.tile_base, g8, st));
         }
         uint32_t levels_this_round = 0;
         while (n_large) {
@@ -275,38 +259,38 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
                 return fail(SSORT_EINTERNAL, "partition levels exceeded 4096");
             stats.partition_levels++;
             LAUNCH(this, "sample",
-                   launch_sample(a, lcur, n_large, (ulonglong2 *)spl.p, (uint32_t *)nspl.p,
-                                 (uint16_t *)tbl.p, (uint32_t *)ntiles.p, (uint32_t *)cm_size.p,
+                   launch_sample(a, lcur, n_large, ws.spl, ws.nspl,
+                                 ws.tbl, ws.ntiles, ws.cm_size,
                                  st));
-            SS_TRY(scan((const uint32_t *)ntiles.p, (uint32_t *)tile_base.p, n_large, nullptr));
-            SS_TRY(scan((const uint32_t *)cm_size.p, (uint32_t *)cm_base.p, n_large, nullptr));
+            SS_TRY(scan(ws.ntiles, ws.tile_base, n_large, nullptr));
+            SS_TRY(scan(ws.cm_size, ws.cm_base, n_large, nullptr));
             LAUNCH(this, "count",
-                   launch_count(a, lcur, n_large, (const uint32_t *)tile_base.p,
-                                (const ulonglong2 *)spl.p, (const uint32_t *)nspl.p,
-                                (const uint16_t *)tbl.p, (const uint32_t *)cm_base.p,
-                                (uint32_t *)cm.p, g2, st));
-            SS_TRY(scan((const uint32_t *)cm.p, (uint32_t *)cm.p, (uint32_t)(cm_cap - 1),
-                        (const uint32_t *)cm_base.p + n_large));
+                   launch_count(a, lcur, n_large, ws.tile_base,
+                                ws.spl, ws.nspl,
+                                ws.tbl, ws.cm_base,
+                                ws.cm, g2, st));
+            SS_TRY(scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
+                        ws.cm_base + n_large));
             LAUNCH(this, "scatter",
-                   launch_scatter(a, lcur, n_large, (const uint32_t *)tile_base.p,
-                                  (const ulonglong2 *)spl.p, (const uint32_t *)nspl.p,
-                                  (const uint16_t *)tbl.p, (const uint32_t *)cm_base.p,
-                                  (const uint32_t *)cm.p, g2, st));
+                   launch_scatter(a, lcur, n_large, ws.tile_base,
+                                  ws.spl, ws.nspl,
+                                  ws.tbl, ws.cm_base,
+                                  ws.cm, g2, st));
             LAUNCH(this, "emit",
-                   launch_emit(a, lcur, n_large, (const uint32_t *)tile_base.p,
-                               (const uint32_t *)nspl.p, (const uint32_t *)cm_base.p,
-                               (const uint32_t *)cm.p, (Seg *)W1.p, (Seg *)W8.p, (Seg *)S.p, lnext,
-                               (Seg *)E.p, (uint2 *)B.p, nxt, dc, st));
+                   launch_emit(a, lcur, n_large, ws.tile_base,
+                               ws.nspl, ws.cm_base,
+                               ws.cm, ws.W1, ws.W8, ws.S, lnext,
+                               ws.E, ws.B, nxt, dc, st));
             SS_TRY(sync_counters());
             n_large = h_ctr->n_large_next;
             SS_CUDA(cudaMemsetAsync(&dc->n_large_next, 0, 4, st));
             std::swap(lcur, lnext);
         }
-        LAUNCH(this, "warp1", launch_warp1(a, (Seg *)W1.p, nxt, dc, g8, st));
-        LAUNCH(this, "warp8", launch_warp8(a, (Seg *)W8.p, nxt, dc, g8, st));
-        LAUNCH(this, "block", launch_block(a, (Seg *)S.p, nxt, dc, g8, st));
-        LAUNCH(this, "equal", launch_equal(a, (Seg *)E.p, nxt, dc, g8, st));
-        LAUNCH(this, "boundary", launch_boundary(a, (uint2 *)B.p, dc, g4, st));
+        LAUNCH(this, "warp1", launch_warp1(a, ws.W1, nxt, dc, g8, st));
+        LAUNCH(this, "warp8", launch_warp8(a, ws.W8, nxt, dc, g8, st));
+        LAUNCH(this, "block", launch_block(a, ws.S, nxt, dc, g8, st));
+        LAUNCH(this, "equal", launch_equal(a, ws.E, nxt, dc, g8, st));
+        LAUNCH(this, "boundary", launch_boundary(a, ws.B, dc, g4, st));
         SS_TRY(sync_counters());
         stats.small_segments += h_ctr->n_w1 + h_ctr->n_w8 + h_ctr->n_small;
         stats.partitioned += h_ctr->partitioned;
@@ -358,10 +342,7 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
     ctx->stats.device_ms = ms;
     if (ctx->prof) ctx->prof_collect();
     size_t held = 0;
-    for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->W1,
-                    &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl, &ctx->tbl,
-                    &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
-                    &ctx->cm, &ctx->partials, &ctx->arena, &ctx->offs, &ctx->perm})
+    for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm})
         held += b->cap;
     ctx->stats.device_bytes = held;
     return SSORT_OK;
@@ -452,11 +433,7 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
     if (!ctx) return;
     with_device(ctx, [&]() -> int {
         if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
-        for (DBuf *b : {&ctx->idx1, &ctx->key0, &ctx->key1, &ctx->lcp, &ctx->R, &ctx->N, &ctx->W1,
-                        &ctx->W8, &ctx->S, &ctx->E, &ctx->B, &ctx->L, &ctx->L2, &ctx->spl, &ctx->nspl, &ctx->tbl,
-                        &ctx->ntiles, &ctx->cm_size, &ctx->tile_base, &ctx->cm_base, &ctx->tmp,
-                        &ctx->cm, &ctx->partials, &ctx->ctr, &ctx->arena, &ctx->offs,
-                        &ctx->perm})
+        for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm})
             if (b->p) cudaFree(b->p);
         for (HBuf *b : {&ctx->h_offs, &ctx->h_arena, &ctx->h_perm})
             if (b->p) cudaFreeHost(b->p);
@@ -662,3 +639,74 @@ void msd_gpu(unsigned char **strings, size_t n) {
 }
 
 }  // extern "C"
+
+// ---- sort without device allocation ----------------------------------------
+// Some callers cannot let a library call cudaMalloc/cudaFree: cudaFree waits
+// for the whole device, allocation can fail or fragment memory that the
+// application budgets itself (a server that reserves its device memory up
+// front for its own pool, a latency-critical loop that must not block on a
+// device-wide synchronisation).  For them the sort's scratch lives in one
+// file-scope device array of fixed size, loaded with the library on every
+// device that uses it and kept until the process exits.
+namespace {
+
+constexpr uint32_t NOALLOC_MAX_N = SSORT_NOALLOC_MAX_N;
+constexpr size_t NOALLOC_SCRATCH_BYTES = ws_layout(NOALLOC_MAX_N).total;
+
+// Host code may only name this array to look up its device address; the
+// symbol itself is a host-side stand-in, not a device pointer.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+struct NoallocDevice {
+    bool ready = false;
+    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch
+    int num_sms = 0;
+    Counters host_ctr{};               // plain host copy of the round counters
+};
+
+std::mutex g_noalloc_mu;
+NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+
+}  // namespace
+
+extern "C" int ssort_sort_device_noalloc(const uint8_t *d_arena, uint64_t arena_bytes,
+                                         const void *d_offs, int off_width, uint64_t n,
+                                         uint32_t *d_perm, uint32_t *d_lcp, void *stream) {
+    if (off_width != 4 && off_width != 8) return fail(SSORT_EINVAL, "off_width must be 4 or 8");
+    if (n > NOALLOC_MAX_N)
+        return fail(SSORT_EINVAL, "n = " + std::to_string(n) +
+                                      " exceeds the fixed scratch of ssort_sort_device_noalloc (" +
+                                      std::to_string(NOALLOC_MAX_N) + " strings)");
+    if (n == 0) return SSORT_OK;
+    if (!d_arena || !d_offs || !d_perm) return fail(SSORT_EINVAL, "null device buffer");
+    if (((uintptr_t)d_arena & 15) != 0)
+        return fail(SSORT_EINVAL, "arena must be 16-byte aligned");
+    int dev = -1;
+    SS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(SSORT_EINVAL, "device index too large");
+    // One sort at a time per process: every call shares the scratch array.
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoallocDevice &d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        // First call on this device (with it current): resolve the array's
+        // device address.
+        void *p = nullptr;
+        SS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        SS_CUDA(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev));
+        d.scratch = (unsigned char *)p;
+        d.ready = true;
+    }
+    ssort_ctx c;
+    c.device = dev;
+    c.num_sms = d.num_sms;
+    c.st = (cudaStream_t)stream;
+    c.h_ctr = &d.host_ctr;
+    c.ws = ws_bind(ws_layout(NOALLOC_MAX_N), d.scratch);
+    c.ws_n = NOALLOC_MAX_N;
+    const int rc = c.run_ws(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, d_perm, d_lcp);
+    if (rc == SSORT_OK) SS_CUDA(cudaStreamSynchronize(c.st));
+    c.h_ctr = nullptr;
+    return rc;
+}

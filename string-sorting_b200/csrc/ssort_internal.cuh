@@ -91,6 +91,102 @@ struct SortArgs {
     uint32_t *lcp;
 };
 
+// ---- device workspace ---------------------------------------------------------
+// Every scratch buffer of one sort of up to n strings, carved from one block
+// of device memory by ws_layout (offsets, 256-byte aligned).
+constexpr uint32_t SCAN_CHUNK_ELEMS = 4096;  // keys per block in the scan kernels
+
+constexpr uint32_t scan_partials_for(uint64_t n) {
+    return (uint32_t)((n ? n : 1) + SCAN_CHUNK_ELEMS - 1) / SCAN_CHUNK_ELEMS + 1;
+}
+
+struct WsLayout {
+    size_t idx1, key0, key1, lcp, R, N, W1, W8, S, E, B, L, L2, spl, nspl, tbl, ntiles,
+        cm_size, cm_base, tile_base, tmp, cm, partials, ctr;
+    size_t cm_cap, total;
+};
+
+constexpr WsLayout ws_layout(uint64_t n) {
+    WsLayout o{};
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+        const size_t at = off;
+        off += (bytes + 255) & ~size_t(255);
+        return at;
+    };
+    const size_t half = n / 2 + 2;
+    const size_t nlarge = n / (SMALL_CAP + 1) + 2;
+    o.idx1 = take(n * 4);
+    o.key0 = take(n * 16);
+    o.key1 = take(n * 16);
+    o.lcp = take(n * 4);
+    o.R = take(half * sizeof(Seg));
+    o.N = take(half * sizeof(Seg));
+    o.W1 = take(half * sizeof(Seg));
+    o.W8 = take((n / (WARP1_CAP + 1) + 2) * sizeof(Seg));
+    o.S = take((n / (WARP8_CAP + 1) + 2) * sizeof(Seg));
+    // equality work items: buckets of >= 2 strings, one item per EQ_TILE
+    o.E = take((half + n / EQ_TILE + 2) * sizeof(Seg));
+    o.B = take((n + 2) * 8);
+    o.L = take(nlarge * sizeof(Seg));
+    o.L2 = take(nlarge * sizeof(Seg));
+    o.spl = take(nlarge * SPL_STRIDE * 16);
+    o.nspl = take(nlarge * 4);
+    o.tbl = take(nlarge * TBL_STRIDE * 2);
+    o.ntiles = take(nlarge * 4);
+    o.cm_size = take(nlarge * 4);
+    o.cm_base = take((nlarge + 1) * 4);
+    o.tile_base = take((nlarge + 1) * 4);
+    o.tmp = take((nlarge + 1) * 4);
+    // bucket-count matrix: at most NB_MAX buckets per tile of each segment
+    o.cm_cap = (size_t)NB_MAX * (n / PART_TILE + nlarge + 1) + 1;
+    o.cm = take(o.cm_cap * 4);
+    o.partials = take((size_t)scan_partials_for(o.cm_cap) * 4);
+    o.ctr = take(sizeof(Counters));
+    o.total = off;
+    return o;
+}
+
+struct Workspace {
+    uint32_t *idx1, *lcp, *nspl, *ntiles, *cm_size, *cm_base, *tile_base, *tmp, *cm, *partials;
+    ulonglong2 *key0, *key1, *spl;
+    Seg *R, *N, *W1, *W8, *S, *E, *L, *L2;
+    uint2 *B;
+    uint16_t *tbl;
+    Counters *ctr;
+    size_t cm_cap;
+};
+
+inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
+    Workspace w;
+    w.idx1 = (uint32_t *)(base + o.idx1);
+    w.key0 = (ulonglong2 *)(base + o.key0);
+    w.key1 = (ulonglong2 *)(base + o.key1);
+    w.lcp = (uint32_t *)(base + o.lcp);
+    w.R = (Seg *)(base + o.R);
+    w.N = (Seg *)(base + o.N);
+    w.W1 = (Seg *)(base + o.W1);
+    w.W8 = (Seg *)(base + o.W8);
+    w.S = (Seg *)(base + o.S);
+    w.E = (Seg *)(base + o.E);
+    w.B = (uint2 *)(base + o.B);
+    w.L = (Seg *)(base + o.L);
+    w.L2 = (Seg *)(base + o.L2);
+    w.spl = (ulonglong2 *)(base + o.spl);
+    w.nspl = (uint32_t *)(base + o.nspl);
+    w.tbl = (uint16_t *)(base + o.tbl);
+    w.ntiles = (uint32_t *)(base + o.ntiles);
+    w.cm_size = (uint32_t *)(base + o.cm_size);
+    w.cm_base = (uint32_t *)(base + o.cm_base);
+    w.tile_base = (uint32_t *)(base + o.tile_base);
+    w.tmp = (uint32_t *)(base + o.tmp);
+    w.cm = (uint32_t *)(base + o.cm);
+    w.partials = (uint32_t *)(base + o.partials);
+    w.ctr = (Counters *)(base + o.ctr);
+    w.cm_cap = o.cm_cap;
+    return w;
+}
+
 // ---- launchers (ssort_kernels.cu) ----------------------------------------
 void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st);
 void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L, Counters *c,

@@ -21,7 +21,7 @@ SSORT_MAX_ROUNDS = 64
 EXPORTS = (
     "msd_gpu", "ssort_strerror", "ssort_last_error", "ssort_ctx_create", "ssort_ctx_destroy",
     "ssort_sort_device", "ssort_sort_host", "ssort_sort_strings", "ssort_get_stats",
-    "ssort_set_profiling", "ssort_get_kernel_times",
+    "ssort_set_profiling", "ssort_get_kernel_times", "ssort_sort_device_noalloc",
 )
 
 
@@ -80,6 +80,7 @@ def lib():
         L.ssort_ctx_destroy.argtypes = [vp]
         L.ssort_ctx_destroy.restype = None
         L.ssort_sort_device.argtypes = [vp, vp, u64, vp, i32, u64, vp, vp, vp]
+        L.ssort_sort_device_noalloc.argtypes = [vp, u64, vp, i32, u64, vp, vp, vp]
         L.ssort_sort_host.argtypes = [vp, vp, u64, vp, i32, u64, vp, vp]
         L.ssort_sort_strings.argtypes = [vp, vp, ctypes.c_size_t, vp]
         L.ssort_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
