@@ -142,6 +142,23 @@ class Clocks:
 # ---- algorithmic bytes -----------------------------------------------------------
 KB = 16  # key bytes per round
 
+# DRAM bytes (read + write) per string handled, from one ncu capture of a small
+# case of the same kernel (profiles/*.md); scaled by the strings a launch
+# handles to give `roofline.traffic` per launch.
+TRAFFIC_PER_STRING = {
+    "count": 16.8,    # profiles/count_scatter_zipf_words_10m.md
+    "scatter": 48.8,  # profiles/count_scatter_zipf_words_10m.md
+}
+
+
+def kernel_strings(st):
+    """Strings each kernel handled during one sort (stats counters)."""
+    return {
+        "gather": st.gather_elems, "count": st.partitioned, "scatter": st.partitioned,
+        "warp1": st.warp1_fresh + st.warp1_keyed, "warp8": st.warp8_fresh + st.warp8_keyed,
+        "block": st.block_fresh + st.block_keyed,
+    }
+
 
 def kernel_bytes(st, w):
     """Algorithmic bytes each kernel must move for one sort, from the per-kernel
@@ -286,9 +303,13 @@ def run_ours(args, rank, world, local_rank, dist):
         per_launch_bytes = kb[dom] * args.steps / d["launches"]
         per_launch_s = d["ms_total"] / 1e3 / d["launches"]
         ach = per_launch_bytes / per_launch_s / 1e9
+        traffic = None
+        if dom in TRAFFIC_PER_STRING:
+            strings_per_launch = kernel_strings(st)[dom] * args.steps / d["launches"]
+            traffic = int(TRAFFIC_PER_STRING[dom] * strings_per_launch)
         roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
-                    "traffic": None, "algorithmic_bytes_per_launch": int(per_launch_bytes),
+                    "traffic": traffic, "algorithmic_bytes_per_launch": int(per_launch_bytes),
                     "launch_ms": round(per_launch_s * 1e3, 4)}
     live8 = intrinsic_live(d_lcp.cpu().numpy().view(np.uint32), n)
     sort_bytes = sort_algorithmic_bytes(live8, n, w)
