@@ -218,6 +218,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.key[0] = ws.key0;
     a.key[1] = ws.key1;
     a.lcp = d_lcp ? d_lcp : ws.lcp;
+    a.bkt = ws.bkt;
 
     Seg *cur = ws.R, *nxt = ws.N;
     Counters *dc = ws.ctr;

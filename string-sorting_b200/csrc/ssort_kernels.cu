@@ -447,10 +447,21 @@ __device__ __forceinline__ uint32_t merge_split(const ulonglong2 *sk, const uint
 // layout), write its indices, LCPs and first/last keys, and emit the runs of
 // equal non-final keys as next-round segments.  Called by `threads` threads
 // numbered t = 0..threads-1.
+// Sorted position e -> shared-memory slot of its record: the slot itself
+// (records already in order) or the position field of the e-th packed key.
+template <bool IND>
+__device__ __forceinline__ uint32_t rec_slot(const uint64_t *sv, uint32_t e) {
+    if constexpr (IND)
+        return pad((uint32_t)(sv[pad(e)] & POS_MASK));
+    else
+        return pad(e);
+}
+
+template <bool IND>
 __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
                                                const ulonglong2 *sk, const uint32_t *sx,
-                                               uint32_t t, uint32_t threads, Seg *N,
-                                               Counters *c) {
+                                               const uint64_t *sv, uint32_t t, uint32_t threads,
+                                               Seg *N, Counters *c) {
     // Uniform trip count so that every warp reaches the collective append.
     for (uint32_t e0 = 0; e0 < s.len; e0 += threads) {
         const uint32_t e = e0 + t;
@@ -458,12 +469,13 @@ __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
         uint32_t run_lo = 0;
         if (e < s.len) {
             const uint32_t p = s.start + e;
-            const Key k = to_key(sk[pad(e)]);
-            a.idx[0][p] = sx[pad(e)];
+            const uint32_t q = rec_slot<IND>(sv, e);
+            const Key k = to_key(sk[q]);
+            a.idx[0][p] = sx[q];
             if (e == 0 || e == s.len - 1) a.key[0][p] = from_key(k);
             bool same_prev = false;
             if (e > 0) {
-                const Key kp = to_key(sk[pad(e - 1)]);
+                const Key kp = to_key(sk[rec_slot<IND>(sv, e - 1)]);
                 same_prev = key_eq(kp, k);
                 if (!same_prev)
                     a.lcp[p] = s.depth + key_lcp(kp, k);
@@ -471,11 +483,11 @@ __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
                     a.lcp[p] = s.depth + key_len(k);
             }
             if (same_prev && !key_is_end(k) &&
-                (e == s.len - 1 || !key_eq(to_key(sk[pad(e + 1)]), k))) {
+                (e == s.len - 1 || !key_eq(to_key(sk[rec_slot<IND>(sv, e + 1)]), k))) {
                 uint32_t lo = 0, hi = e;  // first position of this run
                 while (lo < hi) {
                     const uint32_t mid = (lo + hi) >> 1;
-                    if (key_lt(to_key(sk[pad(mid)]), k))
+                    if (key_lt(to_key(sk[rec_slot<IND>(sv, mid)]), k))
                         lo = mid + 1;
                     else
                         hi = mid;
@@ -486,6 +498,40 @@ __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
         }
         emit_next_warp(N, c, want, s.start + run_lo, e - run_lo + 1, s.depth + KEY_BYTES);
     }
+}
+
+// True when the sorted order (through the packed keys) agrees with full
+// (key, index) order wherever the packed keys could not tell records apart
+// (equal windows).  Called by `threads` threads numbered t; per-thread verdict.
+__device__ __forceinline__ bool window_pairs_ok_ind(const ulonglong2 *sk, const uint64_t *sv,
+                                                    uint32_t len, uint32_t t, uint32_t threads) {
+    bool ok = true;
+    for (uint32_t e = t + 1; e < len; e += threads) {
+        const uint64_t va = sv[pad(e - 1)], vb = sv[pad(e)];
+        if ((va >> POS_BITS) == (vb >> POS_BITS)) {
+            const Key kp = to_key(sk[pad((uint32_t)(va & POS_MASK))]);
+            const Key k = to_key(sk[pad((uint32_t)(vb & POS_MASK))]);
+            if (key_lt(k, kp)) ok = false;
+        }
+    }
+    return ok;
+}
+
+// One warp: packed keys of the records at slots base .. base + 32*ITEMS - 1
+// (positions >= len pad with all-ones), sorted, stored to sv.
+template <int ITEMS>
+__device__ __forceinline__ void warp_run_packed(const ulonglong2 *sk, uint64_t *sv,
+                                                uint32_t base, uint32_t len, uint32_t f,
+                                                uint32_t lane) {
+    uint64_t v[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t e = base + lane * ITEMS + i;
+        v[i] = e < len ? sort_key(to_key(sk[pad(e)]), f, e) : ~0ull;
+    }
+    warp_bitonic64<ITEMS>(v, lane);
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) sv[pad(base + lane * ITEMS + i)] = v[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -830,6 +876,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
         for (int c = 0; c < PART_ITEMS; ++c) {
             const uint32_t e = lo + c * 32 + lane;
             const uint32_t b = e < s.len ? classify_tbl(sm.spl, sm.tbl, u, f, kk[c]) : nb;
+            if (e < s.len) a.bkt[s.start + e] = (uint16_t)b;
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
             if ((peers & lanemask_lt()) == 0) hist[w][b] += (uint16_t)__popc(peers);
             __syncwarp();
@@ -865,14 +912,10 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_scatter(SortArgs a, const S
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
-        const uint32_t u = nspl[si] & 0xFFFF, f = nspl[si] >> 16, nb = 2 * u + 1;
+        const uint32_t u = nspl[si] & 0xFFFF, nb = 2 * u + 1;
         const uint32_t tl = t - tile_base[si];
         const uint32_t nt = tile_base[si + 1] - tile_base[si];
         const uint32_t lo = tl * PART_TILE + w * SUB;
-        if (si != loaded) {
-            load_splitters(sm, spl, tbl, si, u, f);
-            loaded = si;
-        }
         {
             uint32_t *w32 = reinterpret_cast<uint32_t *>(&wcnt[0][0]);
             for (uint32_t q = threadIdx.x; q < PART_WARPS * (NB_MAX + 1) / 2; q += PART_THREADS)
@@ -883,22 +926,24 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_scatter(SortArgs a, const S
         const uint32_t *Iin = a.idxb(ib) + s.start;
         ulonglong2 *Kout = a.keyb(ib ^ 1) + s.start;
         uint32_t *Iout = a.idxb(ib ^ 1) + s.start;
+        const uint16_t *Bin = a.bkt + s.start;  // buckets found by k_count
         Key kk[PART_ITEMS];
         uint32_t ii[PART_ITEMS];
         uint32_t br[PART_ITEMS];
+        uint32_t bb[PART_ITEMS];
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
             const uint32_t e = lo + c * 32 + lane;
             const bool v = e < s.len;
             kk[c] = v ? to_key(Kin[e]) : key_max();
             ii[c] = v ? Iin[e] : 0;
+            bb[c] = v ? Bin[e] : nb;
         }
         __syncthreads();
         const uint32_t lt = lanemask_lt();
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t e = lo + c * 32 + lane;
-            const uint32_t b = e < s.len ? classify_tbl(sm.spl, sm.tbl, u, f, kk[c]) : nb;
+            const uint32_t b = bb[c];
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
             const uint32_t r = __popc(peers & lt);
             const uint32_t base = wcnt[w][b];
@@ -1123,21 +1168,6 @@ __global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *_
     }
 }
 
-// True when the records at padded positions 0..len-1 are in (key, index)
-// order wherever the packed keys could not tell them apart (equal windows).
-// Called by `threads` threads numbered t; returns a per-thread verdict that
-// the caller combines.
-__device__ __forceinline__ bool window_pairs_ok(const ulonglong2 *sk, uint32_t len, uint32_t f,
-                                                uint32_t t, uint32_t threads) {
-    bool ok = true;
-    for (uint32_t e = t + 1; e < len; e += threads) {
-        const Key kp = to_key(sk[pad(e - 1)]), k = to_key(sk[pad(e)]);
-        if ((window64(kp, f) >> POS_BITS) == (window64(k, f) >> POS_BITS) && key_lt(k, kp))
-            ok = false;
-    }
-    return ok;
-}
-
 // Warp-wide OR of key ^ key0 over the records at padded positions 0..len-1.
 __device__ __forceinline__ uint32_t warp_diff_bit(const ulonglong2 *sk, uint32_t len,
                                                   uint32_t lane) {
@@ -1156,53 +1186,23 @@ __device__ __forceinline__ uint32_t warp_diff_bit(const ulonglong2 *sk, uint32_t
     return (dh | dl) ? clz128(dh, dl) : 128u;
 }
 
-// One warp sorts the len (<= 32 * ITEMS) records at padded positions
-// 0..len-1 of sk/sx by packed keys; returns false if the window check fails.
-template <int ITEMS>
-__device__ __forceinline__ bool warp_sort_packed(ulonglong2 *sk, uint32_t *sx, uint32_t len,
-                                                 uint32_t f, uint32_t lane) {
-    uint64_t v[ITEMS];
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        const uint32_t e = lane * ITEMS + i;
-        v[i] = e < len ? sort_key(to_key(sk[pad(e)]), f, e) : ~0ull;
-    }
-    warp_bitonic64<ITEMS>(v, lane);
-    Key k[ITEMS];
-    uint32_t x[ITEMS];
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        const uint32_t e = lane * ITEMS + i;
-        if (e < len) {
-            const uint32_t src = (uint32_t)(v[i] & POS_MASK);
-            k[i] = to_key(sk[pad(src)]);
-            x[i] = sx[pad(src)];
-        }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        const uint32_t e = lane * ITEMS + i;
-        if (e < len) {
-            sk[pad(e)] = from_key(k[i]);
-            sx[pad(e)] = x[i];
-        }
-    }
-    __syncwarp();
-    return __all_sync(0xffffffffu, window_pairs_ok(sk, len, f, lane, 32));
-}
-
 // ---- segments of 33..256 strings: one warp, 2/4/8 strings per lane ----------
 constexpr int W8_PAD = WARP8_CAP + WARP8_CAP / 8;
+constexpr int W8_WARPS = WARP_THREADS / 32;
+constexpr size_t W8_SMEM = (size_t)W8_WARPS * W8_PAD * (sizeof(ulonglong2) + sizeof(uint64_t) +
+                                                         sizeof(uint32_t));
 
-__global__ void __launch_bounds__(WARP_THREADS, 2) k_warp8(SortArgs a, const Seg *__restrict__ T,
+__global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg *__restrict__ T,
                                                            Seg *N, Counters *c) {
-    __shared__ ulonglong2 sk_all[WARP_THREADS / 32][W8_PAD];
-    __shared__ uint32_t sx_all[WARP_THREADS / 32][W8_PAD];
+    extern __shared__ __align__(16) unsigned char w8_smem[];
     const uint32_t nT = c->n_w8;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    ulonglong2 *sk = sk_all[w];
-    uint32_t *sx = sx_all[w];
+    ulonglong2 *sk = reinterpret_cast<ulonglong2 *>(w8_smem) + w * W8_PAD;
+    uint64_t *sv = reinterpret_cast<uint64_t *>(reinterpret_cast<ulonglong2 *>(w8_smem) +
+                                                W8_WARPS * W8_PAD) + w * W8_PAD;
+    uint32_t *sx = reinterpret_cast<uint32_t *>(reinterpret_cast<uint64_t *>(
+                       reinterpret_cast<ulonglong2 *>(w8_smem) + W8_WARPS * W8_PAD) +
+                                                W8_WARPS * W8_PAD) + w * W8_PAD;
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long fresh = 0, keyed = 0;
@@ -1222,15 +1222,17 @@ __global__ void __launch_bounds__(WARP_THREADS, 2) k_warp8(SortArgs a, const Seg
         }
         __syncwarp();
         const uint32_t f = warp_diff_bit(sk, s.len, lane);
+        bool packed = false;
         if (f < 128) {
-            bool ok;
             if (P <= 64)
-                ok = warp_sort_packed<2>(sk, sx, s.len, f, lane);
+                warp_run_packed<2>(sk, sv, 0, s.len, f, lane);
             else if (P <= 128)
-                ok = warp_sort_packed<4>(sk, sx, s.len, f, lane);
+                warp_run_packed<4>(sk, sv, 0, s.len, f, lane);
             else
-                ok = warp_sort_packed<8>(sk, sx, s.len, f, lane);
-            if (!ok) {
+                warp_run_packed<8>(sk, sv, 0, s.len, f, lane);
+            __syncwarp();
+            packed = __all_sync(0xffffffffu, window_pairs_ok_ind(sk, sv, s.len, lane, 32));
+            if (!packed) {
                 if (P <= 64)
                     warp_sort_run<2>(sk, sx, 0, lane);
                 else if (P <= 128)
@@ -1240,7 +1242,10 @@ __global__ void __launch_bounds__(WARP_THREADS, 2) k_warp8(SortArgs a, const Seg
             }
         }
         __syncwarp();
-        finish_segment(a, s, sk, sx, lane, 32, N, c);
+        if (packed)
+            finish_segment<true>(a, s, sk, sx, sv, lane, 32, N, c);
+        else
+            finish_segment<false>(a, s, sk, sx, sv, lane, 32, N, c);
         __syncwarp();
     }
     if (lane == 0 && (fresh | keyed)) {
@@ -1311,14 +1316,14 @@ __device__ __noinline__ void block_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
     }
 }
 
-__global__ void __launch_bounds__(SMALL_THREADS, 2) k_block(SortArgs a, const Seg *__restrict__ S,
+__global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
                                                             Seg *N, Counters *c) {
     extern __shared__ __align__(16) unsigned char block_smem[];
     ulonglong2 *sk = reinterpret_cast<ulonglong2 *>(block_smem);
     uint64_t *sv = reinterpret_cast<uint64_t *>(sk + SMALL_PAD);
     uint32_t *sx = reinterpret_cast<uint32_t *>(sv + SMALL_PAD);
     __shared__ uint64_t red[2][SMALL_THREADS / 32];
-    constexpr uint32_t RUN = 32 * SMALL_ITEMS;
+    constexpr uint32_t FULL_RUN = 32 * SMALL_ITEMS;
     const uint32_t nS = c->n_small;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     unsigned long long fresh = 0, keyed = 0;
@@ -1328,9 +1333,14 @@ __global__ void __launch_bounds__(SMALL_THREADS, 2) k_block(SortArgs a, const Se
             keyed += s.len;
         else
             fresh += s.len;
-        const uint32_t nruns = (s.len + RUN - 1) / RUN;
-        const uint32_t span = nruns * RUN;
-        for (uint32_t e = threadIdx.x; e < span; e += SMALL_THREADS) {
+        // Runs of 64/128/256 packed keys so that most of the 8 warps get one.
+        const uint32_t per = (s.len + SMALL_THREADS - 1) / SMALL_THREADS;  // 2..8
+        const uint32_t items = per <= 2 ? 2u : (per <= 4 ? 4u : 8u);
+        const uint32_t run0 = 32 * items;
+        const uint32_t nruns = (s.len + run0 - 1) / run0;
+        const uint32_t span = nruns * run0;
+        const uint32_t full_span = (s.len + FULL_RUN - 1) / FULL_RUN * FULL_RUN;
+        for (uint32_t e = threadIdx.x; e < full_span; e += SMALL_THREADS) {
             Key k = key_max();
             uint32_t id = IDX_MAX;
             if (e < s.len) load_elem(a, s, e, k, id);
@@ -1364,23 +1374,19 @@ __global__ void __launch_bounds__(SMALL_THREADS, 2) k_block(SortArgs a, const Se
             dh |= red[0][q];
             dl |= red[1][q];
         }
+        bool packed = false;
         if (dh | dl) {
             const uint32_t f = clz128(dh, dl);
-            // Packed keys: warp runs of RUN, then merges, all on uint64.
             if (w < nruns) {
-                uint64_t v[SMALL_ITEMS];
-#pragma unroll
-                for (int i = 0; i < SMALL_ITEMS; ++i) {
-                    const uint32_t e = w * RUN + lane * SMALL_ITEMS + i;
-                    v[i] = e < s.len ? sort_key(to_key(sk[pad(e)]), f, e) : ~0ull;
-                }
-                warp_bitonic64<SMALL_ITEMS>(v, lane);
-#pragma unroll
-                for (int i = 0; i < SMALL_ITEMS; ++i)
-                    sv[pad(w * RUN + lane * SMALL_ITEMS + i)] = v[i];
+                if (items == 2)
+                    warp_run_packed<2>(sk, sv, w * run0, s.len, f, lane);
+                else if (items == 4)
+                    warp_run_packed<4>(sk, sv, w * run0, s.len, f, lane);
+                else
+                    warp_run_packed<8>(sk, sv, w * run0, s.len, f, lane);
             }
             __syncthreads();
-            for (uint32_t run = RUN; run < span; run <<= 1) {
+            for (uint32_t run = run0; run < span; run <<= 1) {
                 const uint32_t o = threadIdx.x * SMALL_ITEMS;
                 uint64_t ov[SMALL_ITEMS];
                 const bool active = o < span;
@@ -1409,34 +1415,15 @@ __global__ void __launch_bounds__(SMALL_THREADS, 2) k_block(SortArgs a, const Se
                 }
                 __syncthreads();
             }
-            // Move every record to its rank (through registers: in place).
-            Key k[SMALL_ITEMS];
-            uint32_t x[SMALL_ITEMS];
-#pragma unroll
-            for (int i = 0; i < SMALL_ITEMS; ++i) {
-                const uint32_t e = threadIdx.x + i * SMALL_THREADS;
-                if (e < s.len) {
-                    const uint32_t src = (uint32_t)(sv[pad(e)] & POS_MASK);
-                    k[i] = to_key(sk[pad(src)]);
-                    x[i] = sx[pad(src)];
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int i = 0; i < SMALL_ITEMS; ++i) {
-                const uint32_t e = threadIdx.x + i * SMALL_THREADS;
-                if (e < s.len) {
-                    sk[pad(e)] = from_key(k[i]);
-                    sx[pad(e)] = x[i];
-                }
-            }
-            __syncthreads();
-            const bool ok =
-                __syncthreads_and(window_pairs_ok(sk, s.len, f, threadIdx.x, SMALL_THREADS));
-            if (!ok) block_sort_full(sk, sx, span);
+            packed = __syncthreads_and(window_pairs_ok_ind(sk, sv, s.len, threadIdx.x,
+                                                           SMALL_THREADS));
+            if (!packed) block_sort_full(sk, sx, full_span);
         }
         __syncthreads();
-        finish_segment(a, s, sk, sx, threadIdx.x, SMALL_THREADS, N, c);
+        if (packed)
+            finish_segment<true>(a, s, sk, sx, sv, threadIdx.x, SMALL_THREADS, N, c);
+        else
+            finish_segment<false>(a, s, sk, sx, sv, threadIdx.x, SMALL_THREADS, N, c);
         __syncthreads();
     }
     if (threadIdx.x == 0 && (fresh | keyed)) {
@@ -1581,7 +1568,12 @@ void launch_warp1(const SortArgs &a, const Seg *W1, Seg *N, Counters *c, int gri
 
 void launch_warp8(const SortArgs &a, const Seg *W8, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
-    k_warp8<<<grid, WARP_THREADS, 0, st>>>(a, W8, N, c);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_warp8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W8_SMEM);
+        attr = true;
+    }
+    k_warp8<<<grid, WARP_THREADS, W8_SMEM, st>>>(a, W8, N, c);
 }
 
 void launch_block(const SortArgs &a, const Seg *S, Seg *N, Counters *c, int grid,
