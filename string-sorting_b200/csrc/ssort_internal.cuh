@@ -89,7 +89,7 @@ struct SortArgs {
     uint32_t *idx[2];
     ulonglong2 *key[2];
     uint32_t *lcp;
-    uint16_t *bkt;  // bucket of each position during a partition level
+    uint32_t *bkt;  // per position during a partition level: bucket << 12 | offset
 };
 
 // ---- device workspace ---------------------------------------------------------
@@ -121,7 +121,7 @@ constexpr WsLayout ws_layout(uint64_t n) {
     o.key0 = take(n * 16);
     o.key1 = take(n * 16);
     o.lcp = take(n * 4);
-    o.bkt = take(n * 2);
+    o.bkt = take(n * 4);
     o.R = take(half * sizeof(Seg));
     o.N = take(half * sizeof(Seg));
     o.W1 = take(half * sizeof(Seg));
@@ -154,7 +154,8 @@ struct Workspace {
     ulonglong2 *key0, *key1, *spl;
     Seg *R, *N, *W1, *W8, *S, *E, *L, *L2;
     uint2 *B;
-    uint16_t *tbl, *bkt;
+    uint16_t *tbl;
+    uint32_t *bkt;
     Counters *ctr;
     size_t cm_cap;
 };
@@ -165,7 +166,7 @@ inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
     w.key0 = (ulonglong2 *)(base + o.key0);
     w.key1 = (ulonglong2 *)(base + o.key1);
     w.lcp = (uint32_t *)(base + o.lcp);
-    w.bkt = (uint16_t *)(base + o.bkt);
+    w.bkt = (uint32_t *)(base + o.bkt);
     w.R = (Seg *)(base + o.R);
     w.N = (Seg *)(base + o.N);
     w.W1 = (Seg *)(base + o.W1);

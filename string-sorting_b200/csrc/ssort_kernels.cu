@@ -847,6 +847,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr int SUB = PART_TILE / PART_WARPS;
     const uint32_t total_tiles = tile_base[nL];
+    const uint32_t lt = lanemask_lt();
     uint32_t loaded = ~0u;
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
@@ -872,111 +873,156 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
             const uint32_t e = lo + c * 32 + lane;
             kk[c] = e < s.len ? to_key(K[e]) : key_max();
         }
+        // Bucket and rank among the warp's earlier keys of the same bucket
+        // (keys are visited in position order: the scatter stays stable).
+        uint32_t br[PART_ITEMS];
 #pragma unroll
         for (int c = 0; c < PART_ITEMS; ++c) {
             const uint32_t e = lo + c * 32 + lane;
             const uint32_t b = e < s.len ? classify_tbl(sm.spl, sm.tbl, u, f, kk[c]) : nb;
-            if (e < s.len) a.bkt[s.start + e] = (uint16_t)b;
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
-            if ((peers & lanemask_lt()) == 0) hist[w][b] += (uint16_t)__popc(peers);
+            const uint32_t r = __popc(peers & lt);
+            const uint32_t base = hist[w][b];
             __syncwarp();
+            if (r == 0) hist[w][b] = (uint16_t)(base + __popc(peers));
+            __syncwarp();
+            br[c] = (b << 16) | (base + r);
         }
         __syncthreads();
+        // Per bucket: the tile's count (to the count matrix) and each warp's
+        // offset inside the tile's run of that bucket.
         for (uint32_t q = threadIdx.x; q < nb; q += PART_THREADS) {
-            uint32_t sum = 0;
+            uint32_t run = 0;
 #pragma unroll
-            for (int ww = 0; ww < PART_WARPS; ++ww) sum += hist[ww][q];
-            cm[cm_base[si] + (uint64_t)q * nt + tl] = sum;
+            for (int ww = 0; ww < PART_WARPS; ++ww) {
+                const uint32_t x = hist[ww][q];
+                hist[ww][q] = (uint16_t)run;
+                run += x;
+            }
+            cm[cm_base[si] + (uint64_t)q * nt + tl] = run;
+        }
+        __syncthreads();
+        // Packed destination for the scatter: bucket << 12 | offset in the
+        // tile's run of that bucket (< PART_TILE).
+#pragma unroll
+        for (int c = 0; c < PART_ITEMS; ++c) {
+            const uint32_t e = lo + c * 32 + lane;
+            if (e < s.len) {
+                const uint32_t b = br[c] >> 16;
+                a.bkt[s.start + e] = (b << 12) | (hist[w][b] + (br[c] & 0xFFFF));
+            }
         }
         __syncthreads();
     }
 }
 
-// ---- partition scatter: stable within and across tiles ---------------------
-__global__ void __launch_bounds__(PART_THREADS, 2) k_scatter(SortArgs a, const Seg *__restrict__ L,
-                                                          uint32_t nL,
-                                                          const uint32_t *__restrict__ tile_base,
-                                                          const ulonglong2 *__restrict__ spl,
-                                                          const uint32_t *__restrict__ nspl,
-                                                          const uint16_t *__restrict__ tbl,
-                                                          const uint32_t *__restrict__ cm_base,
-                                                          const uint32_t *__restrict__ cm_scan) {
-    extern __shared__ __align__(16) unsigned char part_smem[];
-    PartSmem &sm = *reinterpret_cast<PartSmem *>(part_smem);
-    auto &wcnt = sm.cnt;
-    uint32_t *gbase = sm.gbase;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    constexpr int SUB = PART_TILE / PART_WARPS;  // consecutive keys per warp
+// ---- partition scatter: a copy to precomputed destinations --------------------
+// k_count left every key's bucket and its offset inside the tile's run of that
+// bucket; the run's start comes from the scanned count matrix.  Tile order
+// and within-tile order follow positions, so the scatter is stable.  Each
+// tile is first laid out in shared memory in output order (its bucket runs
+// back to back), so consecutive threads store to consecutive addresses within
+// every run.
+constexpr int SCATTER_THREADS = 256;
+constexpr int SCATTER_ITEMS = PART_TILE / SCATTER_THREADS;  // 16
+struct ScatterSmem {
+    ulonglong2 key[PART_TILE];
+    uint32_t idx[PART_TILE];
+    uint32_t dst[PART_TILE];
+    uint32_t gbase[NB_MAX + 1];
+    uint32_t tstart[NB_MAX + 1];
+    uint32_t wsum[SCATTER_THREADS / 32];
+};
+
+__global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const Seg *__restrict__ L,
+                                                             uint32_t nL,
+                                                             const uint32_t *__restrict__ tile_base,
+                                                             const uint32_t *__restrict__ nspl,
+                                                             const uint32_t *__restrict__ cm_base,
+                                                             const uint32_t *__restrict__ cm_scan) {
+    extern __shared__ __align__(16) unsigned char scatter_smem[];
+    ScatterSmem &sm = *reinterpret_cast<ScatterSmem *>(scatter_smem);
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr uint32_t QPT = (NB_MAX + 1) / SCATTER_THREADS;  // buckets per thread (4)
     const uint32_t total_tiles = tile_base[nL];
-    uint32_t loaded = ~0u;
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
         const uint32_t u = nspl[si] & 0xFFFF, nb = 2 * u + 1;
         const uint32_t tl = t - tile_base[si];
         const uint32_t nt = tile_base[si + 1] - tile_base[si];
-        const uint32_t lo = tl * PART_TILE + w * SUB;
-        {
-            uint32_t *w32 = reinterpret_cast<uint32_t *>(&wcnt[0][0]);
-            for (uint32_t q = threadIdx.x; q < PART_WARPS * (NB_MAX + 1) / 2; q += PART_THREADS)
-                w32[q] = 0;
-        }
+        const uint32_t cmb = cm_base[si];
+        const uint32_t seg0 = cm_scan[cmb];
+        const uint32_t lo = tl * PART_TILE;
+        const uint32_t tlen = min((uint32_t)PART_TILE, s.len - lo);
         const int ib = s.flags & SEG_BUF1;
         const ulonglong2 *Kin = a.keyb(ib) + s.start;
         const uint32_t *Iin = a.idxb(ib) + s.start;
+        const uint32_t *Din = a.bkt + s.start;
+        // Element loads first (they overlap the count-matrix reads below).
+        ulonglong2 kk[SCATTER_ITEMS];
+        uint32_t ii[SCATTER_ITEMS], dd[SCATTER_ITEMS];
+#pragma unroll
+        for (int c = 0; c < SCATTER_ITEMS; ++c) {
+            const uint32_t e = c * SCATTER_THREADS + threadIdx.x;
+            if (e < tlen) {
+                kk[c] = Kin[lo + e];
+                ii[c] = Iin[lo + e];
+                dd[c] = Din[lo + e];
+            }
+        }
+        // Per bucket: the tile's run start in the segment and the tile's
+        // count (difference of consecutive scanned entries), then an exclusive
+        // scan of the counts gives each run's start inside the tile.
+        uint32_t cnt[QPT];
+        uint32_t mysum = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < QPT; ++j) {
+            const uint32_t q = threadIdx.x * QPT + j;
+            uint32_t c0 = 0;
+            if (q < nb) {
+                const uint64_t at = cmb + (uint64_t)q * nt + tl;
+                const uint32_t g = cm_scan[at];
+                c0 = cm_scan[at + 1] - g;  // next tile, or next bucket's first tile
+                sm.gbase[q] = g - seg0;
+            }
+            cnt[j] = c0;
+            mysum += c0;
+        }
+        uint32_t incl = mysum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (uint32_t)d) incl += y;
+        }
+        if (lane == 31) sm.wsum[w] = incl;
+        __syncthreads();
+        uint32_t run = incl - mysum;
+        for (uint32_t q = 0; q < w; ++q) run += sm.wsum[q];
+#pragma unroll
+        for (uint32_t j = 0; j < QPT; ++j) {
+            sm.tstart[threadIdx.x * QPT + j] = run;
+            run += cnt[j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < SCATTER_ITEMS; ++c) {
+            const uint32_t e = c * SCATTER_THREADS + threadIdx.x;
+            if (e < tlen) {
+                const uint32_t b = dd[c] >> 12, off = dd[c] & (PART_TILE - 1);
+                const uint32_t slot = sm.tstart[b] + off;
+                sm.key[slot] = kk[c];
+                sm.idx[slot] = ii[c];
+                sm.dst[slot] = sm.gbase[b] + off;
+            }
+        }
+        __syncthreads();
         ulonglong2 *Kout = a.keyb(ib ^ 1) + s.start;
         uint32_t *Iout = a.idxb(ib ^ 1) + s.start;
-        const uint16_t *Bin = a.bkt + s.start;  // buckets found by k_count
-        Key kk[PART_ITEMS];
-        uint32_t ii[PART_ITEMS];
-        uint32_t br[PART_ITEMS];
-        uint32_t bb[PART_ITEMS];
-#pragma unroll
-        for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t e = lo + c * 32 + lane;
-            const bool v = e < s.len;
-            kk[c] = v ? to_key(Kin[e]) : key_max();
-            ii[c] = v ? Iin[e] : 0;
-            bb[c] = v ? Bin[e] : nb;
-        }
-        __syncthreads();
-        const uint32_t lt = lanemask_lt();
-#pragma unroll
-        for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t b = bb[c];
-            const uint32_t peers = __match_any_sync(0xffffffffu, b);
-            const uint32_t r = __popc(peers & lt);
-            const uint32_t base = wcnt[w][b];
-            __syncwarp();
-            if (r == 0) wcnt[w][b] = (uint16_t)(base + __popc(peers));
-            __syncwarp();
-            br[c] = (b << 16) | (base + r);
-        }
-        __syncthreads();
-        // Exclusive scan over warps per bucket (tile-local, < PART_TILE) and
-        // the tile's global base per bucket.
-        const uint32_t cmb = cm_base[si];
-        const uint32_t seg0 = cm_scan[cmb];
-        for (uint32_t q = threadIdx.x; q < nb; q += PART_THREADS) {
-            gbase[q] = cm_scan[cmb + (uint64_t)q * nt + tl] - seg0;
-            uint32_t run = 0;
-#pragma unroll
-            for (int ww = 0; ww < PART_WARPS; ++ww) {
-                const uint32_t x = wcnt[ww][q];
-                wcnt[ww][q] = (uint16_t)run;
-                run += x;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t e = lo + c * 32 + lane;
-            if (e < s.len) {
-                const uint32_t b = br[c] >> 16;
-                const uint32_t o = gbase[b] + wcnt[w][b] + (br[c] & 0xFFFF);
-                Kout[o] = from_key(kk[c]);
-                Iout[o] = ii[c];
-            }
+        for (uint32_t i = threadIdx.x; i < tlen; i += SCATTER_THREADS) {
+            const uint32_t o = sm.dst[i];
+            Kout[o] = sm.key[i];
+            Iout[o] = sm.idx[i];
         }
         __syncthreads();
     }
@@ -1545,11 +1591,11 @@ void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(PartSmem));
+                             (int)sizeof(ScatterSmem));
         attr = true;
     }
-    k_scatter<<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl, tbl,
-                                                            cm_base, cm_scan);
+    k_scatter<<<grid, SCATTER_THREADS, sizeof(ScatterSmem), st>>>(a, L, nL, tile_base, nspl,
+                                                                  cm_base, cm_scan);
 }
 
 void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
