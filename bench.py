@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(pyssort.WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--target-bucket", type=int, default=0,
+                    help="override the partition's wanted strings per range bucket")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the workload's string count (profiling runs only; "
                          "the reported workload is the full one at 1.0)")
@@ -217,6 +219,8 @@ def run_ours(args, rank, world, local_rank, dist):
     d_perm = torch.empty(n, dtype=torch.int32, device=f"cuda:{local_rank}")
     d_lcp = torch.empty(n, dtype=torch.int32, device=f"cuda:{local_rank}")
     sorter = pyssort.Sorter(local_rank)
+    if args.target_bucket:
+        sorter.set_param(pyssort.SSORT_PARAM_TARGET_BUCKET, args.target_bucket)
     stream = torch.cuda.Stream(device=local_rank)
     ab = ss.arena.nbytes
 

@@ -133,6 +133,12 @@ typedef struct {
 
 int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
 
+/* Tuning parameters of a context (defaults are chosen per size class inside
+ * the library; these override them for every later sort on the context). */
+#define SSORT_PARAM_TARGET_BUCKET 1 /* wanted strings per range bucket of a sample
+                                       partition, 32..2048 (default 512) */
+int ssort_set_param(ssort_ctx *ctx, int param, int64_t value);
+
 /* Kernel-level timing: when enabled, each kernel launch of a sort is bracketed
  * by CUDA events and its time is accumulated per kernel name. */
 int ssort_set_profiling(ssort_ctx *ctx, int enabled);

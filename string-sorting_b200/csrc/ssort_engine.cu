@@ -73,6 +73,7 @@ struct ssort_ctx {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 
     bool prof = false;
+    uint32_t target_bucket = TARGET_BUCKET;  // tuning: wanted strings per range bucket
     struct Rec {
         const char *name;
         cudaEvent_t a, b;
@@ -219,6 +220,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.key[1] = ws.key1;
     a.lcp = d_lcp ? d_lcp : ws.lcp;
     a.bkt = ws.bkt;
+    a.target_bucket = target_bucket;
 
     Seg *cur = ws.R, *nxt = ws.N;
     Counters *dc = ws.ctr;
@@ -245,9 +247,8 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
         Seg *lcur = ws.L, *lnext = ws.L2;
         if (n_large) {
             // Keys of the large segments at this depth.
-            LAUNCH(this, "tile_counts",
-                   launch_tile_counts(lcur, n_large, GATHER_TILE, ws.tmp, st));
-            SS_TRY(scan(ws.tmp, ws.tile_base, n_large, nullptr));
+            LAUNCH(this, "seg_tiles",
+                   launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));
             LAUNCH(this, "gather",
                    launch_gather(a, lcur, n_large, ws.tile_base, g8, st));
         }
@@ -263,8 +264,9 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
                    launch_sample(a, lcur, n_large, ws.spl, ws.nspl,
                                  ws.tbl, ws.ntiles, ws.cm_size,
                                  st));
-            SS_TRY(scan(ws.ntiles, ws.tile_base, n_large, nullptr));
-            SS_TRY(scan(ws.cm_size, ws.cm_base, n_large, nullptr));
+            LAUNCH(this, "scan_pair",
+                   launch_scan_pair(ws.ntiles, ws.tile_base, ws.cm_size, ws.cm_base, n_large,
+                                    st));
             LAUNCH(this, "count",
                    launch_count(a, lcur, n_large, ws.tile_base,
                                 ws.spl, ws.nspl,
@@ -593,6 +595,18 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out) {
     if (!ctx || !out) return fail(SSORT_EINVAL, "null argument");
     *out = ctx->stats;
     return SSORT_OK;
+}
+
+int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
+    if (!ctx) return fail(SSORT_EINVAL, "null context");
+    switch (param) {
+        case SSORT_PARAM_TARGET_BUCKET:
+            if (value < 32 || value > SMALL_CAP) return fail(SSORT_EINVAL, "target_bucket out of range");
+            ctx->target_bucket = (uint32_t)value;
+            return SSORT_OK;
+        default:
+            return fail(SSORT_EINVAL, "unknown parameter");
+    }
 }
 
 int ssort_set_profiling(ssort_ctx *ctx, int enabled) {

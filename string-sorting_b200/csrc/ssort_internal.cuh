@@ -53,7 +53,7 @@ constexpr int TBL_N = 1 << TBL_BITS;
 constexpr int TBL_STRIDE = TBL_N + 64;  // uint16 entries per segment (TBL_N + 1 used)
 constexpr int NB_MAX = 2 * KMAX + 1;    // range + equality buckets
 constexpr int SAMPLES_MAX = 4096;       // keys sampled per large segment
-constexpr int TARGET_BUCKET = 512;      // wanted strings per range bucket
+constexpr int TARGET_BUCKET = 512;      // default wanted strings per range bucket
 constexpr int PART_THREADS = 512;
 constexpr int PART_WARPS = PART_THREADS / 32;
 constexpr int PART_ITEMS = 8;
@@ -90,6 +90,7 @@ struct SortArgs {
     ulonglong2 *key[2];
     uint32_t *lcp;
     uint32_t *bkt;  // per position during a partition level: bucket << 12 | offset
+    uint32_t target_bucket;  // wanted strings per range bucket of a partition
 };
 
 // ---- device workspace ---------------------------------------------------------
@@ -197,6 +198,10 @@ void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L
                      cudaStream_t st);
 void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
                         cudaStream_t st);
+// Single-CTA scans of short per-segment arrays (out*[n] = totals).
+void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,
+                      uint32_t n, cudaStream_t st);
+void launch_seg_tiles(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out, cudaStream_t st);
 // exclusive scan of in[0..n) into out[0..n); out[n] = total (out has n+1 slots).
 // n is read from *n_dev when n_dev is not null (n_host is then an upper bound).
 void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,

@@ -565,6 +565,74 @@ __global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *W1, Seg 
     }
 }
 
+// ---- single-CTA exclusive scans of short per-segment arrays -----------------
+constexpr int SMALL_SCAN_THREADS = 1024;
+
+// Inclusive scan of v across the CTA; returns the CTA total in `total`.
+__device__ __forceinline__ uint32_t cta_inclusive_scan(uint32_t v, uint32_t &total,
+                                                       uint32_t *warp_sums) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= (uint32_t)d) v += y;
+    }
+    if (lane == 31) warp_sums[w] = v;
+    __syncthreads();
+    uint32_t before = 0;
+    total = 0;
+    for (uint32_t q = 0; q < SMALL_SCAN_THREADS / 32; ++q) {
+        const uint32_t x = warp_sums[q];
+        if (q < w) before += x;
+        total += x;
+    }
+    __syncthreads();
+    return v + before;
+}
+
+// out0/out1 = exclusive scans of in0/in1 (n entries); out*[n] = totals.
+__global__ void __launch_bounds__(SMALL_SCAN_THREADS) k_scan_pair(const uint32_t *__restrict__ in0,
+                                                                   uint32_t *out0,
+                                                                   const uint32_t *__restrict__ in1,
+                                                                   uint32_t *out1, uint32_t n) {
+    __shared__ uint32_t warp_sums[SMALL_SCAN_THREADS / 32];
+    uint32_t c0 = 0, c1 = 0;
+    for (uint32_t b = 0; b < n; b += SMALL_SCAN_THREADS) {
+        const uint32_t i = b + threadIdx.x;
+        const uint32_t v0 = i < n ? in0[i] : 0, v1 = i < n ? in1[i] : 0;
+        uint32_t t0, t1;
+        const uint32_t s0 = cta_inclusive_scan(v0, t0, warp_sums);
+        const uint32_t s1 = cta_inclusive_scan(v1, t1, warp_sums);
+        if (i < n) {
+            out0[i] = c0 + s0 - v0;
+            out1[i] = c1 + s1 - v1;
+        }
+        c0 += t0;
+        c1 += t1;
+    }
+    if (threadIdx.x == 0) {
+        out0[n] = c0;
+        out1[n] = c1;
+    }
+}
+
+// out = exclusive scan of ceil(len / tile) over the segments; out[n] = total.
+__global__ void __launch_bounds__(SMALL_SCAN_THREADS) k_seg_tiles(const Seg *__restrict__ segs,
+                                                                   uint32_t n, uint32_t tile,
+                                                                   uint32_t *out) {
+    __shared__ uint32_t warp_sums[SMALL_SCAN_THREADS / 32];
+    uint32_t c = 0;
+    for (uint32_t b = 0; b < n; b += SMALL_SCAN_THREADS) {
+        const uint32_t i = b + threadIdx.x;
+        const uint32_t v = i < n ? (segs[i].len + tile - 1) / tile : 0;
+        uint32_t t;
+        const uint32_t s = cta_inclusive_scan(v, t, warp_sums);
+        if (i < n) out[i] = c + s - v;
+        c += t;
+    }
+    if (threadIdx.x == 0) out[n] = c;
+}
+
 __global__ void k_tile_counts(const Seg *__restrict__ segs, uint32_t n, uint32_t tile,
                               uint32_t *out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -720,47 +788,124 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
                                                            ulonglong2 *spl, uint32_t *nspl,
                                                            uint16_t *tbl, uint32_t *ntiles,
                                                            uint32_t *cm_size) {
-    extern __shared__ ulonglong2 smp[];  // SAMPLES_MAX keys
+    // smp: SAMPLES_MAX keys; sv: their packed sort keys (padded layout)
+    extern __shared__ __align__(16) unsigned char sample_smem[];
+    ulonglong2 *smp = reinterpret_cast<ulonglong2 *>(sample_smem);
+    uint64_t *sv = reinterpret_cast<uint64_t *>(smp + SAMPLES_MAX);
+    __shared__ ulonglong2 cands[SAMPLE_THREADS];
     __shared__ uint32_t warp_cnt[SAMPLE_THREADS / 32 + 1];
+    __shared__ uint64_t red[2][SAMPLE_THREADS / 32];
     const Seg s = L[blockIdx.x];
     const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
-    uint32_t k = (s.len + TARGET_BUCKET - 1) / TARGET_BUCKET;
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t k = (s.len + a.target_bucket - 1) / a.target_bucket;
     if (k > (uint32_t)KMAX) k = KMAX;
     if (k < 1) k = 1;
     uint32_t S = next_pow2(8 * (k + 1));
-    if (S < 128) S = 128;
+    if (S < 256) S = 256;
     if (S > (uint32_t)SAMPLES_MAX) S = SAMPLES_MAX;
     for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
         const uint32_t r = hash32(s.start * 0x9E3779B1u + i * 0x85EBCA77u + s.len);
         smp[i] = K[(uint32_t)(((uint64_t)r * s.len) >> 32)];
     }
     __syncthreads();
-    for (uint32_t kk = 2; kk <= S; kk <<= 1) {
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
-                const uint32_t l = i ^ j;
-                if (l > i) {
-                    const Key x = to_key(smp[i]), y = to_key(smp[l]);
-                    if (key_lt(y, x) == ((i & kk) == 0)) {
-                        smp[i] = from_key(y);
-                        smp[l] = from_key(x);
-                    }
-                }
+    // Order the samples by packed keys (window after the samples' common
+    // prefix, 12-bit sample index): warp runs of 256, then merges.  The order
+    // only picks quantiles; the chosen candidates are sorted by full key below.
+    {
+        const Key k0 = to_key(smp[0]);
+        uint64_t dh = 0, dl = 0;
+        for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
+            const Key x = to_key(smp[i]);
+            dh |= x.hi ^ k0.hi;
+            dl |= x.lo ^ k0.lo;
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            dh |= __shfl_xor_sync(0xffffffffu, dh, d);
+            dl |= __shfl_xor_sync(0xffffffffu, dl, d);
+        }
+        if (lane == 0) {
+            red[0][w] = dh;
+            red[1][w] = dl;
+        }
+    }
+    __syncthreads();
+    uint64_t dh = 0, dl = 0;
+#pragma unroll
+    for (int q = 0; q < SAMPLE_THREADS / 32; ++q) {
+        dh |= red[0][q];
+        dl |= red[1][q];
+    }
+    const uint32_t fs = (dh | dl) ? clz128(dh, dl) : 128u;
+    if (w * 256 < S) {
+        uint64_t v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t e = w * 256 + lane * 8 + i;
+            v[i] = fs < 128 ? ((window64(to_key(smp[e]), fs) & ~0xFFFull) | e) : e;
+        }
+        warp_bitonic64<8>(v, lane);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) sv[pad(w * 256 + lane * 8 + i)] = v[i];
+    }
+    __syncthreads();
+    for (uint32_t run = 256; run < S; run <<= 1) {
+        const uint32_t o = threadIdx.x * 8;
+        uint64_t ov[8];
+        const bool active = o < S;
+        if (active) {
+            const uint32_t a0 = o / (2 * run) * (2 * run), b0 = a0 + run;
+            const uint32_t d = o - a0;
+            uint32_t ia = merge_split64(sv, a0, run, b0, run, d);
+            uint32_t ib = d - ia;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const uint64_t va = ia < run ? sv[pad(a0 + ia)] : ~0ull;
+                const uint64_t vb = ib < run ? sv[pad(b0 + ib)] : ~0ull;
+                const bool take_a = ib >= run || (ia < run && va < vb);
+                ov[i] = take_a ? va : vb;
+                ia += take_a;
+                ib += !take_a;
             }
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) sv[pad(o + i)] = ov[i];
+        }
+        __syncthreads();
+    }
+    // Candidates at ranks (j+1)*S/(k+1), padded with the all-ones key, sorted
+    // by full key with a bitonic network over SAMPLE_THREADS slots.
+    {
+        const uint32_t j = threadIdx.x;
+        cands[j] = j < k ? smp[sv[pad(((j + 1) * S) / (k + 1))] & 0xFFF] : from_key(key_max());
+    }
+    __syncthreads();
+    for (uint32_t kk = 2; kk <= (uint32_t)SAMPLE_THREADS; kk <<= 1) {
+        for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+            const uint32_t i = threadIdx.x, l = i ^ jj;
+            Key x = to_key(cands[i]), y = to_key(cands[l]);
+            const bool lower = l > i;
+            const bool asc = (i & kk) == 0;
+            // the lower slot keeps the min when ascending, the max otherwise
+            const bool take = lower ? (asc ? key_lt(y, x) : key_lt(x, y))
+                                    : (asc ? key_lt(x, y) : key_lt(y, x));
+            __syncthreads();
+            if (take) cands[i] = from_key(y);
             __syncthreads();
         }
     }
-    // Candidate j < k sits at sample rank (j+1)*S/(k+1); it survives if it
-    // differs from candidate j-1.  Survivors are compacted in order.
+    // Survivors: the distinct candidates, compacted in order.
     const uint32_t j = threadIdx.x;
     Key cand{0, 0};
     bool keep = false;
     if (j < k) {
-        cand = to_key(smp[((j + 1) * S) / (k + 1)]);
-        keep = j == 0 || !key_eq(to_key(smp[(j * S) / (k + 1)]), cand);
+        cand = to_key(cands[j]);
+        keep = j == 0 || !key_eq(to_key(cands[j - 1]), cand);
     }
     const uint32_t bal = __ballot_sync(0xffffffffu, keep);
-    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0) warp_cnt[w] = __popc(bal);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1536,6 +1681,15 @@ void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L
     k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, W1, W8, S, L, c);
 }
 
+void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,
+                      uint32_t n, cudaStream_t st) {
+    k_scan_pair<<<1, SMALL_SCAN_THREADS, 0, st>>>(in0, out0, in1, out1, n);
+}
+
+void launch_seg_tiles(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out, cudaStream_t st) {
+    k_seg_tiles<<<1, SMALL_SCAN_THREADS, 0, st>>>(segs, n, tile, out);
+}
+
 void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
                         cudaStream_t st) {
     if (!n) return;
@@ -1562,7 +1716,8 @@ void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl
                    uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size, cudaStream_t st) {
     if (!nL) return;
     static bool attr = false;
-    const int smem = SAMPLES_MAX * sizeof(ulonglong2);
+    const int smem = SAMPLES_MAX * sizeof(ulonglong2) +
+                     (SAMPLES_MAX + SAMPLES_MAX / 8) * sizeof(uint64_t);
     if (!attr) {
         cudaFuncSetAttribute(k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;

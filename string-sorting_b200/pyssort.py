@@ -22,7 +22,9 @@ EXPORTS = (
     "msd_gpu", "ssort_strerror", "ssort_last_error", "ssort_ctx_create", "ssort_ctx_destroy",
     "ssort_sort_device", "ssort_sort_host", "ssort_sort_strings", "ssort_get_stats",
     "ssort_set_profiling", "ssort_get_kernel_times", "ssort_sort_device_noalloc",
+    "ssort_set_param",
 )
+SSORT_PARAM_TARGET_BUCKET = 1
 
 
 class SsortError(RuntimeError):
@@ -85,6 +87,7 @@ def lib():
         L.ssort_sort_strings.argtypes = [vp, vp, ctypes.c_size_t, vp]
         L.ssort_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.ssort_set_profiling.argtypes = [vp, i32]
+        L.ssort_set_param.argtypes = [vp, i32, ctypes.c_int64]
         L.ssort_get_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p),
                                              ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_uint64), i32]
@@ -176,6 +179,9 @@ class Sorter:
         s = Stats()
         _check(lib().ssort_get_stats(self._ctx, ctypes.byref(s)))
         return s
+
+    def set_param(self, param, value):
+        _check(lib().ssort_set_param(self._ctx, int(param), int(value)))
 
     def set_profiling(self, on):
         _check(lib().ssort_set_profiling(self._ctx, 1 if on else 0))
