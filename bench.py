@@ -42,6 +42,9 @@ DESCRIPTIONS = {
     "zipf_words_100m": "100,000,000 copies of Zipf(1.0) words from 1,000,000 distinct "
                        "geometric(0.15)-length [a-z] words clipped to [1,24]; seed 3; uint64 offsets",
     "uniform_1m": "1,000,000 strings, length U[1,20], bytes U{'a'..'z'}; seed 1",
+    "batch_c4": "independent instances, counts log-uniform in [100, 2,000,000], alphabet "
+                "{4 from 'A', 26 from 'a', 95 from ' '}, length U[1, L], L in {8, 32, 128}; "
+                "the instance list stops at 1.5e9 expected key bytes; seeds 5 (list), 4 (strings)",
 }
 
 
@@ -51,7 +54,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(pyssort.WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    choices=sorted(pyssort.WORKLOADS) + ["batch_c4"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--target-bucket", type=int, default=0,
@@ -349,6 +353,74 @@ def run_ours(args, rank, world, local_rank, dist):
     return out
 
 
+def run_batch(args):
+    """Batched form vs plain form on the same GPU: one ssort_sort_batch_device
+    call over all instances vs one ssort_sort_device call per instance."""
+    import torch
+    torch.cuda.set_device(0)
+    params = pyssort.batch_instance_params(20000, 5, key_byte_limit=1.5e9 * args.scale)
+    ss = pyssort.gen_instances(params, seed=4)
+    n, k = ss.n, len(params)
+    d_arena = torch.from_numpy(ss.arena).cuda()
+    d_offs = torch.from_numpy(ss.offs.view(np.int64)).cuda()
+    d_inst = torch.from_numpy(ss.inst_start.view(np.int32)).cuda()
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_lcp = torch.empty(n, dtype=torch.int32, device="cuda")
+    sorter = pyssort.Sorter(0)
+    stream = torch.cuda.Stream()
+    ab = ss.arena.nbytes
+
+    def batched():
+        sorter.sort_batch_device(d_arena, ab, d_offs, 8, n, d_inst, k, d_perm, d_lcp,
+                                 stream=stream.cuda_stream)
+
+    starts = [int(x) for x in ss.inst_start]
+
+    def plain():
+        for i in range(k):
+            lo, hi = starts[i], starts[i + 1]
+            if hi > lo:
+                sorter.sort_device(d_arena, ab, d_offs.data_ptr() + 8 * lo, 8, hi - lo,
+                                   d_perm.data_ptr() + 4 * lo, d_lcp.data_ptr() + 4 * lo,
+                                   stream=stream.cuda_stream)
+
+    def timed(fn, steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    for _ in range(args.warmup):
+        batched()
+    clocks = Clocks(0)
+    clocks.start()
+    time.sleep(0.3)
+    ms_b = timed(batched, args.steps)
+    st = sorter.stats()
+    plain()
+    ms_p = timed(plain, max(1, min(args.steps, 3)))
+    clocks.stop()
+    return {
+        "metric": METRIC, "value": n / (ms_b / 1e3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
+        "config": {"workload": "batch_c4", "description": DESCRIPTIONS["batch_c4"],
+                   "n_instances": k, "n_strings": n, "key_bytes": int(ss.text_bytes),
+                   "parallelism": "single", "l2": f"inputs larger than L2 (arena {ab / 1e9:.2f} GB)"},
+        "key_gbs": round(ss.text_bytes / (ms_b / 1e3) / 1e9, 2),
+        "plain": {"value": n / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p,
+                  "calls_per_step": k},
+        "batched_vs_plain": round(ms_p / ms_b, 2),
+        "clocks": clocks.summary(), "stats": st.as_dict(),
+    }
+
+
 def _ref_lib():
     p = os.path.join(ROOT, "oracle", "_ref", "libref.so")
     if not os.path.exists(p):
@@ -437,6 +509,10 @@ def main():
         out = run_reference(args, rank)
         if out is not None:
             print(json.dumps(out), flush=True)
+        return
+    if args.workload == "batch_c4":
+        if rank == 0:
+            print(json.dumps(run_batch(args)), flush=True)
         return
     dist = None
     if world > 1:

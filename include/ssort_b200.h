@@ -105,6 +105,25 @@ int ssort_sort_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes,
                     const void *offs, int off_width, uint64_t n, uint32_t *perm,
                     uint32_t *lcp);
 
+/*
+ * Batched sort: ninst independent instances in one call (no counterpart in
+ * the reference, which sorts one array per call).  Instance i owns positions
+ * inst_start[i] .. inst_start[i+1]-1 of the offsets array (inst_start has
+ * ninst + 1 non-decreasing entries, inst_start[0] = 0, inst_start[ninst] = n);
+ * its strings may live anywhere in the shared arena.  For a position p of
+ * instance i, perm[p] is the index, counted from inst_start[i], of the string
+ * of instance i ranked p - inst_start[i]; lcp restarts at 0 for every
+ * instance.  All instances are refined together: every kernel launch works
+ * on the live segments of all of them.
+ */
+int ssort_sort_batch_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                            const void *d_offs, int off_width, uint64_t n,
+                            const uint32_t *d_inst_start, uint32_t ninst, uint32_t *d_perm,
+                            uint32_t *d_lcp, void *stream);
+int ssort_sort_batch_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes,
+                          const void *offs, int off_width, uint64_t n, const uint32_t *inst_start,
+                          uint32_t ninst, uint32_t *perm, uint32_t *lcp);
+
 /* Pointer-array form behind msd_gpu with a status return: permutes
  * strings[0..n) in place and, when lcp_out is not NULL, writes the LCP array
  * of the sorted order. */

@@ -65,7 +65,7 @@ struct ssort_ctx {
     DBuf ws_buf;    // one block holding every scratch buffer (ws_layout)
     Workspace ws{};
     size_t ws_n = 0;  // string capacity ws is laid out for
-    DBuf arena, offs, perm;  // staging for the host-buffer entry points
+    DBuf arena, offs, perm, inst;  // staging for the host-buffer entry points
     HBuf h_offs, h_arena, h_perm;
     Counters *h_ctr = nullptr;
 
@@ -163,9 +163,11 @@ struct ssort_ctx {
     int reserve(uint32_t n);
     int scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev);
     int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
-            uint32_t n, uint32_t *d_perm, uint32_t *d_lcp);
+            uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
+            uint32_t ninst = 0);
     int run_ws(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
-               uint32_t n, uint32_t *d_perm, uint32_t *d_lcp);
+               uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
+               uint32_t ninst = 0);
 };
 
 #define LAUNCH(ctx, name, call)                 \
@@ -200,14 +202,18 @@ int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const ui
 // device twice per round (segment counts after classification, and the
 // next round's count) plus once per partition level.
 int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
-                   int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp) {
+                   int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp,
+                   const uint32_t *d_inst, uint32_t ninst) {
     SS_TRY(reserve(n));
-    return run_ws(arena_p, arena_bytes, offs_p, off_width, n, d_perm, d_lcp);
+    return run_ws(arena_p, arena_bytes, offs_p, off_width, n, d_perm, d_lcp, d_inst, ninst);
 }
 
-// The round loop over an already laid-out workspace `ws`.
+// The round loop over an already laid-out workspace `ws`.  With an instance
+// table (d_inst, ninst > 0) every instance starts as its own round-0 segment
+// and the result indices are made instance-local at the end.
 int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
-                      int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp) {
+                      int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp,
+                      const uint32_t *d_inst, uint32_t ninst) {
     SortArgs a{};
     a.arena = arena_p;
     a.arena_bytes = arena_bytes;
@@ -227,10 +233,17 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
 
     LAUNCH(this, "iota", launch_iota(d_perm, n, st));
     SS_CUDA(cudaMemsetAsync(a.lcp, 0, 4, st));
-    if (n < 2) return SSORT_OK;
-    Seg first{0, n, 0, 0};
-    SS_CUDA(cudaMemcpyAsync(cur, &first, sizeof(Seg), cudaMemcpyHostToDevice, st));
     uint32_t n_cur = 1;
+    if (d_inst) {
+        SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+        LAUNCH(this, "init_batch", launch_init_batch(d_inst, ninst, cur, a.lcp, dc, st));
+        SS_TRY(sync_counters());
+        n_cur = h_ctr->n_next;
+    } else {
+        if (n < 2) return SSORT_OK;
+        Seg first{0, n, 0, 0};
+        SS_CUDA(cudaMemcpyAsync(cur, &first, sizeof(Seg), cudaMemcpyHostToDevice, st));
+    }
     uint64_t live = n;
     uint32_t round = 0;
     const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
@@ -312,6 +325,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
         ++round;
     }
     stats.rounds = round;
+    if (d_inst) LAUNCH(this, "localize", launch_localize(d_perm, n, d_inst, ninst, st));
     return SSORT_OK;
 }
 
@@ -327,11 +341,12 @@ int validate_common(ssort_ctx *ctx, int off_width, uint64_t n) {
 
 int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                      const void *d_offs, int off_width, uint64_t n, uint32_t *d_perm,
-                     uint32_t *d_lcp) {
+                     uint32_t *d_lcp, const uint32_t *d_inst = nullptr, uint32_t ninst = 0) {
     ctx->stats = ssort_stats{};
     ctx->stats.n = n;
     SS_CUDA(cudaEventRecord(ctx->ev_start, ctx->st));
-    int rc = ctx->run(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, d_perm, d_lcp);
+    int rc = ctx->run(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, d_perm, d_lcp, d_inst,
+                      ninst);
     if (rc != SSORT_OK) {
         cudaStreamSynchronize(ctx->st);
         ctx->recs.clear();
@@ -345,7 +360,7 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
     ctx->stats.device_ms = ms;
     if (ctx->prof) ctx->prof_collect();
     size_t held = 0;
-    for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm})
+    for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst})
         held += b->cap;
     ctx->stats.device_bytes = held;
     return SSORT_OK;
@@ -436,7 +451,7 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
     if (!ctx) return;
     with_device(ctx, [&]() -> int {
         if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
-        for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm})
+        for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst})
             if (b->p) cudaFree(b->p);
         for (HBuf *b : {&ctx->h_offs, &ctx->h_arena, &ctx->h_perm})
             if (b->p) cudaFreeHost(b->p);
@@ -463,6 +478,61 @@ int ssort_sort_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byt
         int rc = sort_device_impl(ctx, d_arena, arena_bytes, d_offs, off_width, n, d_perm, d_lcp);
         ctx->st = ctx->own_stream;
         return rc;
+    });
+}
+
+int ssort_sort_batch_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                            const void *d_offs, int off_width, uint64_t n,
+                            const uint32_t *d_inst_start, uint32_t ninst, uint32_t *d_perm,
+                            uint32_t *d_lcp, void *stream) {
+    SS_TRY(validate_common(ctx, off_width, n));
+    if (n == 0) return SSORT_OK;
+    if (!d_arena || !d_offs || !d_perm || !d_inst_start)
+        return fail(SSORT_EINVAL, "null device buffer");
+    if (ninst == 0) return fail(SSORT_EINVAL, "no instances");
+    if (((uintptr_t)d_arena & 15) != 0)
+        return fail(SSORT_EINVAL, "arena must be 16-byte aligned");
+    return with_device(ctx, [&]() -> int {
+        ctx->st = stream ? (cudaStream_t)stream : ctx->own_stream;
+        int rc = sort_device_impl(ctx, d_arena, arena_bytes, d_offs, off_width, n, d_perm, d_lcp,
+                                  d_inst_start, ninst);
+        ctx->st = ctx->own_stream;
+        return rc;
+    });
+}
+
+int ssort_sort_batch_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes,
+                          const void *offs, int off_width, uint64_t n, const uint32_t *inst_start,
+                          uint32_t ninst, uint32_t *perm, uint32_t *lcp) {
+    SS_TRY(validate_common(ctx, off_width, n));
+    if (n == 0) return SSORT_OK;
+    if (!arena || !offs || !perm || !inst_start) return fail(SSORT_EINVAL, "null host buffer");
+    if (ninst == 0) return fail(SSORT_EINVAL, "no instances");
+    if (inst_start[0] != 0 || inst_start[ninst] != n)
+        return fail(SSORT_EINVAL, "instance table must start at 0 and end at n");
+    for (uint32_t i = 0; i < ninst; ++i)
+        if (inst_start[i + 1] < inst_start[i])
+            return fail(SSORT_EINVAL, "instance table must be non-decreasing");
+    return with_device(ctx, [&]() -> int {
+        ctx->st = ctx->own_stream;
+        SS_TRY(ctx->ensure(ctx->arena, arena_bytes + 16));
+        SS_TRY(ctx->ensure(ctx->offs, n * off_width));
+        SS_TRY(ctx->ensure(ctx->perm, n * 4 * (lcp ? 2 : 1)));
+        SS_TRY(ctx->ensure(ctx->inst, ((size_t)ninst + 1) * 4));
+        uint8_t *d_arena = (uint8_t *)ctx->arena.p;
+        uint32_t *d_perm = (uint32_t *)ctx->perm.p;
+        uint32_t *d_lcp = lcp ? d_perm + n : nullptr;
+        SS_CUDA(cudaMemcpyAsync(d_arena, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->st));
+        SS_CUDA(cudaMemsetAsync(d_arena + arena_bytes, 0, 16, ctx->st));
+        SS_CUDA(cudaMemcpyAsync(ctx->offs.p, offs, n * off_width, cudaMemcpyHostToDevice, ctx->st));
+        SS_CUDA(cudaMemcpyAsync(ctx->inst.p, inst_start, ((size_t)ninst + 1) * 4,
+                                cudaMemcpyHostToDevice, ctx->st));
+        SS_TRY(sort_device_impl(ctx, d_arena, arena_bytes + 16, ctx->offs.p, off_width, n, d_perm,
+                                d_lcp, (const uint32_t *)ctx->inst.p, ninst));
+        SS_CUDA(cudaMemcpyAsync(perm, d_perm, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        if (lcp) SS_CUDA(cudaMemcpyAsync(lcp, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        SS_CUDA(cudaStreamSynchronize(ctx->st));
+        return SSORT_OK;
     });
 }
 

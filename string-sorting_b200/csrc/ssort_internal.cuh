@@ -198,6 +198,11 @@ void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L
                      cudaStream_t st);
 void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
                         cudaStream_t st);
+// Batches: one round-0 segment per instance; instance-local result indices.
+void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
+                       Counters *c, cudaStream_t st);
+void launch_localize(uint32_t *perm, uint32_t n, const uint32_t *inst_start, uint32_t ninst,
+                     cudaStream_t st);
 // Single-CTA scans of short per-segment arrays (out*[n] = totals).
 void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,
                       uint32_t n, cudaStream_t st);

@@ -565,6 +565,36 @@ __global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *W1, Seg 
     }
 }
 
+// ---- batches of independent instances ---------------------------------------
+// Instance i owns positions inst_start[i] .. inst_start[i+1]-1: it enters
+// round 0 as its own segment, and its first LCP entry is 0.
+__global__ void k_init_batch(const uint32_t *__restrict__ inst_start, uint32_t ninst, Seg *R,
+                             uint32_t *lcp, Counters *c) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool v = i < ninst;
+    const uint32_t s = v ? inst_start[i] : 0, e = v ? inst_start[i + 1] : 0;
+    if (v && e > s) lcp[s] = 0;
+    const bool seg = v && e - s >= 2;
+    const uint32_t slot = warp_append(&c->n_next, seg);
+    if (seg) R[slot] = Seg{s, e - s, 0, 0};
+}
+
+// Global positions -> indices within each position's instance.
+__global__ void k_localize(uint32_t *perm, uint32_t n, const uint32_t *__restrict__ inst_start,
+                           uint32_t ninst) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = ninst;  // largest i with inst_start[i] <= p
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(inst_start + mid) <= p)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        perm[p] -= __ldg(inst_start + lo);
+    }
+}
+
 // ---- single-CTA exclusive scans of short per-segment arrays -----------------
 constexpr int SMALL_SCAN_THREADS = 1024;
 
@@ -1679,6 +1709,18 @@ void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L
                      cudaStream_t st) {
     if (!nR) return;
     k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, W1, W8, S, L, c);
+}
+
+void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
+                       Counters *c, cudaStream_t st) {
+    if (!ninst) return;
+    k_init_batch<<<cdiv(ninst, 256), 256, 0, st>>>(inst_start, ninst, R, lcp, c);
+}
+
+void launch_localize(uint32_t *perm, uint32_t n, const uint32_t *inst_start, uint32_t ninst,
+                     cudaStream_t st) {
+    const uint32_t g = cdiv(n, 256) < 148 * 8 ? cdiv(n, 256) : 148 * 8;
+    k_localize<<<g ? g : 1, 256, 0, st>>>(perm, n, inst_start, ninst);
 }
 
 void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,

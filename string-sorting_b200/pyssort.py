@@ -22,7 +22,7 @@ EXPORTS = (
     "msd_gpu", "ssort_strerror", "ssort_last_error", "ssort_ctx_create", "ssort_ctx_destroy",
     "ssort_sort_device", "ssort_sort_host", "ssort_sort_strings", "ssort_get_stats",
     "ssort_set_profiling", "ssort_get_kernel_times", "ssort_sort_device_noalloc",
-    "ssort_set_param",
+    "ssort_set_param", "ssort_sort_batch_device", "ssort_sort_batch_host",
 )
 SSORT_PARAM_TARGET_BUCKET = 1
 
@@ -88,6 +88,10 @@ def lib():
         L.ssort_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.ssort_set_profiling.argtypes = [vp, i32]
         L.ssort_set_param.argtypes = [vp, i32, ctypes.c_int64]
+        L.ssort_sort_batch_device.argtypes = [vp, vp, u64, vp, i32, u64, vp, ctypes.c_uint32,
+                                              vp, vp, vp]
+        L.ssort_sort_batch_host.argtypes = [vp, vp, u64, vp, i32, u64, vp, ctypes.c_uint32,
+                                            vp, vp]
         L.ssort_get_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p),
                                              ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_uint64), i32]
@@ -161,6 +165,31 @@ class Sorter:
         _check(lib().ssort_sort_device(self._ctx, p(d_arena), int(arena_bytes), p(d_offs),
                                        int(off_width), int(n), p(d_perm), p(d_lcp),
                                        stream))
+
+    def sort_batch_host(self, arena, offs, inst_start, with_lcp=True, perm=None, lcp=None):
+        """Batched sort from host buffers: inst_start (uint32, ninst + 1 entries)
+        splits the offsets into independent instances; perm is instance-local."""
+        arena = np.ascontiguousarray(arena, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs)
+        inst = np.ascontiguousarray(inst_start, dtype=np.uint32)
+        n = offs.shape[0]
+        if perm is None:
+            perm = np.empty(n, dtype=np.uint32)
+        if with_lcp and lcp is None:
+            lcp = np.empty(n, dtype=np.uint32)
+        _check(lib().ssort_sort_batch_host(self._ctx, _ptr(arena), arena.nbytes, _ptr(offs),
+                                           offs.dtype.itemsize, n, _ptr(inst), inst.shape[0] - 1,
+                                           _ptr(perm), _ptr(lcp) if with_lcp else None))
+        return perm, (lcp if with_lcp else None)
+
+    def sort_batch_device(self, d_arena, arena_bytes, d_offs, off_width, n, d_inst, ninst,
+                          d_perm, d_lcp=None, stream=None):
+        """Batched sort of device-resident buffers (torch tensors or pointers)."""
+        def p(x):
+            return x if isinstance(x, int) or x is None else x.data_ptr()
+        _check(lib().ssort_sort_batch_device(self._ctx, p(d_arena), int(arena_bytes), p(d_offs),
+                                             int(off_width), int(n), p(d_inst), int(ninst),
+                                             p(d_perm), p(d_lcp), stream))
 
     def sort_strings(self, strings, with_lcp=False):
         """Pointer-array form: strings is a list of bytes objects (no NULs).
@@ -249,6 +278,9 @@ def wlib():
         W.ssw_gen_zipf_words.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double,
                                          ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64,
                                          pp8, u64p, pp8]
+        W.ssw_gen_instances.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                        ctypes.c_void_p, pp8, u64p, pp8]
         W.ssw_free.argtypes = [ctypes.c_void_p]
         W.ssw_free.restype = None
         W.ssw_uniform_doubles.argtypes = [ctypes.c_uint64, ctypes.c_uint64,
@@ -281,6 +313,60 @@ def gen_urls(n, n_hosts=4096, zipf_s=1.1, seed=2):
 def gen_zipf_words(n, vocab=1_000_000, p_geom=0.15, max_len=24, zipf_s=1.0, seed=3):
     a, nb, o = _gen(wlib().ssw_gen_zipf_words, n, vocab, p_geom, max_len, zipf_s, seed)
     return StringSet(a, nb, o, n)
+
+
+class InstanceSet(StringSet):
+    """Several independent sort instances in one arena; inst_start has
+    ninst + 1 entries (position ranges of the instances)."""
+
+    def __init__(self, arena_ptr, arena_bytes, offs_ptr, n, inst_start, params):
+        super().__init__(arena_ptr, arena_bytes, offs_ptr, n)
+        self.inst_start = inst_start
+        self.params = params  # per instance: (count, max_len, alpha_lo, alpha_size)
+
+
+# Per-instance shapes of the batched workload: alphabets of 4 from 'A', 26
+# from 'a', 95 from ' '; length bounds 8, 32, 128.
+BATCH_ALPHABETS = ((ord("A"), 4), (ord("a"), 26), (ord(" "), 95))
+BATCH_MAX_LENS = (8, 32, 128)
+
+
+def batch_instance_params(ninst, seed, lo=100, hi=2_000_000, key_byte_limit=None):
+    """Instance parameters of the batched workload: string counts log-uniform
+    in [lo, hi], alphabet and length bound drawn uniformly from the sets
+    above.  With key_byte_limit, the list stops once the expected key bytes
+    (count * (mean length + 1)) reach the limit."""
+    import math
+    u = uniform_doubles(3 * ninst, seed)
+    out, total = [], 0.0
+    for k in range(ninst):
+        count = int(round(math.exp(math.log(lo) + u[3 * k] * (math.log(hi) - math.log(lo)))))
+        a_lo, a_sz = BATCH_ALPHABETS[min(2, int(u[3 * k + 1] * 3))]
+        L = BATCH_MAX_LENS[min(2, int(u[3 * k + 2] * 3))]
+        out.append((count, L, a_lo, a_sz))
+        total += count * ((1 + L) / 2 + 1)
+        if key_byte_limit is not None and total >= key_byte_limit:
+            break
+    return out
+
+
+def gen_instances(params, seed=4):
+    """Generate the instances described by batch_instance_params."""
+    k = len(params)
+    counts = np.array([p[0] for p in params], dtype=np.uint64)
+    lens = np.array([p[1] for p in params], dtype=np.uint32)
+    alo = np.array([p[2] for p in params], dtype=np.uint32)
+    asz = np.array([p[3] for p in params], dtype=np.uint32)
+    inst = np.zeros(k + 1, dtype=np.uint32)
+    a = ctypes.c_void_p()
+    o = ctypes.c_void_p()
+    nb = ctypes.c_uint64()
+    rc = wlib().ssw_gen_instances(k, counts.ctypes.data, lens.ctypes.data, alo.ctypes.data,
+                                  asz.ctypes.data, seed, inst.ctypes.data, ctypes.byref(a),
+                                  ctypes.byref(nb), ctypes.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"instance generator failed ({rc})")
+    return InstanceSet(a.value, nb.value, o.value, int(counts.sum()), inst, params)
 
 
 def uniform_doubles(n, seed):

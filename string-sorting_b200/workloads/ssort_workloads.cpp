@@ -106,7 +106,7 @@ int build(uint64_t n, uint64_t seed, F gen, uint8_t **arena_out, uint64_t *bytes
         t.reserve((hi - lo) * 16);
         for (uint64_t i = lo; i < hi; ++i) {
             lo_offs[i - lo] = t.size();
-            gen(rng, t);
+            gen(rng, t, i);
             t.push_back(0);
         }
     }
@@ -153,7 +153,7 @@ int ssw_gen_uniform(uint64_t n, uint32_t min_len, uint32_t max_len, uint32_t alp
     const uint64_t span = (uint64_t)max_len - min_len + 1;
     return build(
         n, seed,
-        [=](Rng &r, std::vector<uint8_t> &t) {
+        [=](Rng &r, std::vector<uint8_t> &t, uint64_t) {
             const uint64_t len = min_len + r.below(span);
             for (uint64_t k = 0; k < len; ++k) t.push_back((uint8_t)(alpha_lo + r.below(alpha_size)));
         },
@@ -179,7 +179,7 @@ int ssw_gen_urls(uint64_t n, uint32_t n_hosts, double zipf_s, uint64_t seed, uin
     static const char alnum[] = "abcdefghijklmnopqrstuvwxyz0123456789";
     return build(
         n, seed,
-        [&](Rng &r, std::vector<uint8_t> &t) {
+        [&](Rng &r, std::vector<uint8_t> &t, uint64_t) {
             static const char pfx[] = "http://";
             t.insert(t.end(), pfx, pfx + 7);
             const std::string &h = hosts[z.draw(r)];
@@ -220,9 +220,40 @@ int ssw_gen_zipf_words(uint64_t n, uint32_t vocab, double p_geom, uint32_t max_l
     Zipf z(vocab, zipf_s);
     return build(
         n, seed,
-        [&](Rng &r, std::vector<uint8_t> &t) {
+        [&](Rng &r, std::vector<uint8_t> &t, uint64_t) {
             const std::string &w = words[z.draw(r)];
             t.insert(t.end(), w.begin(), w.end());
+        },
+        arena, arena_bytes, offs);
+}
+
+// Independent sort instances in one arena (the batched workload): instance
+// k has counts[k] strings of length uniform in [1, max_len[k]] with bytes
+// uniform over alpha_size[k] consecutive values from alpha_lo[k].  String
+// positions run instance after instance; inst_start (ninst + 1 entries,
+// caller-allocated) receives each instance's first position.
+int ssw_gen_instances(uint32_t ninst, const uint64_t *counts, const uint32_t *max_len,
+                      const uint32_t *alpha_lo, const uint32_t *alpha_size, uint64_t seed,
+                      uint32_t *inst_start, uint8_t **arena, uint64_t *arena_bytes,
+                      uint64_t **offs) {
+    std::vector<uint64_t> start(ninst + 1, 0);
+    for (uint32_t k = 0; k < ninst; ++k) {
+        if (max_len[k] == 0 || alpha_size[k] == 0 || alpha_lo[k] == 0 ||
+            alpha_lo[k] + alpha_size[k] > 256)
+            return -2;
+        start[k + 1] = start[k] + counts[k];
+    }
+    const uint64_t n = start[ninst];
+    if (n > 0xFFFFFFFEull) return -2;
+    for (uint32_t k = 0; k <= ninst; ++k) inst_start[k] = (uint32_t)start[k];
+    return build(
+        n, seed,
+        [&](Rng &r, std::vector<uint8_t> &t, uint64_t i) {
+            const uint64_t k =
+                (uint64_t)(std::upper_bound(start.begin(), start.end(), i) - start.begin()) - 1;
+            const uint64_t len = 1 + r.below(max_len[k]);
+            for (uint64_t q = 0; q < len; ++q)
+                t.push_back((uint8_t)(alpha_lo[k] + r.below(alpha_size[k])));
         },
         arena, arena_bytes, offs);
 }
