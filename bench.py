@@ -2,7 +2,7 @@
 """Benchmark of the B200 MSD radix string sort (one JSON line on rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload urls_50m|zipf_words_100m|uniform_1m]
+                  [--workload urls_50m|zipf_words_100m|uniform_1m|batch_c4|serve_c5]
 
 A step is one complete sort of the workload (perm + LCP) from inputs resident
 in HBM.  `value` is strings/s over the whole job; `e2e` repeats the
@@ -45,6 +45,10 @@ DESCRIPTIONS = {
     "batch_c4": "independent instances, counts log-uniform in [100, 2,000,000], alphabet "
                 "{4 from 'A', 26 from 'a', 95 from ' '}, length U[1, L], L in {8, 32, 128}; "
                 "the instance list stops at 1.5e9 expected key bytes; seeds 5 (list), 4 (strings)",
+    "serve_c5": "Poisson request stream swept over 1k-50k req/s; request string counts "
+                "log-uniform in [1,000, 5,000,000], strings as batch_c4; requests drawn from a "
+                "pool of distinct requests in pinned host memory; uint32 offsets; 120 GB arena "
+                "budget",
 }
 
 
@@ -55,11 +59,18 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
-                    choices=sorted(pyssort.WORKLOADS) + ["batch_c4"])
+                    choices=sorted(pyssort.WORKLOADS) + ["batch_c4", "serve_c5"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--target-bucket", type=int, default=0,
                     help="override the partition's wanted strings per range bucket")
+    ap.add_argument("--serve-requests", type=int, default=1000,
+                    help="requests per arrival rate of the serve_c5 sweep")
+    ap.add_argument("--serve-rates", default="1000,2000,5000,10000,20000,50000")
+    ap.add_argument("--serve-pool", type=int, default=64,
+                    help="distinct requests the serve_c5 stream draws from")
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
+    ap.add_argument("--serve-max-strings", type=int, default=1 << 26)
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the workload's string count (profiling runs only; "
                          "the reported workload is the full one at 1.0)")
@@ -421,6 +432,208 @@ def run_batch(args):
     }
 
 
+# ---- serving: Poisson request stream ------------------------------------------------
+class RequestPool:
+    """Distinct sort requests in pinned host memory: string counts log-uniform
+    in [1,000, 5,000,000], strings as in the batched workload.  Each request's
+    bytes start 16-byte aligned in one arena; its uint32 offsets are relative
+    to that start; perm/lcp output buffers per request."""
+
+    def __init__(self, npool, seed=6):
+        import torch
+        params = pyssort.batch_instance_params(npool, seed, lo=1000, hi=5_000_000)
+        ss = pyssort.gen_instances(params, seed=seed + 1)
+        spans = []
+        for i in range(len(params)):
+            lo, hi = int(ss.inst_start[i]), int(ss.inst_start[i + 1])
+            a0 = int(ss.offs[lo])
+            a1 = int(ss.offs[hi]) if hi < ss.n else ss.text_bytes
+            spans.append((lo, hi, a0, a1))
+        total = sum((a1 - a0 + 15) // 16 * 16 for _, _, a0, a1 in spans) + 16
+        self.arena = torch.zeros(total, dtype=torch.uint8, pin_memory=True).numpy()
+        u32 = lambda m: torch.empty(max(m, 1), dtype=torch.int32,  # noqa: E731
+                                    pin_memory=True).numpy().view(np.uint32)
+        self.offs, self.perm, self.lcp = u32(ss.n), u32(ss.n), u32(ss.n)
+        self.reqs = []
+        at = 0
+        for lo, hi, a0, a1 in spans:
+            nb = a1 - a0
+            self.arena[at:at + nb] = ss.arena[a0:a1]
+            self.offs[lo:hi] = ss.offs[lo:hi] - np.uint64(a0)
+            self.reqs.append({"at": at, "nb": nb, "lo": lo, "m": hi - lo})
+            at += (nb + 15) // 16 * 16
+        self.n = ss.n
+        self.key_bytes = ss.text_bytes
+        self.dev = None
+
+    def host(self, k):
+        r = self.reqs[k]
+        lo, m = r["lo"], r["m"]
+        return (self.arena[r["at"]:r["at"] + r["nb"]], self.offs[lo:lo + m],
+                self.perm[lo:lo + m], self.lcp[lo:lo + m])
+
+    def to_device(self):
+        """Device copies of the pool (inputs resident in HBM) plus device
+        output buffers; returns base addresses."""
+        import torch
+        d_arena = torch.from_numpy(self.arena).cuda()
+        d_offs = torch.from_numpy(self.offs.view(np.int32)).cuda()
+        d_perm = torch.empty_like(d_offs)
+        d_lcp = torch.empty_like(d_offs)
+        self.dev = (d_arena, d_offs, d_perm, d_lcp)
+        return [t.data_ptr() for t in self.dev]
+
+    def device(self, k):
+        a, o, p, c = [t.data_ptr() for t in self.dev]
+        r = self.reqs[k]
+        lo = r["lo"]
+        return a + r["at"], r["nb"], o + 4 * lo, r["m"], p + 4 * lo, c + 4 * lo
+
+
+def _arrivals(nreq, rate, npool, seed):
+    u = pyssort.uniform_doubles(2 * nreq, seed)
+    gaps = -np.log1p(-u[:nreq]) / rate
+    t = np.cumsum(gaps)
+    t -= t[0]
+    picks = np.minimum((u[nreq:] * npool).astype(np.int64), npool - 1)
+    return t, picks
+
+
+def _wait_until(t0, t):
+    while True:
+        d = t - (time.perf_counter() - t0)
+        if d <= 0:
+            return
+        time.sleep(d if d > 2e-3 else 0)
+
+
+def _lat_summary(lat_s, strings, span_s, key_bytes):
+    a = np.asarray(lat_s) * 1e3
+    return {"p50_ms": round(float(np.percentile(a, 50)), 3),
+            "p99_ms": round(float(np.percentile(a, 99)), 3),
+            "p999_ms": round(float(np.percentile(a, 99.9)), 3),
+            "max_ms": round(float(a.max()), 3),
+            "strings_per_s": strings / span_s, "key_gbs": round(key_bytes / span_s / 1e9, 2),
+            "req_per_s": round(len(a) / span_s, 1), "span_s": round(span_s, 3)}
+
+
+def serve_stream(srv, pool, arrivals, picks, resident=False):
+    """Open-loop stream through the request server: each request is submitted
+    at its arrival time; latency runs from arrival to the step that reports
+    it done (results in host memory, or in device memory when resident)."""
+    n = len(arrivals)
+    lat = np.zeros(n)
+    owner = {}
+    nxt = done = strings = kb = 0
+    t0 = time.perf_counter()
+    while done < n:
+        now = time.perf_counter() - t0
+        while nxt < n and arrivals[nxt] <= now:
+            k = picks[nxt]
+            if resident:
+                a, nb, o, m, p, c = pool.device(k)
+                rid = srv.submit_ptr(a, nb, o, 4, m, p, c)
+            else:
+                a, o, p, c = pool.host(k)
+                rid, _, _ = srv.submit(a, o, perm=p, lcp=c)
+            owner[rid] = nxt
+            nxt += 1
+        ids = srv.step()
+        t = time.perf_counter() - t0
+        for rid in ids:
+            k = owner.pop(rid)
+            lat[k] = t - arrivals[k]
+            r = pool.reqs[picks[k]]
+            strings += r["m"]
+            kb += r["nb"]
+            done += 1
+        if not ids and nxt < n and not owner:
+            _wait_until(t0, arrivals[nxt])
+    span = time.perf_counter() - t0
+    return _lat_summary(lat, strings, span, kb)
+
+
+def plain_stream(sorter, pool, arrivals, picks, resident=False):
+    """The same stream through the plain entry points, one request at a time
+    in arrival order: ssort_sort_host (copy in, sort, copy out), or
+    ssort_sort_device on the resident copy."""
+    n = len(arrivals)
+    lat = np.zeros(n)
+    strings = kb = 0
+    t0 = time.perf_counter()
+    for j in range(n):
+        _wait_until(t0, arrivals[j])
+        k = picks[j]
+        if resident:
+            a, nb, o, m, p, c = pool.device(k)
+            sorter.sort_device(a, nb, o, 4, m, p, c)
+        else:
+            a, o, p, c = pool.host(k)
+            sorter.sort_host(a, o, perm=p, lcp=c)
+        lat[j] = time.perf_counter() - t0 - arrivals[j]
+        r = pool.reqs[k]
+        strings += r["m"]
+        kb += r["nb"]
+    span = time.perf_counter() - t0
+    return _lat_summary(lat, strings, span, kb)
+
+
+def run_serve(args):
+    import torch
+    torch.cuda.set_device(0)
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
+    pool = RequestPool(args.serve_pool)
+    pool.to_device()
+    budget = int(args.serve_budget_gb * 1e9)
+    srv = pyssort.Server(budget, args.serve_max_strings)
+    sorter = pyssort.Sorter(0)
+    # warm-up: every pool request once through each path, largest first so
+    # that the plain context's buffers reach their final size
+    order = np.array(sorted(range(len(pool.reqs)), key=lambda k: -pool.reqs[k]["m"]))
+    w_arr = np.zeros(len(order))
+    for _ in range(max(1, args.warmup)):
+        for resident in (False, True):
+            serve_stream(srv, pool, w_arr, order, resident)
+    for resident in (False, True):
+        plain_stream(sorter, pool, w_arr, order, resident)
+    clocks = Clocks(0)
+    clocks.start()
+    sweeps = {}
+    for resident in (False, True):
+        rows = []
+        for i, rate in enumerate(rates):
+            arr, picks = _arrivals(args.serve_requests, rate, len(pool.reqs), 100 + i)
+            served = serve_stream(srv, pool, arr, picks, resident)
+            plain = plain_stream(sorter, pool, arr, picks, resident)
+            rows.append({"rate_req_s": rate, "served": served, "plain": plain,
+                         "served_vs_plain": round(served["strings_per_s"] /
+                                                  plain["strings_per_s"], 2)})
+        sweeps["resident" if resident else "host"] = rows
+    clocks.stop()
+    info = srv.info()
+    srv.close()
+    best_h = max(sweeps["host"], key=lambda r: r["served"]["strings_per_s"])
+    best_d = max(sweeps["resident"], key=lambda r: r["served"]["strings_per_s"])
+    return {
+        "metric": "served sort throughput (strings/s) with p50/p99/p99.9 latency",
+        "value": best_d["served"]["strings_per_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": args.serve_requests, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
+        "config": {"workload": "serve_c5", "description": DESCRIPTIONS["serve_c5"],
+                   "requests_per_rate": args.serve_requests, "pool_requests": len(pool.reqs),
+                   "pool_strings": pool.n, "pool_key_bytes": pool.key_bytes,
+                   "arena_budget_bytes": budget, "max_strings": args.serve_max_strings,
+                   "parallelism": "single",
+                   "l2": "inputs larger than L2 (pool of requests, GBs)"},
+        "e2e": {"value": best_h["served"]["strings_per_s"], "unit": UNIT,
+                "note": "requests from pinned host buffers; copies in and out inside each "
+                        "request's latency"},
+        "sweep_resident": sweeps["resident"], "sweep_host": sweeps["host"],
+        "server": info, "clocks": clocks.summary(),
+    }
+
 def _ref_lib():
     p = os.path.join(ROOT, "oracle", "_ref", "libref.so")
     if not os.path.exists(p):
@@ -510,9 +723,10 @@ def main():
         if out is not None:
             print(json.dumps(out), flush=True)
         return
-    if args.workload == "batch_c4":
+    if args.workload in ("batch_c4", "serve_c5"):
         if rank == 0:
-            print(json.dumps(run_batch(args)), flush=True)
+            fn = run_batch if args.workload == "batch_c4" else run_serve
+            print(json.dumps(fn(args)), flush=True)
         return
     dist = None
     if world > 1:

@@ -165,6 +165,64 @@ int ssort_set_profiling(ssort_ctx *ctx, int enabled);
 int ssort_get_kernel_times(const ssort_ctx *ctx, const char **names, double *total_ms,
                            uint64_t *launches, int max);
 
+/* ---- request server (continuous batching) ----------------------------------
+ * No reference counterpart: the reference sorts one pointer array per call.
+ * A server owns one device: a pool arena of arena_budget_bytes for the
+ * strings of admitted requests and per-string state for max_strings
+ * positions.  Requests are submitted from host buffers and queued; each
+ * ssort_server_step admits queued requests in FIFO order while their bytes
+ * (arena_bytes + 1, rounded up to 256) and strings fit the free pool and
+ * position ranges, starts their copies on a copy stream, joins the requests
+ * whose copies have landed into the running segment list as depth-0
+ * segments, runs ONE refinement round over the segments of every joined
+ * request together, and starts the device-to-host copy of each request that
+ * has no segment left.  Requests therefore enter and leave the batch between
+ * rounds.  Each result is exactly what ssort_sort_host returns for the same
+ * request alone: perm local to the request, lcp[0] = 0.
+ *
+ * The caller's arena, offs, perm_out and lcp_out may be host memory or
+ * device memory of the server's device (copies use unified addressing); they
+ * must stay valid and the inputs unmodified until the request is reported
+ * done.  Pinned host memory lets host copies overlap the rounds.  A server is not shared between
+ * threads without outside locking; every call takes its lock. */
+typedef struct ssort_server ssort_server;
+
+#define SSORT_REQ_QUEUED 0   /* submitted, waiting for pool space */
+#define SSORT_REQ_LOADING 1  /* admitted, host-to-device copy in flight */
+#define SSORT_REQ_ACTIVE 2   /* segments in the running batch */
+#define SSORT_REQ_DRAINING 3 /* sorted, device-to-host copy in flight */
+#define SSORT_REQ_DONE 4     /* perm_out / lcp_out written */
+
+typedef struct {
+    uint32_t queued, loading, active, draining; /* requests per state */
+    uint32_t max_active;                        /* most requests joined at once */
+    uint64_t rounds;                            /* rounds run */
+    uint64_t requests_done, strings_done;       /* completed so far */
+    uint64_t arena_in_use, strings_in_use;      /* pool bytes / positions held */
+    uint64_t arena_budget, max_strings;         /* capacities */
+    uint64_t device_bytes;                      /* device memory held */
+} ssort_server_info;
+
+int ssort_server_create(int device, uint64_t arena_budget_bytes, uint64_t max_strings,
+                        ssort_server **out);
+void ssort_server_destroy(ssort_server *srv);
+/* Queues one request (n strings at arena + offs[i], offsets of off_width 4 or
+ * 8 bytes).  SSORT_ENOMEM when it could never fit the server's capacities.
+ * lcp_out may be NULL.  n == 0 completes at once. */
+int ssort_server_submit(ssort_server *srv, const uint8_t *arena, uint64_t arena_bytes,
+                        const void *offs, int off_width, uint64_t n, uint32_t *perm_out,
+                        uint32_t *lcp_out, uint64_t *id_out);
+/* One scheduling step (see above).  Writes up to cap ids of requests that
+ * completed since the last report into done_ids and their count into *n_done;
+ * the rest are reported by later steps. */
+int ssort_server_step(ssort_server *srv, uint64_t *done_ids, uint32_t cap, uint32_t *n_done);
+/* State (SSORT_REQ_*) of request id. */
+int ssort_server_poll(ssort_server *srv, uint64_t id, int *state);
+/* Steps until every submitted request is done; completions are still
+ * reported by the next ssort_server_step calls. */
+int ssort_server_drain(ssort_server *srv);
+int ssort_server_get_info(ssort_server *srv, ssort_server_info *out);
+
 #ifdef __cplusplus
 }
 #endif

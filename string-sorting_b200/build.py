@@ -59,8 +59,9 @@ def _run(cmd, cwd=None):
 
 
 def build_cuda(force=False, extra_flags=()):
-    srcs = [os.path.join(CSRC, f) for f in ("ssort_kernels.cu", "ssort_engine.cu")]
-    deps = srcs + [os.path.join(CSRC, "ssort_internal.cuh"), os.path.join(INCLUDE, "ssort_b200.h")]
+    srcs = [os.path.join(CSRC, f) for f in ("ssort_kernels.cu", "ssort_engine.cu", "ssort_server.cu")]
+    deps = srcs + [os.path.join(CSRC, h) for h in ("ssort_internal.cuh", "ssort_host.cuh")]
+    deps.append(os.path.join(INCLUDE, "ssort_b200.h"))
     if not force and not _newer(LIB, deps):
         return LIB
     nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")

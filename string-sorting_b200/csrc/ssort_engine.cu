@@ -3,8 +3,7 @@
 // C ABI declared in include/ssort_b200.h (including the drop-in routine
 // msd_gpu that registers through the reference's ROUTINE_REGISTER,
 // src/routine.h:41-59).
-#include "ssort_b200.h"
-#include "ssort_internal.cuh"
+#include "ssort_host.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -19,164 +18,17 @@
 using namespace ssort;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
-int fail(int code, const std::string &msg) {
+int ssort::fail(int code, const std::string &msg) {
     g_last_error = msg;
     return code;
 }
 
-int cuda_fail(cudaError_t e, const char *what) {
+int ssort::cuda_fail(cudaError_t e, const char *what) {
     return fail(SSORT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-#define SS_CUDA(call)                                        \
-    do {                                                     \
-        cudaError_t e_ = (call);                             \
-        if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
-    } while (0)
-
-#define SS_TRY(call)                 \
-    do {                             \
-        int r_ = (call);             \
-        if (r_ != SSORT_OK) return r_; \
-    } while (0)
-
-struct DBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-};
-
-struct HBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-};
-
-}  // namespace
-
-struct ssort_ctx {
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t st = nullptr;
-
-    // workspace
-    DBuf ws_buf;    // one block holding every scratch buffer (ws_layout)
-    Workspace ws{};
-    size_t ws_n = 0;  // string capacity ws is laid out for
-    DBuf arena, offs, perm, inst;  // staging for the host-buffer entry points
-    HBuf h_offs, h_arena, h_perm;
-    Counters *h_ctr = nullptr;
-
-    ssort_stats stats{};
-    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
-
-    bool prof = false;
-    uint32_t target_bucket = TARGET_BUCKET;  // tuning: wanted strings per range bucket
-    struct Rec {
-        const char *name;
-        cudaEvent_t a, b;
-    };
-    std::vector<Rec> recs;
-    std::vector<cudaEvent_t> ev_pool;
-    size_t ev_used = 0;
-    std::map<std::string, std::pair<double, uint64_t>> ktimes;
-
-    int ensure(DBuf &b, size_t bytes) {
-        if (b.cap >= bytes) return SSORT_OK;
-        if (b.p) cudaFree(b.p);
-        b.p = nullptr;
-        b.cap = 0;
-        size_t want = std::max<size_t>(bytes, 256);
-        cudaError_t e = cudaMalloc(&b.p, want);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            b.p = nullptr;
-            return fail(SSORT_ENOMEM, "device allocation of " + std::to_string(want) +
-                                          " bytes failed: " + cudaGetErrorString(e));
-        }
-        b.cap = want;
-        return SSORT_OK;
-    }
-
-    int ensure_host(HBuf &b, size_t bytes) {
-        if (b.cap >= bytes) return SSORT_OK;
-        if (b.p) cudaFreeHost(b.p);
-        b.p = nullptr;
-        b.cap = 0;
-        cudaError_t e = cudaHostAlloc(&b.p, std::max<size_t>(bytes, 256), cudaHostAllocDefault);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            b.p = nullptr;
-            return fail(SSORT_ENOMEM, "pinned host allocation failed");
-        }
-        b.cap = std::max<size_t>(bytes, 256);
-        return SSORT_OK;
-    }
-
-    cudaEvent_t pool_event() {
-        if (ev_used == ev_pool.size()) {
-            cudaEvent_t e;
-            cudaEventCreate(&e);
-            ev_pool.push_back(e);
-        }
-        return ev_pool[ev_used++];
-    }
-
-    void prof_begin(const char *name) {
-        if (!prof) return;
-        Rec r{name, pool_event(), pool_event()};
-        cudaEventRecord(r.a, st);
-        recs.push_back(r);
-    }
-    void prof_end() {
-        if (!prof) return;
-        cudaEventRecord(recs.back().b, st);
-    }
-    void prof_collect() {
-        for (auto &r : recs) {
-            float ms = 0;
-            cudaEventElapsedTime(&ms, r.a, r.b);
-            auto &slot = ktimes[r.name];
-            slot.first += ms;
-            slot.second += 1;
-        }
-        recs.clear();
-        ev_used = 0;
-    }
-
-    int check_launch(const char *name) {
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(e, name);
-        return SSORT_OK;
-    }
-
-    int sync_counters() {
-        SS_CUDA(cudaMemcpyAsync(h_ctr, ws.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
-        SS_CUDA(cudaStreamSynchronize(st));
-        return SSORT_OK;
-    }
-
-    int grid_for(int per_sm) const { return num_sms * per_sm; }
-
-    int reserve(uint32_t n);
-    int scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev);
-    int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
-            uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
-            uint32_t ninst = 0);
-    int run_ws(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
-               uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
-               uint32_t ninst = 0);
-};
-
-#define LAUNCH(ctx, name, call)                 \
-    do {                                        \
-        (ctx)->prof_begin(name);                \
-        call;                                   \
-        (ctx)->prof_end();                      \
-        SS_TRY((ctx)->check_launch(name));      \
-    } while (0)
 
 int ssort_ctx::reserve(uint32_t n) {
     if (ws_buf.p && n <= ws_n) return SSORT_OK;
@@ -195,12 +47,88 @@ int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const ui
     return SSORT_OK;
 }
 
-// The round loop.  Every position's final index lands in d_perm (= idx[0]);
-// every lcp entry is written exactly once: inside an on-chip sort or an
-// equality bucket for pairs in the same leaf, by the boundary pass for pairs
-// split by a partition, and lcp[0] = 0 up front.  The host waits for the
-// device twice per round (segment counts after classification, and the
-// next round's count) plus once per partition level.
+// One refinement round over the n_cur segments in `cur`: classification,
+// key gather and sample partitioning of large segments, on-chip sorts,
+// equality buckets and boundary LCPs.  The next round's segments are
+// appended to `nxt`; their count is returned in n_next.
+int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint32_t &n_next,
+                     uint32_t round_no) {
+    Counters *dc = ws.ctr;
+    const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
+    SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+    LAUNCH(this, "classify",
+           launch_classify(cur, n_cur, ws.W1, ws.W8, ws.S, ws.L, dc,
+                           st));
+    SS_TRY(sync_counters());
+    if (round_no < SSORT_MAX_ROUNDS) stats.live[round_no] = h_ctr->live_next;
+    uint32_t n_large = h_ctr->n_large;
+    Seg *lcur = ws.L, *lnext = ws.L2;
+    if (n_large) {
+        // Keys of the large segments at this depth.
+        LAUNCH(this, "seg_tiles",
+               launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));
+        LAUNCH(this, "gather",
+               launch_gather(a, lcur, n_large, ws.tile_base, g8, st));
+    }
+    uint32_t levels_this_round = 0;
+    while (n_large) {
+        // Every level strictly shrinks each range bucket (its splitter keys
+        // leave for equality buckets), so this bound is never reached on
+        // valid input; it turns a logic error into a status, not a hang.
+        if (++levels_this_round > 4096)
+            return fail(SSORT_EINTERNAL, "partition levels exceeded 4096");
+        stats.partition_levels++;
+        LAUNCH(this, "sample",
+               launch_sample(a, lcur, n_large, ws.spl, ws.nspl,
+                             ws.tbl, ws.ntiles, ws.cm_size,
+                             st));
+        LAUNCH(this, "scan_pair",
+               launch_scan_pair(ws.ntiles, ws.tile_base, ws.cm_size, ws.cm_base, n_large,
+                                st));
+        LAUNCH(this, "count",
+               launch_count(a, lcur, n_large, ws.tile_base,
+                            ws.spl, ws.nspl,
+                            ws.tbl, ws.cm_base,
+                            ws.cm, g2, st));
+        SS_TRY(scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
+                    ws.cm_base + n_large));
+        LAUNCH(this, "scatter",
+               launch_scatter(a, lcur, n_large, ws.tile_base,
+                              ws.spl, ws.nspl,
+                              ws.tbl, ws.cm_base,
+                              ws.cm, g2, st));
+        LAUNCH(this, "emit",
+               launch_emit(a, lcur, n_large, ws.tile_base,
+                           ws.nspl, ws.cm_base,
+                           ws.cm, ws.W1, ws.W8, ws.S, lnext,
+                           ws.E, ws.B, nxt, dc, st));
+        SS_TRY(sync_counters());
+        n_large = h_ctr->n_large_next;
+        SS_CUDA(cudaMemsetAsync(&dc->n_large_next, 0, 4, st));
+        std::swap(lcur, lnext);
+    }
+    LAUNCH(this, "warp1", launch_warp1(a, ws.W1, nxt, dc, g8, st));
+    LAUNCH(this, "warp8", launch_warp8(a, ws.W8, nxt, dc, g8, st));
+    LAUNCH(this, "block", launch_block(a, ws.S, nxt, dc, g8, st));
+    LAUNCH(this, "equal", launch_equal(a, ws.E, nxt, dc, g8, st));
+    LAUNCH(this, "boundary", launch_boundary(a, ws.B, dc, g4, st));
+    SS_TRY(sync_counters());
+    stats.small_segments += h_ctr->n_w1 + h_ctr->n_w8 + h_ctr->n_small;
+    stats.partitioned += h_ctr->partitioned;
+    stats.gather_elems += h_ctr->gather_elems;
+    stats.warp1_fresh += h_ctr->warp1_fresh;
+    stats.warp1_keyed += h_ctr->warp1_keyed;
+    stats.warp8_fresh += h_ctr->warp8_fresh;
+    stats.warp8_keyed += h_ctr->warp8_keyed;
+    stats.block_fresh += h_ctr->block_fresh;
+    stats.block_keyed += h_ctr->block_keyed;
+    stats.equal_moved += h_ctr->equal_moved;
+    stats.equal_final += h_ctr->equal_final;
+    stats.boundaries += h_ctr->n_bound;
+    n_next = h_ctr->n_next;
+    return SSORT_OK;
+}
+
 int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
                    int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp,
                    const uint32_t *d_inst, uint32_t ninst) {
@@ -208,9 +136,14 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
     return run_ws(arena_p, arena_bytes, offs_p, off_width, n, d_perm, d_lcp, d_inst, ninst);
 }
 
-// The round loop over an already laid-out workspace `ws`.  With an instance
-// table (d_inst, ninst > 0) every instance starts as its own round-0 segment
-// and the result indices are made instance-local at the end.
+// The round loop over an already laid-out workspace `ws`.  Every position's
+// final index lands in d_perm (= idx[0]); every lcp entry is written exactly
+// once: inside an on-chip sort or an equality bucket for pairs in the same
+// leaf, by the boundary pass for pairs split by a partition, and lcp[0] = 0 up
+// front.  The host waits for the device twice per round (segment counts after
+// classification, and the next round's count) plus once per partition level.
+// With an instance table (d_inst, ninst > 0) every instance starts as its own
+// round-0 segment and the result indices are made instance-local at the end.
 int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
                       int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp,
                       const uint32_t *d_inst, uint32_t ninst) {
@@ -244,87 +177,15 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
         Seg first{0, n, 0, 0};
         SS_CUDA(cudaMemcpyAsync(cur, &first, sizeof(Seg), cudaMemcpyHostToDevice, st));
     }
-    uint64_t live = n;
-    uint32_t round = 0;
-    const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
-
+    uint32_t round_no = 0;
     while (n_cur) {
-        SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
-        LAUNCH(this, "classify",
-               launch_classify(cur, n_cur, ws.W1, ws.W8, ws.S, ws.L, dc,
-                               st));
-        SS_TRY(sync_counters());
-        live = h_ctr->live_next;  // strings in this round's segments
-        if (round < SSORT_MAX_ROUNDS) stats.live[round] = live;
-        uint32_t n_large = h_ctr->n_large;
-        Seg *lcur = ws.L, *lnext = ws.L2;
-        if (n_large) {
-            // Keys of the large segments at this depth.
-            LAUNCH(this, "seg_tiles",
-                   launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));
-            LAUNCH(this, "gather",
-                   launch_gather(a, lcur, n_large, ws.tile_base, g8, st));
-        }
-        uint32_t levels_this_round = 0;
-        while (n_large) {
-            // Every level strictly shrinks each range bucket (its splitter keys
-            // leave for equality buckets), so this bound is never reached on
-            // valid input; it turns a logic error into a status, not a hang.
-            if (++levels_this_round > 4096)
-                return fail(SSORT_EINTERNAL, "partition levels exceeded 4096");
-            stats.partition_levels++;
-            LAUNCH(this, "sample",
-                   launch_sample(a, lcur, n_large, ws.spl, ws.nspl,
-                                 ws.tbl, ws.ntiles, ws.cm_size,
-                                 st));
-            LAUNCH(this, "scan_pair",
-                   launch_scan_pair(ws.ntiles, ws.tile_base, ws.cm_size, ws.cm_base, n_large,
-                                    st));
-            LAUNCH(this, "count",
-                   launch_count(a, lcur, n_large, ws.tile_base,
-                                ws.spl, ws.nspl,
-                                ws.tbl, ws.cm_base,
-                                ws.cm, g2, st));
-            SS_TRY(scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
-                        ws.cm_base + n_large));
-            LAUNCH(this, "scatter",
-                   launch_scatter(a, lcur, n_large, ws.tile_base,
-                                  ws.spl, ws.nspl,
-                                  ws.tbl, ws.cm_base,
-                                  ws.cm, g2, st));
-            LAUNCH(this, "emit",
-                   launch_emit(a, lcur, n_large, ws.tile_base,
-                               ws.nspl, ws.cm_base,
-                               ws.cm, ws.W1, ws.W8, ws.S, lnext,
-                               ws.E, ws.B, nxt, dc, st));
-            SS_TRY(sync_counters());
-            n_large = h_ctr->n_large_next;
-            SS_CUDA(cudaMemsetAsync(&dc->n_large_next, 0, 4, st));
-            std::swap(lcur, lnext);
-        }
-        LAUNCH(this, "warp1", launch_warp1(a, ws.W1, nxt, dc, g8, st));
-        LAUNCH(this, "warp8", launch_warp8(a, ws.W8, nxt, dc, g8, st));
-        LAUNCH(this, "block", launch_block(a, ws.S, nxt, dc, g8, st));
-        LAUNCH(this, "equal", launch_equal(a, ws.E, nxt, dc, g8, st));
-        LAUNCH(this, "boundary", launch_boundary(a, ws.B, dc, g4, st));
-        SS_TRY(sync_counters());
-        stats.small_segments += h_ctr->n_w1 + h_ctr->n_w8 + h_ctr->n_small;
-        stats.partitioned += h_ctr->partitioned;
-        stats.gather_elems += h_ctr->gather_elems;
-        stats.warp1_fresh += h_ctr->warp1_fresh;
-        stats.warp1_keyed += h_ctr->warp1_keyed;
-        stats.warp8_fresh += h_ctr->warp8_fresh;
-        stats.warp8_keyed += h_ctr->warp8_keyed;
-        stats.block_fresh += h_ctr->block_fresh;
-        stats.block_keyed += h_ctr->block_keyed;
-        stats.equal_moved += h_ctr->equal_moved;
-        stats.equal_final += h_ctr->equal_final;
-        stats.boundaries += h_ctr->n_bound;
-        n_cur = h_ctr->n_next;
+        uint32_t n_next = 0;
+        SS_TRY(round(a, cur, n_cur, nxt, n_next, round_no));
+        n_cur = n_next;
         std::swap(cur, nxt);
-        ++round;
+        ++round_no;
     }
-    stats.rounds = round;
+    stats.rounds = round_no;
     if (d_inst) LAUNCH(this, "localize", launch_localize(d_perm, n, d_inst, ninst, st));
     return SSORT_OK;
 }
@@ -364,17 +225,6 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
         held += b->cap;
     ctx->stats.device_bytes = held;
     return SSORT_OK;
-}
-
-// Run fn with the context's device current, restoring the caller's device.
-template <class F>
-int with_device(ssort_ctx *ctx, F fn) {
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) cudaSetDevice(ctx->device);
-    int rc = fn();
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
-    return rc;
 }
 
 // Readable mappings of this process, for the drop-in's one-span fast path.

@@ -1,0 +1,180 @@
+// ssort_host.cuh -- host-side context shared by the sort engine and the
+// request server: the device workspace, the stream the kernels run on, the
+// per-kernel profiling records, status helpers and the LAUNCH macro.
+#pragma once
+#include "ssort_b200.h"
+#include "ssort_internal.cuh"
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace ssort {
+
+// Records msg as this thread's last error (ssort_last_error) and returns code.
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+struct DBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+struct HBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace ssort
+
+#define SS_CUDA(call)                                               \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return ssort::cuda_fail(e_, #call);  \
+    } while (0)
+
+#define SS_TRY(call)                   \
+    do {                               \
+        int r_ = (call);               \
+        if (r_ != SSORT_OK) return r_; \
+    } while (0)
+
+struct ssort_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t st = nullptr;
+
+    // workspace
+    ssort::DBuf ws_buf;    // one block holding every scratch buffer (ws_layout)
+    ssort::Workspace ws{};
+    size_t ws_n = 0;  // string capacity ws is laid out for
+    ssort::DBuf arena, offs, perm, inst;  // staging for the host-buffer entry points
+    ssort::HBuf h_offs, h_arena, h_perm;
+    ssort::Counters *h_ctr = nullptr;
+
+    ssort_stats stats{};
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+
+    bool prof = false;
+    uint32_t target_bucket = ssort::TARGET_BUCKET;  // tuning: wanted strings per range bucket
+    struct Rec {
+        const char *name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::map<std::string, std::pair<double, uint64_t>> ktimes;
+
+    int ensure(ssort::DBuf &b, size_t bytes) {
+        if (b.cap >= bytes) return SSORT_OK;
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&b.p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return ssort::fail(SSORT_ENOMEM, "device allocation of " + std::to_string(want) +
+                                          " bytes failed: " + cudaGetErrorString(e));
+        }
+        b.cap = want;
+        return SSORT_OK;
+    }
+
+    int ensure_host(ssort::HBuf &b, size_t bytes) {
+        if (b.cap >= bytes) return SSORT_OK;
+        if (b.p) cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        cudaError_t e = cudaHostAlloc(&b.p, std::max<size_t>(bytes, 256), cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return ssort::fail(SSORT_ENOMEM, "pinned host allocation failed");
+        }
+        b.cap = std::max<size_t>(bytes, 256);
+        return SSORT_OK;
+    }
+
+    cudaEvent_t pool_event() {
+        if (ev_used == ev_pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
+
+    void prof_begin(const char *name) {
+        if (!prof) return;
+        Rec r{name, pool_event(), pool_event()};
+        cudaEventRecord(r.a, st);
+        recs.push_back(r);
+    }
+    void prof_end() {
+        if (!prof) return;
+        cudaEventRecord(recs.back().b, st);
+    }
+    void prof_collect() {
+        for (auto &r : recs) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            auto &slot = ktimes[r.name];
+            slot.first += ms;
+            slot.second += 1;
+        }
+        recs.clear();
+        ev_used = 0;
+    }
+
+    int check_launch(const char *name) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return ssort::cuda_fail(e, name);
+        return SSORT_OK;
+    }
+
+    int sync_counters() {
+        SS_CUDA(cudaMemcpyAsync(h_ctr, ws.ctr, sizeof(ssort::Counters), cudaMemcpyDeviceToHost, st));
+        SS_CUDA(cudaStreamSynchronize(st));
+        return SSORT_OK;
+    }
+
+    int grid_for(int per_sm) const { return num_sms * per_sm; }
+
+    int reserve(uint32_t n);
+    int scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev);
+    int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
+            uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
+            uint32_t ninst = 0);
+    int round(const ssort::SortArgs &a, ssort::Seg *cur, uint32_t n_cur, ssort::Seg *nxt,
+              uint32_t &n_next,
+              uint32_t round_no);
+    int run_ws(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
+               uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
+               uint32_t ninst = 0);
+};
+
+#define LAUNCH(ctx, name, call)                 \
+    do {                                        \
+        (ctx)->prof_begin(name);                \
+        call;                                   \
+        (ctx)->prof_end();                      \
+        SS_TRY((ctx)->check_launch(name));      \
+    } while (0)
+
+
+// Run fn with the context's device current, restoring the caller's device.
+template <class F>
+inline int with_device(ssort_ctx *ctx, F fn) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ctx->device) cudaSetDevice(ctx->device);
+    int rc = fn();
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    return rc;
+}
+

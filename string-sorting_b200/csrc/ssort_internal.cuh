@@ -201,6 +201,12 @@ void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *ou
 // Batches: one round-0 segment per instance; instance-local result indices.
 void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
                        Counters *c, cudaStream_t st);
+void launch_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, uint32_t pos_base, uint32_t n,
+                 uint64_t region_base, uint64_t arena_bytes, int off_width, Seg *R, uint32_t slot,
+                 cudaStream_t st);
+void launch_mark(const Seg *R, uint32_t nR, const uint32_t *base, uint32_t nact, uint32_t *flag,
+                 cudaStream_t st);
+void launch_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n, cudaStream_t st);
 void launch_localize(uint32_t *perm, uint32_t n, const uint32_t *inst_start, uint32_t ninst,
                      cudaStream_t st);
 // Single-CTA scans of short per-segment arrays (out*[n] = totals).

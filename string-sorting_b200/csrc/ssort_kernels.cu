@@ -64,7 +64,8 @@ __device__ __forceinline__ Key load_key(const uint8_t *__restrict__ arena, uint6
     uint64_t w0, w1;  // little-endian: byte 0 of w0 is arena[pos]
     const uint64_t a = pos & ~15ull;
     const uint32_t off = (uint32_t)(pos & 15);
-    if (a + 32 <= arena_bytes) {
+    // (no a + 32 here: an offset near 2^64 must not wrap into the fast path)
+    if (arena_bytes >= 32 && a <= arena_bytes - 32) {
         const ulonglong2 v0 = __ldg(reinterpret_cast<const ulonglong2 *>(arena + a));
         if (off == 0) {
             w0 = v0.x;
@@ -593,6 +594,56 @@ __global__ void k_localize(uint32_t *perm, uint32_t n, const uint32_t *__restric
         }
         perm[p] -= __ldg(inst_start + lo);
     }
+}
+
+// ---- request server: joining and retiring requests between rounds ----------
+// Joins one admitted request at positions [pos_base, pos_base + n) whose bytes
+// sit at region_base in the pool arena.  Its offsets arrive either as uint64
+// in place in goffs or as uint32 staged in lcp at its positions; each becomes
+// a pool offset.  An offset at or past the request's own arena_bytes is
+// clamped to arena_bytes, where the server stores a NUL byte: the same empty
+// string the single-request sort reads past the end of its arena.  Positions
+// get their identity index, lcp of the first position becomes 0, and the
+// request's positions become one depth-0 segment at R[slot].
+__global__ void k_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, uint32_t pos_base,
+                       uint32_t n, uint64_t region_base, uint64_t arena_bytes, int off_width,
+                       Seg *R, uint32_t slot) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const uint32_t p = pos_base + i;
+        uint64_t o = off_width == 4 ? (uint64_t)lcp[p] : goffs[p];
+        if (o > arena_bytes) o = arena_bytes;
+        goffs[p] = region_base + o;
+        perm[p] = p;
+        if (i == 0) lcp[p] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n >= 2) R[slot] = Seg{pos_base, n, 0, 0};
+}
+
+// flag[j] = 1 for every active request j that still owns a segment of R;
+// base[] holds the active requests' first positions in ascending order.
+__global__ void k_mark(const Seg *__restrict__ R, uint32_t nR, const uint32_t *__restrict__ base,
+                       uint32_t nact, uint32_t *flag) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nR;
+         i += gridDim.x * blockDim.x) {
+        const uint32_t s = R[i].start;
+        uint32_t lo = 0, hi = nact;  // largest j with base[j] <= s
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(base + mid) <= s)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        flag[lo] = 1;
+    }
+}
+
+// Global positions of one finished request -> indices within the request.
+__global__ void k_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        perm[pos_base + i] -= pos_base;
 }
 
 // ---- single-CTA exclusive scans of short per-segment arrays -----------------
@@ -1721,6 +1772,27 @@ void launch_localize(uint32_t *perm, uint32_t n, const uint32_t *inst_start, uin
                      cudaStream_t st) {
     const uint32_t g = cdiv(n, 256) < 148 * 8 ? cdiv(n, 256) : 148 * 8;
     k_localize<<<g ? g : 1, 256, 0, st>>>(perm, n, inst_start, ninst);
+}
+
+void launch_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, uint32_t pos_base, uint32_t n,
+                 uint64_t region_base, uint64_t arena_bytes, int off_width, Seg *R, uint32_t slot,
+                 cudaStream_t st) {
+    const uint32_t g = cdiv(n, 256) < 148 * 8 ? cdiv(n, 256) : 148 * 8;
+    k_join<<<g ? g : 1, 256, 0, st>>>(goffs, lcp, perm, pos_base, n, region_base, arena_bytes,
+                                      off_width, R, slot);
+}
+
+void launch_mark(const Seg *R, uint32_t nR, const uint32_t *base, uint32_t nact, uint32_t *flag,
+                 cudaStream_t st) {
+    if (!nR || !nact) return;
+    const uint32_t g = cdiv(nR, 256) < 148 * 8 ? cdiv(nR, 256) : 148 * 8;
+    k_mark<<<g, 256, 0, st>>>(R, nR, base, nact, flag);
+}
+
+void launch_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n, cudaStream_t st) {
+    if (!n) return;
+    const uint32_t g = cdiv(n, 256) < 148 * 8 ? cdiv(n, 256) : 148 * 8;
+    k_unbase<<<g, 256, 0, st>>>(perm, pos_base, n);
 }
 
 void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,

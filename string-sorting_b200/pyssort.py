@@ -23,7 +23,11 @@ EXPORTS = (
     "ssort_sort_device", "ssort_sort_host", "ssort_sort_strings", "ssort_get_stats",
     "ssort_set_profiling", "ssort_get_kernel_times", "ssort_sort_device_noalloc",
     "ssort_set_param", "ssort_sort_batch_device", "ssort_sort_batch_host",
+    "ssort_server_create", "ssort_server_destroy", "ssort_server_submit", "ssort_server_step",
+    "ssort_server_poll", "ssort_server_drain", "ssort_server_get_info",
 )
+# request states reported by ssort_server_poll
+REQ_QUEUED, REQ_LOADING, REQ_ACTIVE, REQ_DRAINING, REQ_DONE = range(5)
 SSORT_PARAM_TARGET_BUCKET = 1
 
 
@@ -61,6 +65,27 @@ class Stats(ctypes.Structure):
         return d
 
 
+class ServerInfo(ctypes.Structure):
+    _fields_ = [
+        ("queued", ctypes.c_uint32),
+        ("loading", ctypes.c_uint32),
+        ("active", ctypes.c_uint32),
+        ("draining", ctypes.c_uint32),
+        ("max_active", ctypes.c_uint32),
+        ("rounds", ctypes.c_uint64),
+        ("requests_done", ctypes.c_uint64),
+        ("strings_done", ctypes.c_uint64),
+        ("arena_in_use", ctypes.c_uint64),
+        ("strings_in_use", ctypes.c_uint64),
+        ("arena_budget", ctypes.c_uint64),
+        ("max_strings", ctypes.c_uint64),
+        ("device_bytes", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
 _lib = None
 _wlib = None
 
@@ -95,6 +120,16 @@ def lib():
         L.ssort_get_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p),
                                              ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_uint64), i32]
+        L.ssort_server_create.argtypes = [i32, u64, u64, ctypes.POINTER(vp)]
+        L.ssort_server_destroy.argtypes = [vp]
+        L.ssort_server_destroy.restype = None
+        L.ssort_server_submit.argtypes = [vp, vp, u64, vp, i32, u64, vp, vp,
+                                          ctypes.POINTER(u64)]
+        L.ssort_server_step.argtypes = [vp, ctypes.POINTER(u64), ctypes.c_uint32,
+                                        ctypes.POINTER(ctypes.c_uint32)]
+        L.ssort_server_poll.argtypes = [vp, u64, ctypes.POINTER(i32)]
+        L.ssort_server_drain.argtypes = [vp]
+        L.ssort_server_get_info.argtypes = [vp, ctypes.POINTER(ServerInfo)]
         L.msd_gpu.argtypes = [vp, ctypes.c_size_t]
         L.msd_gpu.restype = None
         _lib = L
@@ -225,6 +260,99 @@ class Sorter:
         return {names[i].decode(): (ms[i], cnt[i]) for i in range(k)}
 
 
+class Server:
+    """Request server: sort requests from host buffers, batched between rounds
+    (ssort_server_* in include/ssort_b200.h).  The buffers of each request are
+    kept referenced here until the request is reported done."""
+
+    def __init__(self, arena_budget, max_strings, device=0):
+        self._srv = ctypes.c_void_p()
+        _check(lib().ssort_server_create(int(device), int(arena_budget), int(max_strings),
+                                         ctypes.byref(self._srv)))
+        self._held = {}
+        self._ids = (ctypes.c_uint64 * 4096)()
+
+    def close(self):
+        if self._srv:
+            lib().ssort_server_destroy(self._srv)
+            self._srv = ctypes.c_void_p()
+            self._held.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, arena, offs, perm=None, lcp=None, with_lcp=True):
+        """Queue one request; returns (id, perm, lcp) with perm/lcp filled once
+        the request is done.  arena (uint8) and offs (uint32/uint64) are numpy
+        arrays, ideally in pinned memory."""
+        arena = np.ascontiguousarray(arena, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs)
+        if offs.dtype not in (np.uint32, np.uint64):
+            raise TypeError("offsets must be uint32 or uint64")
+        n = offs.shape[0]
+        if perm is None:
+            perm = np.empty(n, dtype=np.uint32)
+        if with_lcp and lcp is None:
+            lcp = np.empty(n, dtype=np.uint32)
+        rid = ctypes.c_uint64()
+        _check(lib().ssort_server_submit(self._srv, _ptr(arena), arena.nbytes, _ptr(offs),
+                                         offs.dtype.itemsize, n, _ptr(perm),
+                                         _ptr(lcp) if with_lcp else None, ctypes.byref(rid)))
+        self._held[rid.value] = (arena, offs, perm, lcp)
+        return rid.value, perm, (lcp if with_lcp else None)
+
+    def submit_ptr(self, arena, arena_bytes, offs, off_width, n, perm, lcp=None):
+        """Queue one request given raw addresses or torch tensors, in host
+        memory or in device memory of the server's device; returns its id."""
+        def p(x):
+            return x if isinstance(x, int) or x is None else x.data_ptr()
+        rid = ctypes.c_uint64()
+        _check(lib().ssort_server_submit(self._srv, p(arena), int(arena_bytes), p(offs),
+                                         int(off_width), int(n), p(perm), p(lcp),
+                                         ctypes.byref(rid)))
+        self._held[rid.value] = (arena, offs, perm, lcp)
+        return rid.value
+
+    def step(self):
+        """One scheduling step; returns the ids completed since the last step."""
+        k = ctypes.c_uint32()
+        _check(lib().ssort_server_step(self._srv, self._ids, len(self._ids), ctypes.byref(k)))
+        done = [int(self._ids[i]) for i in range(k.value)]
+        for rid in done:
+            self._held.pop(rid, None)
+        return done
+
+    def poll(self, rid):
+        st = ctypes.c_int()
+        _check(lib().ssort_server_poll(self._srv, int(rid), ctypes.byref(st)))
+        return st.value
+
+    def drain(self):
+        """Run until every submitted request is done; returns their ids."""
+        _check(lib().ssort_server_drain(self._srv))
+        done = []
+        while True:
+            got = self.step()
+            if not got:
+                break
+            done += got
+        return done
+
+    def info(self):
+        i = ServerInfo()
+        _check(lib().ssort_server_get_info(self._srv, ctypes.byref(i)))
+        return i.as_dict()
+
+
 # ---- synthetic workloads ------------------------------------------------------
 class StringSet:
     """An arena of NUL-terminated strings plus uint64 offsets, owned by the
@@ -323,6 +451,16 @@ class InstanceSet(StringSet):
         super().__init__(arena_ptr, arena_bytes, offs_ptr, n)
         self.inst_start = inst_start
         self.params = params  # per instance: (count, max_len, alpha_lo, alpha_size)
+
+    def request(self, i, off_dtype=np.uint32):
+        """Instance i as a stand-alone request: (arena view, offsets relative
+        to it).  The instance's strings are contiguous in the shared arena."""
+        lo, hi = int(self.inst_start[i]), int(self.inst_start[i + 1])
+        if hi == lo:
+            return self.arena[:0], np.zeros(0, dtype=off_dtype)
+        a0 = int(self.offs[lo])
+        a1 = int(self.offs[hi]) if hi < self.n else self.text_bytes
+        return self.arena[a0:a1], (self.offs[lo:hi] - np.uint64(a0)).astype(off_dtype)
 
 
 # Per-instance shapes of the batched workload: alphabets of 4 from 'A', 26

@@ -61,3 +61,26 @@ def test_null_context_is_rejected():
     assert L.ssort_sort_host(None, None, 0, None, 8, 0, None, None) == -1
     assert L.ssort_sort_device(None, None, 0, None, 8, 0, None, None, None) == -1
     assert L.ssort_set_profiling(None, 1) == -1
+
+
+def test_server_without_device_is_reported():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pyssort.SsortError) as e:
+        pyssort.Server(1 << 20, 1000)
+    assert e.value.status == -4
+
+
+def test_null_server_is_rejected():
+    import ctypes
+    L = pyssort.lib()
+    rid = ctypes.c_uint64()
+    st = ctypes.c_int()
+    assert L.ssort_server_submit(None, None, 0, None, 8, 0, None, None, ctypes.byref(rid)) == -1
+    assert L.ssort_server_step(None, None, 0, None) == -1
+    assert L.ssort_server_poll(None, 1, ctypes.byref(st)) == -1
+    assert L.ssort_server_drain(None) == -1
+    L.ssort_server_destroy(None)
+    out = ctypes.c_void_p()
+    assert L.ssort_server_create(0, 1 << 20, 0, ctypes.byref(out)) == -1
