@@ -129,6 +129,42 @@ int ssort_sort_batch_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_b
  * of the sorted order. */
 int ssort_sort_strings(ssort_ctx *ctx, unsigned char **strings, size_t n, uint32_t *lcp_out);
 
+/*
+ * Text inputs: the strings of a whole input file, as the reference's
+ * sortstring makes them (src/sortstring.c:310-358), found on the GPU instead
+ * of by a host pass that builds a pointer array.
+ *   SSORT_TEXT_LINES     every '\n' ends a string and becomes its NUL
+ *                        (create_strings_delim with '\n', the default mode);
+ *   SSORT_TEXT_RAW       every NUL ends a string (--raw);
+ *   SSORT_TEXT_SUFFIXES  every position starts a string: all suffixes of the
+ *                        text (--suffix-sorting, create_suffixes).
+ * In the delimited modes the string after the last delimiter is not a string
+ * (as in the reference).  Bytes at or past text_len read as NUL.
+ *
+ * ssort_text_offsets_device writes the string starts into d_offs (width 4 or
+ * 8; width 4 needs text_len < 2^32) on `stream` and returns their number in
+ * *n_out.  With SSORT_TEXT_LINES it overwrites the '\n' bytes of d_text with
+ * NUL.  When the strings would exceed cap entries it writes nothing, sets
+ * *n_out to the number needed and returns SSORT_EINVAL.
+ *
+ * ssort_sort_text_host sorts the strings of a host text: sorted_offs[k] is the
+ * start (offset into text) of the k-th smallest string; lcp (optional) as for
+ * every sort.  Capacity and *n_out as above.  The host text is not modified.
+ */
+#define SSORT_TEXT_LINES 0
+#define SSORT_TEXT_RAW 1
+#define SSORT_TEXT_SUFFIXES 2
+int ssort_text_offsets_device(ssort_ctx *ctx, uint8_t *d_text, uint64_t text_len, int mode,
+                              void *d_offs, int off_width, uint64_t cap, uint64_t *n_out,
+                              void *stream);
+int ssort_sort_text_host(ssort_ctx *ctx, const uint8_t *text, uint64_t text_len, int mode,
+                         uint64_t *sorted_offs, uint32_t *lcp, uint64_t cap, uint64_t *n_out);
+
+/* Page-locked host memory (for reading inputs straight into a buffer that the
+ * copy engines read at full speed); freed with ssort_pinned_free. */
+int ssort_pinned_alloc(size_t bytes, void **out);
+void ssort_pinned_free(void *p);
+
 /* Per-call statistics of the last sort on this context. */
 typedef struct {
     uint64_t n;                              /* strings sorted */

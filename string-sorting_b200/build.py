@@ -24,6 +24,7 @@ REF_DIR = os.environ.get("SSORT_REF_DIR", "/root/reference")
 
 LIB = os.path.join(PKG, "libssort_b200.so")
 WLIB = os.path.join(PKG, "libssort_workloads.so")
+CLI = os.path.join(PKG, "ssort-sort")
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -95,9 +96,22 @@ def build_oracle(force=False):
         _run(env_cmd + ["-j8", "REF_DIR=" + REF_DIR, "ref", "ref-bins"])
 
 
+def build_cli(force=False):
+    """ssort-sort: the whole-file command-line front end (links the library)."""
+    src = os.path.join(PKG, "cli", "ssort_cli.cpp")
+    if not force and not _newer(CLI, [src, LIB, os.path.join(INCLUDE, "ssort_b200.h")]):
+        return CLI
+    tmp = CLI + ".tmp"
+    _run([_host_cxx(), "-O2", "-std=c++17", "-I", INCLUDE, src, "-o", tmp, "-L", PKG,
+          "-lssort_b200", "-Wl,-rpath,$ORIGIN"])
+    os.replace(tmp, CLI)
+    return CLI
+
+
 def build_all(force=False):
     build_cuda(force)
     build_workloads(force)
+    build_cli(force)
     build_oracle(force)
 
 

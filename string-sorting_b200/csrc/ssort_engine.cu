@@ -221,7 +221,8 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
     ctx->stats.device_ms = ms;
     if (ctx->prof) ctx->prof_collect();
     size_t held = 0;
-    for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst})
+    for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst, &ctx->aux,
+                     &ctx->aux2})
         held += b->cap;
     ctx->stats.device_bytes = held;
     return SSORT_OK;
@@ -301,7 +302,8 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
     if (!ctx) return;
     with_device(ctx, [&]() -> int {
         if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
-        for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst})
+        for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst, &ctx->aux,
+                     &ctx->aux2})
             if (b->p) cudaFree(b->p);
         for (HBuf *b : {&ctx->h_offs, &ctx->h_arena, &ctx->h_perm})
             if (b->p) cudaFreeHost(b->p);
@@ -571,6 +573,156 @@ void msd_gpu(unsigned char **strings, size_t n) {
         std::fprintf(stderr, "msd_gpu: %s: %s\n", ssort_strerror(rc), ssort_last_error());
         std::abort();
     }
+}
+
+}  // extern "C"
+
+// ---- text inputs ---------------------------------------------------------------
+namespace {
+
+// Count phase of the delimited modes: per-tile delimiter counts (kept in
+// ctx->aux for the write phase) and their total.
+int text_count(ssort_ctx *ctx, const uint8_t *d_text, uint64_t len, uint8_t delim,
+               uint64_t *n_out) {
+    const uint64_t tiles = text_tiles(len);
+    *n_out = 0;
+    if (!tiles) return SSORT_OK;
+    if (tiles >= 0xFFFFFFF0ull) return fail(SSORT_EINVAL, "text too long");
+    const uint32_t nt = (uint32_t)tiles;
+    const size_t parts = scan_partials_needed(nt);
+    SS_TRY(ctx->ensure(ctx->aux, 256 + ((size_t)nt + 1) * 4 + 256 + parts * 4));
+    unsigned long long *d_total = (unsigned long long *)ctx->aux.p;
+    uint32_t *d_tiles = (uint32_t *)((unsigned char *)ctx->aux.p + 256);
+    SS_CUDA(cudaMemsetAsync(d_total, 0, 8, ctx->st));
+    LAUNCH(ctx, "text_count", launch_text_count(d_text, len, delim, d_tiles, d_total, ctx->st));
+    unsigned long long total = 0;
+    SS_CUDA(cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, ctx->st));
+    SS_CUDA(cudaStreamSynchronize(ctx->st));
+    *n_out = total;
+    return SSORT_OK;
+}
+
+// Write phase: string starts from the scanned tile counts of text_count.
+int text_write(ssort_ctx *ctx, uint8_t *d_text, uint64_t len, uint8_t delim, uint64_t n,
+               void *d_offs, int off_width) {
+    const uint32_t nt = (uint32_t)text_tiles(len);
+    uint32_t *d_tiles = (uint32_t *)((unsigned char *)ctx->aux.p + 256);
+    uint32_t *d_parts =
+        (uint32_t *)((unsigned char *)ctx->aux.p + 256 + (((size_t)nt + 1) * 4 + 255) / 256 * 256);
+    LAUNCH(ctx, "scan", launch_scan(d_tiles, d_tiles, nt, nullptr, d_parts, ctx->st));
+    LAUNCH(ctx, "text_starts",
+           launch_text_starts(d_text, len, delim, d_tiles, n, d_offs, off_width, ctx->st));
+    return SSORT_OK;
+}
+
+int text_check(ssort_ctx *ctx, uint64_t text_len, int mode, int off_width, uint64_t *n_out) {
+    if (!ctx) return fail(SSORT_EINVAL, "null context");
+    if (!n_out) return fail(SSORT_EINVAL, "null count pointer");
+    if (mode != SSORT_TEXT_LINES && mode != SSORT_TEXT_RAW && mode != SSORT_TEXT_SUFFIXES)
+        return fail(SSORT_EINVAL, "unknown text mode");
+    if (off_width != 4 && off_width != 8) return fail(SSORT_EINVAL, "off_width must be 4 or 8");
+    if (off_width == 4 && text_len >= (1ull << 32))
+        return fail(SSORT_EINVAL, "4-byte offsets need a text shorter than 2^32 bytes");
+    return SSORT_OK;
+}
+
+int text_fits(uint64_t n, uint64_t cap) {
+    if (n > SSORT_MAX_N) return fail(SSORT_EINVAL, "text holds more strings than SSORT_MAX_N");
+    if (n > cap)
+        return fail(SSORT_EINVAL, "offset capacity too small: the text holds " +
+                                      std::to_string(n) + " strings");
+    return SSORT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ssort_text_offsets_device(ssort_ctx *ctx, uint8_t *d_text, uint64_t text_len, int mode,
+                              void *d_offs, int off_width, uint64_t cap, uint64_t *n_out,
+                              void *stream) {
+    SS_TRY(text_check(ctx, text_len, mode, off_width, n_out));
+    *n_out = 0;
+    if (!text_len) return SSORT_OK;
+    if (!d_text || !d_offs) return fail(SSORT_EINVAL, "null device buffer");
+    if (((uintptr_t)d_text & 15) != 0) return fail(SSORT_EINVAL, "text must be 16-byte aligned");
+    return with_device(ctx, [&]() -> int {
+        ctx->st = stream ? (cudaStream_t)stream : ctx->own_stream;
+        int rc = [&]() -> int {
+            if (mode == SSORT_TEXT_SUFFIXES) {
+                *n_out = text_len;
+                SS_TRY(text_fits(text_len, cap));
+                LAUNCH(ctx, "iota_offs", launch_iota_offs(d_offs, off_width, text_len, ctx->st));
+                return SSORT_OK;
+            }
+            const uint8_t delim = mode == SSORT_TEXT_LINES ? '\n' : 0;
+            uint64_t n = 0;
+            SS_TRY(text_count(ctx, d_text, text_len, delim, &n));
+            *n_out = n;
+            SS_TRY(text_fits(n, cap));
+            if (n) SS_TRY(text_write(ctx, d_text, text_len, delim, n, d_offs, off_width));
+            return SSORT_OK;
+        }();
+        ctx->st = ctx->own_stream;
+        return rc;
+    });
+}
+
+int ssort_pinned_alloc(size_t bytes, void **out) {
+    if (!out) return fail(SSORT_EINVAL, "null output pointer");
+    *out = nullptr;
+    cudaError_t e = cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return fail(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? SSORT_ENODEV
+                                                                             : SSORT_ENOMEM,
+                    std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
+    }
+    return SSORT_OK;
+}
+
+void ssort_pinned_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+
+int ssort_sort_text_host(ssort_ctx *ctx, const uint8_t *text, uint64_t text_len, int mode,
+                         uint64_t *sorted_offs, uint32_t *lcp, uint64_t cap, uint64_t *n_out) {
+    const int w = text_len < (1ull << 32) ? 4 : 8;
+    SS_TRY(text_check(ctx, text_len, mode, w, n_out));
+    *n_out = 0;
+    if (!text_len) return SSORT_OK;
+    if (!text) return fail(SSORT_EINVAL, "null text");
+    return with_device(ctx, [&]() -> int {
+        ctx->st = ctx->own_stream;
+        SS_TRY(ctx->ensure(ctx->arena, text_len + 16));
+        uint8_t *d_text = (uint8_t *)ctx->arena.p;
+        SS_CUDA(cudaMemcpyAsync(d_text, text, text_len, cudaMemcpyHostToDevice, ctx->st));
+        SS_CUDA(cudaMemsetAsync(d_text + text_len, 0, 16, ctx->st));
+        const uint8_t delim = mode == SSORT_TEXT_LINES ? '\n' : 0;
+        uint64_t n = text_len;
+        if (mode != SSORT_TEXT_SUFFIXES) SS_TRY(text_count(ctx, d_text, text_len, delim, &n));
+        *n_out = n;
+        SS_TRY(text_fits(n, cap));
+        if (!n) return SSORT_OK;
+        if (!sorted_offs) return fail(SSORT_EINVAL, "null output buffer");
+        SS_TRY(ctx->ensure(ctx->offs, n * w));
+        if (mode == SSORT_TEXT_SUFFIXES)
+            LAUNCH(ctx, "iota_offs", launch_iota_offs(ctx->offs.p, w, n, ctx->st));
+        else
+            SS_TRY(text_write(ctx, d_text, text_len, delim, n, ctx->offs.p, w));
+        SS_TRY(ctx->ensure(ctx->perm, n * 4 * (lcp ? 2 : 1)));
+        uint32_t *d_perm = (uint32_t *)ctx->perm.p;
+        uint32_t *d_lcp = lcp ? d_perm + n : nullptr;
+        SS_TRY(sort_device_impl(ctx, d_text, text_len + 16, ctx->offs.p, w, n, d_perm, d_lcp));
+        SS_TRY(ctx->ensure(ctx->aux2, n * 8));
+        LAUNCH(ctx, "sorted_offs",
+               launch_sorted_offs(d_perm, ctx->offs.p, w, n, (uint64_t *)ctx->aux2.p, ctx->st));
+        SS_CUDA(cudaMemcpyAsync(sorted_offs, ctx->aux2.p, n * 8, cudaMemcpyDeviceToHost, ctx->st));
+        if (lcp) SS_CUDA(cudaMemcpyAsync(lcp, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        SS_CUDA(cudaStreamSynchronize(ctx->st));
+        return SSORT_OK;
+    });
 }
 
 }  // extern "C"

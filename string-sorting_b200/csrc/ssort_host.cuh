@@ -51,6 +51,7 @@ struct ssort_ctx {
     ssort::Workspace ws{};
     size_t ws_n = 0;  // string capacity ws is laid out for
     ssort::DBuf arena, offs, perm, inst;  // staging for the host-buffer entry points
+    ssort::DBuf aux, aux2;  // text inputs: tile counts + scan partials, sorted offsets
     ssort::HBuf h_offs, h_arena, h_perm;
     ssort::Counters *h_ctr = nullptr;
 

@@ -201,6 +201,14 @@ void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *ou
 // Batches: one round-0 segment per instance; instance-local result indices.
 void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
                        Counters *c, cudaStream_t st);
+uint64_t text_tiles(uint64_t len);  // CTAs (tile counts) of the text kernels
+void launch_text_count(const uint8_t *text, uint64_t len, uint8_t delim, uint32_t *tile_cnt,
+                       unsigned long long *total, cudaStream_t st);
+void launch_text_starts(uint8_t *text, uint64_t len, uint8_t delim, const uint32_t *tile_base,
+                        uint64_t n, void *offs, int off_width, cudaStream_t st);
+void launch_iota_offs(void *offs, int off_width, uint64_t n, cudaStream_t st);
+void launch_sorted_offs(const uint32_t *perm, const void *offs, int off_width, uint64_t n,
+                        uint64_t *out, cudaStream_t st);
 void launch_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, uint32_t pos_base, uint32_t n,
                  uint64_t region_base, uint64_t arena_bytes, int off_width, Seg *R, uint32_t slot,
                  cudaStream_t st);

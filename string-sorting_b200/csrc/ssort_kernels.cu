@@ -646,6 +646,118 @@ __global__ void k_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n) {
         perm[pos_base + i] -= pos_base;
 }
 
+// ---- text inputs: string starts in a delimited text ---------------------------
+// The reference's sortstring turns a file into strings by create_strings_delim
+// (src/sortstring.c:310-335): every delimiter byte ('\n', or NUL with --raw)
+// ends one string, the next string starts right after it, text after the last
+// delimiter is not a string, and '\n' delimiters are overwritten with NUL.
+// Each CTA covers TEXT_TILE bytes, 16 per thread.
+constexpr int TEXT_THREADS = 256;
+constexpr uint64_t TEXT_TILE = TEXT_THREADS * 16;
+
+// Bit b of the result is set when text[base + b] == delim (positions at or
+// past len never match).
+__device__ __forceinline__ uint32_t delim_mask16(const uint8_t *__restrict__ text, uint64_t len,
+                                                 uint64_t base, uint8_t delim) {
+    uint32_t m = 0;
+    if (base + 16 <= len) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(text + base);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+                if (((w[q] >> (8 * b)) & 0xFF) == delim) m |= 1u << (4 * q + b);
+    } else {
+        for (int b = 0; b < 16 && base + b < len; ++b)
+            if (text[base + b] == delim) m |= 1u << b;
+    }
+    return m;
+}
+
+__global__ void __launch_bounds__(TEXT_THREADS)
+    k_text_count(const uint8_t *__restrict__ text, uint64_t len, uint8_t delim,
+                 uint32_t *tile_cnt, unsigned long long *total) {
+    __shared__ uint32_t warp_sums[TEXT_THREADS / 32];
+    const uint64_t base = blockIdx.x * TEXT_TILE + threadIdx.x * 16ull;
+    uint32_t c = __popc(delim_mask16(text, len, base, delim));
+#pragma unroll
+    for (int d = 16; d; d >>= 1) c += __shfl_xor_sync(0xffffffffu, c, d);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < TEXT_THREADS / 32; ++w) t += warp_sums[w];
+        tile_cnt[blockIdx.x] = t;
+        if (t) atomicAdd(total, (unsigned long long)t);
+    }
+}
+
+// tile_base: exclusive prefix of the tile counts; n: total delimiters.  String
+// r + 1 starts right after delimiter r; string 0 starts at 0.
+__global__ void __launch_bounds__(TEXT_THREADS)
+    k_text_starts(uint8_t *text, uint64_t len, uint8_t delim, const uint32_t *__restrict__ tile_base,
+                  uint64_t n, void *offs, int off_width) {
+    __shared__ uint32_t warp_sums[TEXT_THREADS / 32];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t base = blockIdx.x * TEXT_TILE + threadIdx.x * 16ull;
+    uint32_t m = delim_mask16(text, len, base, delim);
+    const uint32_t c = __popc(m);
+    uint32_t v = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= (uint32_t)d) v += y;
+    }
+    if (lane == 31) warp_sums[w] = v;
+    __syncthreads();
+    uint32_t before = 0;
+    for (uint32_t q = 0; q < w; ++q) before += warp_sums[q];
+    uint64_t r = (uint64_t)tile_base[blockIdx.x] + before + v - c;
+    while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        const uint64_t i = base + b;
+        if (r + 1 < n) {
+            if (off_width == 8)
+                static_cast<uint64_t *>(offs)[r + 1] = i + 1;
+            else
+                static_cast<uint32_t *>(offs)[r + 1] = (uint32_t)(i + 1);
+        }
+        if (delim) text[i] = 0;
+        ++r;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n) {
+        if (off_width == 8)
+            static_cast<uint64_t *>(offs)[0] = 0;
+        else
+            static_cast<uint32_t *>(offs)[0] = 0;
+    }
+}
+
+// offs[i] = i: every suffix of the text (sortstring --suffix-sorting,
+// create_suffixes, src/sortstring.c:349-358).
+__global__ void k_iota_offs(void *offs, int off_width, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (off_width == 8)
+            static_cast<uint64_t *>(offs)[i] = i;
+        else
+            static_cast<uint32_t *>(offs)[i] = (uint32_t)i;
+    }
+}
+
+// out[k] = offs[perm[k]]: the sorted string starts.
+__global__ void k_sorted_offs(const uint32_t *__restrict__ perm, const void *offs, int off_width,
+                              uint64_t n, uint64_t *out) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = perm[k];
+        out[k] = off_width == 8 ? static_cast<const uint64_t *>(offs)[i]
+                                : static_cast<const uint32_t *>(offs)[i];
+    }
+}
+
 // ---- single-CTA exclusive scans of short per-segment arrays -----------------
 constexpr int SMALL_SCAN_THREADS = 1024;
 
@@ -1793,6 +1905,33 @@ void launch_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n, cudaStream_t s
     if (!n) return;
     const uint32_t g = cdiv(n, 256) < 148 * 8 ? cdiv(n, 256) : 148 * 8;
     k_unbase<<<g, 256, 0, st>>>(perm, pos_base, n);
+}
+
+uint64_t text_tiles(uint64_t len) { return (len + TEXT_TILE - 1) / TEXT_TILE; }
+
+void launch_text_count(const uint8_t *text, uint64_t len, uint8_t delim, uint32_t *tile_cnt,
+                       unsigned long long *total, cudaStream_t st) {
+    const uint64_t t = text_tiles(len);
+    if (t) k_text_count<<<(unsigned)t, TEXT_THREADS, 0, st>>>(text, len, delim, tile_cnt, total);
+}
+
+void launch_text_starts(uint8_t *text, uint64_t len, uint8_t delim, const uint32_t *tile_base,
+                        uint64_t n, void *offs, int off_width, cudaStream_t st) {
+    const uint64_t t = text_tiles(len);
+    if (t)
+        k_text_starts<<<(unsigned)t, TEXT_THREADS, 0, st>>>(text, len, delim, tile_base, n, offs,
+                                                            off_width);
+}
+
+void launch_iota_offs(void *offs, int off_width, uint64_t n, cudaStream_t st) {
+    const uint64_t g = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
+    k_iota_offs<<<(unsigned)(g ? g : 1), 256, 0, st>>>(offs, off_width, n);
+}
+
+void launch_sorted_offs(const uint32_t *perm, const void *offs, int off_width, uint64_t n,
+                        uint64_t *out, cudaStream_t st) {
+    const uint64_t g = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
+    k_sorted_offs<<<(unsigned)(g ? g : 1), 256, 0, st>>>(perm, offs, off_width, n, out);
 }
 
 void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,

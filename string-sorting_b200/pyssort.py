@@ -25,7 +25,11 @@ EXPORTS = (
     "ssort_set_param", "ssort_sort_batch_device", "ssort_sort_batch_host",
     "ssort_server_create", "ssort_server_destroy", "ssort_server_submit", "ssort_server_step",
     "ssort_server_poll", "ssort_server_drain", "ssort_server_get_info",
+    "ssort_text_offsets_device", "ssort_sort_text_host", "ssort_pinned_alloc",
+    "ssort_pinned_free",
 )
+# text input modes (sortstring's default line mode, --raw, --suffix-sorting)
+TEXT_LINES, TEXT_RAW, TEXT_SUFFIXES = 0, 1, 2
 # request states reported by ssort_server_poll
 REQ_QUEUED, REQ_LOADING, REQ_ACTIVE, REQ_DRAINING, REQ_DONE = range(5)
 SSORT_PARAM_TARGET_BUCKET = 1
@@ -130,6 +134,9 @@ def lib():
         L.ssort_server_poll.argtypes = [vp, u64, ctypes.POINTER(i32)]
         L.ssort_server_drain.argtypes = [vp]
         L.ssort_server_get_info.argtypes = [vp, ctypes.POINTER(ServerInfo)]
+        L.ssort_text_offsets_device.argtypes = [vp, vp, u64, i32, vp, i32, u64,
+                                                ctypes.POINTER(u64), vp]
+        L.ssort_sort_text_host.argtypes = [vp, vp, u64, i32, vp, vp, u64, ctypes.POINTER(u64)]
         L.msd_gpu.argtypes = [vp, ctypes.c_size_t]
         L.msd_gpu.restype = None
         _lib = L
@@ -238,6 +245,34 @@ class Sorter:
         order = [addr[arr[i]] for i in range(n)]
         out = [strings[i] for i in order]
         return (out, lcp) if with_lcp else out
+
+    def sort_text(self, text, mode=TEXT_LINES, with_lcp=True):
+        """Sort the strings of a whole text (bytes or uint8 array) as sortstring
+        makes them; returns (sorted string starts as uint64 offsets, lcp)."""
+        buf = np.frombuffer(text, dtype=np.uint8) if isinstance(text, (bytes, bytearray)) \
+            else np.ascontiguousarray(text, dtype=np.uint8)
+        L = lib()
+        n = ctypes.c_uint64()
+        rc = L.ssort_sort_text_host(self._ctx, _ptr(buf), buf.nbytes, int(mode), None, None, 0,
+                                    ctypes.byref(n))
+        if rc != SSORT_OK and n.value == 0:
+            _check(rc)
+        out = np.empty(n.value, dtype=np.uint64)
+        lcp = np.empty(n.value, dtype=np.uint32) if with_lcp else None
+        _check(L.ssort_sort_text_host(self._ctx, _ptr(buf), buf.nbytes, int(mode), _ptr(out),
+                                      _ptr(lcp), n.value, ctypes.byref(n)))
+        return out, lcp
+
+    def text_offsets_device(self, d_text, text_len, mode, d_offs, off_width, cap, stream=None):
+        """String starts of a device-resident text (torch tensors or
+        addresses); returns the number of strings."""
+        def p(x):
+            return x if isinstance(x, int) or x is None else x.data_ptr()
+        n = ctypes.c_uint64()
+        _check(lib().ssort_text_offsets_device(self._ctx, p(d_text), int(text_len), int(mode),
+                                               p(d_offs), int(off_width), int(cap),
+                                               ctypes.byref(n), stream))
+        return n.value
 
     def stats(self):
         s = Stats()
