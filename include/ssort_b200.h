@@ -160,6 +160,31 @@ int ssort_text_offsets_device(ssort_ctx *ctx, uint8_t *d_text, uint64_t text_len
 int ssort_sort_text_host(ssort_ctx *ctx, const uint8_t *text, uint64_t text_len, int mode,
                          uint64_t *sorted_offs, uint32_t *lcp, uint64_t cap, uint64_t *n_out);
 
+/*
+ * LCP consumers (no counterpart entry point in the reference; the merge is its
+ * mergesort_lcp two-way LCP merge, src/mergesort_lcp.cpp:133-211).
+ *
+ * ssort_merge_runs merges sorted runs on the host using their LCP arrays.
+ * Run r owns positions run_start[r] .. run_start[r+1]-1 (run_start has
+ * nruns + 1 non-decreasing entries from 0 to n); perm/lcp hold each run's
+ * result as the batched sort returns it (indices local to the run, lcp
+ * restarting at 0).  Writes the global order (indices into offs) and its LCP
+ * array: exactly the sort of all n strings in one call.  The outputs may
+ * alias the inputs.  Runs with OpenMP threads.
+ *
+ * ssort_sort_host_chunked sorts n strings with a device workspace sized for
+ * chunk_strings only: the arena is copied once, consecutive chunks of
+ * chunk_strings offsets are sorted on the GPU one after another, and the runs
+ * are merged with ssort_merge_runs.  Results as ssort_sort_host.
+ */
+int ssort_merge_runs(const uint8_t *arena, uint64_t arena_bytes, const void *offs,
+                     int off_width, uint64_t n, const uint32_t *run_start, uint32_t nruns,
+                     const uint32_t *perm, const uint32_t *lcp, uint32_t *out_perm,
+                     uint32_t *out_lcp);
+int ssort_sort_host_chunked(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes,
+                            const void *offs, int off_width, uint64_t n, uint64_t chunk_strings,
+                            uint32_t *perm, uint32_t *lcp);
+
 /* Page-locked host memory (for reading inputs straight into a buffer that the
  * copy engines read at full speed); freed with ssort_pinned_free. */
 int ssort_pinned_alloc(size_t bytes, void **out);

@@ -668,6 +668,48 @@ int ssort_text_offsets_device(ssort_ctx *ctx, uint8_t *d_text, uint64_t text_len
     });
 }
 
+int ssort_sort_host_chunked(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes,
+                            const void *offs, int off_width, uint64_t n, uint64_t chunk_strings,
+                            uint32_t *perm, uint32_t *lcp) {
+    SS_TRY(validate_common(ctx, off_width, n));
+    if (n == 0) return SSORT_OK;
+    if (!arena || !offs || !perm) return fail(SSORT_EINVAL, "null host buffer");
+    if (chunk_strings == 0) return fail(SSORT_EINVAL, "chunk_strings must be positive");
+    const uint64_t chunk = std::min<uint64_t>(chunk_strings, n);
+    const uint64_t runs = (n + chunk - 1) / chunk;
+    std::vector<uint32_t> run_start(runs + 1);
+    for (uint64_t r = 0; r <= runs; ++r) run_start[r] = (uint32_t)std::min(n, r * chunk);
+    std::vector<uint32_t> own_lcp;
+    if (!lcp) {
+        own_lcp.resize(n);
+        lcp = own_lcp.data();
+    }
+    int rc = with_device(ctx, [&]() -> int {
+        ctx->st = ctx->own_stream;
+        SS_TRY(ctx->ensure(ctx->arena, arena_bytes + 16));
+        SS_TRY(ctx->ensure(ctx->offs, chunk * off_width));
+        SS_TRY(ctx->ensure(ctx->perm, chunk * 8));
+        uint8_t *d_arena = (uint8_t *)ctx->arena.p;
+        uint32_t *d_perm = (uint32_t *)ctx->perm.p, *d_lcp = d_perm + chunk;
+        SS_CUDA(cudaMemcpyAsync(d_arena, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->st));
+        SS_CUDA(cudaMemsetAsync(d_arena + arena_bytes, 0, 16, ctx->st));
+        for (uint64_t r = 0; r < runs; ++r) {
+            const uint64_t lo = run_start[r], m = run_start[r + 1] - lo;
+            SS_CUDA(cudaMemcpyAsync(ctx->offs.p, (const uint8_t *)offs + lo * off_width,
+                                    m * off_width, cudaMemcpyHostToDevice, ctx->st));
+            SS_TRY(sort_device_impl(ctx, d_arena, arena_bytes + 16, ctx->offs.p, off_width, m,
+                                    d_perm, d_lcp));
+            SS_CUDA(cudaMemcpyAsync(perm + lo, d_perm, m * 4, cudaMemcpyDeviceToHost, ctx->st));
+            SS_CUDA(cudaMemcpyAsync(lcp + lo, d_lcp, m * 4, cudaMemcpyDeviceToHost, ctx->st));
+        }
+        SS_CUDA(cudaStreamSynchronize(ctx->st));
+        return SSORT_OK;
+    });
+    if (rc != SSORT_OK) return rc;
+    return ssort_merge_runs(arena, arena_bytes, offs, off_width, n, run_start.data(),
+                            (uint32_t)runs, perm, lcp, perm, lcp);
+}
+
 int ssort_pinned_alloc(size_t bytes, void **out) {
     if (!out) return fail(SSORT_EINVAL, "null output pointer");
     *out = nullptr;

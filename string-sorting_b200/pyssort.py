@@ -26,7 +26,7 @@ EXPORTS = (
     "ssort_server_create", "ssort_server_destroy", "ssort_server_submit", "ssort_server_step",
     "ssort_server_poll", "ssort_server_drain", "ssort_server_get_info",
     "ssort_text_offsets_device", "ssort_sort_text_host", "ssort_pinned_alloc",
-    "ssort_pinned_free",
+    "ssort_pinned_free", "ssort_merge_runs", "ssort_sort_host_chunked",
 )
 # text input modes (sortstring's default line mode, --raw, --suffix-sorting)
 TEXT_LINES, TEXT_RAW, TEXT_SUFFIXES = 0, 1, 2
@@ -137,6 +137,12 @@ def lib():
         L.ssort_text_offsets_device.argtypes = [vp, vp, u64, i32, vp, i32, u64,
                                                 ctypes.POINTER(u64), vp]
         L.ssort_sort_text_host.argtypes = [vp, vp, u64, i32, vp, vp, u64, ctypes.POINTER(u64)]
+        L.ssort_merge_runs.argtypes = [vp, u64, vp, i32, u64, vp, ctypes.c_uint32, vp, vp, vp,
+                                       vp]
+        L.ssort_sort_host_chunked.argtypes = [vp, vp, u64, vp, i32, u64, u64, vp, vp]
+        L.ssort_pinned_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
+        L.ssort_pinned_free.argtypes = [vp]
+        L.ssort_pinned_free.restype = None
         L.msd_gpu.argtypes = [vp, ctypes.c_size_t]
         L.msd_gpu.restype = None
         _lib = L
@@ -246,6 +252,19 @@ class Sorter:
         out = [strings[i] for i in order]
         return (out, lcp) if with_lcp else out
 
+    def sort_host_chunked(self, arena, offs, chunk, with_lcp=True):
+        """Sort with a workspace for `chunk` strings: GPU-sorted chunks merged
+        on the host by their LCPs."""
+        arena = np.ascontiguousarray(arena, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs)
+        n = offs.shape[0]
+        perm = np.empty(n, dtype=np.uint32)
+        lcp = np.empty(n, dtype=np.uint32) if with_lcp else None
+        _check(lib().ssort_sort_host_chunked(self._ctx, _ptr(arena), arena.nbytes, _ptr(offs),
+                                             offs.dtype.itemsize, n, int(chunk), _ptr(perm),
+                                             _ptr(lcp)))
+        return perm, lcp
+
     def sort_text(self, text, mode=TEXT_LINES, with_lcp=True):
         """Sort the strings of a whole text (bytes or uint8 array) as sortstring
         makes them; returns (sorted string starts as uint64 offsets, lcp)."""
@@ -293,6 +312,23 @@ class Sorter:
         cnt = (ctypes.c_uint64 * max(k, 1))()
         L.ssort_get_kernel_times(self._ctx, names, ms, cnt, k)
         return {names[i].decode(): (ms[i], cnt[i]) for i in range(k)}
+
+
+def merge_runs(arena, offs, run_start, perm, lcp):
+    """Host LCP merge of sorted runs (ssort_merge_runs): perm/lcp hold each
+    run's run-local result; returns the global (perm, lcp)."""
+    arena = np.ascontiguousarray(arena, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs)
+    rs = np.ascontiguousarray(run_start, dtype=np.uint32)
+    perm = np.ascontiguousarray(perm, dtype=np.uint32)
+    lcp = np.ascontiguousarray(lcp, dtype=np.uint32)
+    n = offs.shape[0]
+    out_p = np.empty(n, dtype=np.uint32)
+    out_l = np.empty(n, dtype=np.uint32)
+    _check(lib().ssort_merge_runs(_ptr(arena), arena.nbytes, _ptr(offs), offs.dtype.itemsize, n,
+                                  _ptr(rs), rs.shape[0] - 1, _ptr(perm), _ptr(lcp),
+                                  _ptr(out_p), _ptr(out_l)))
+    return out_p, out_l
 
 
 class Server:
