@@ -1700,6 +1700,44 @@ __device__ __noinline__ void block_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
     }
 }
 
+// Pairwise merge-path merges of the sorted runs of length run0 in sv[0..span)
+// (span = runs * run0, padded positions) until one run is left; MI outputs
+// per thread and pass (run0 is a multiple of MI, span <= MI * SMALL_THREADS).
+template <int MI>
+__device__ __forceinline__ void block_merge_passes64(uint64_t *sv, uint32_t run0, uint32_t span) {
+    for (uint32_t run = run0; run < span; run <<= 1) {
+        {
+            const uint32_t o = threadIdx.x * MI;
+            uint64_t ov[MI];
+            const bool active = o < span;
+            if (active) {
+                const uint32_t a0 = o / (2 * run) * (2 * run);
+                const uint32_t b0 = a0 + run;
+                const uint32_t la = min(run, span - a0);
+                const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
+                const uint32_t d = o - a0;
+                uint32_t ia = merge_split64(sv, a0, la, b0, lb, d);
+                uint32_t ib = d - ia;
+#pragma unroll
+                for (int i = 0; i < MI; ++i) {
+                    const uint64_t va = ia < la ? sv[pad(a0 + ia)] : ~0ull;
+                    const uint64_t vb = ib < lb ? sv[pad(b0 + ib)] : ~0ull;
+                    const bool take_a = ib >= lb || (ia < la && va < vb);
+                    ov[i] = take_a ? va : vb;
+                    ia += take_a;
+                    ib += !take_a;
+                }
+            }
+            __syncthreads();
+            if (active) {
+#pragma unroll
+                for (int i = 0; i < MI; ++i) sv[pad(o + i)] = ov[i];
+            }
+            __syncthreads();
+        }
+    }
+}
+
 __global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
                                                             Seg *N, Counters *c) {
     extern __shared__ __align__(16) unsigned char block_smem[];
@@ -1770,35 +1808,14 @@ __global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Se
                     warp_run_packed<8>(sk, sv, w * run0, s.len, f, lane);
             }
             __syncthreads();
-            for (uint32_t run = run0; run < span; run <<= 1) {
-                const uint32_t o = threadIdx.x * SMALL_ITEMS;
-                uint64_t ov[SMALL_ITEMS];
-                const bool active = o < span;
-                if (active) {
-                    const uint32_t a0 = o / (2 * run) * (2 * run);
-                    const uint32_t b0 = a0 + run;
-                    const uint32_t la = min(run, span - a0);
-                    const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
-                    const uint32_t d = o - a0;
-                    uint32_t ia = merge_split64(sv, a0, la, b0, lb, d);
-                    uint32_t ib = d - ia;
-#pragma unroll
-                    for (int i = 0; i < SMALL_ITEMS; ++i) {
-                        const uint64_t va = ia < la ? sv[pad(a0 + ia)] : ~0ull;
-                        const uint64_t vb = ib < lb ? sv[pad(b0 + ib)] : ~0ull;
-                        const bool take_a = ib >= lb || (ia < la && va < vb);
-                        ov[i] = take_a ? va : vb;
-                        ia += take_a;
-                        ib += !take_a;
-                    }
-                }
-                __syncthreads();
-                if (active) {
-#pragma unroll
-                    for (int i = 0; i < SMALL_ITEMS; ++i) sv[pad(o + i)] = ov[i];
-                }
-                __syncthreads();
-            }
+            // Each thread writes `items` outputs per pass, so a segment of
+            // span keys keeps span / items threads busy (not span / 8).
+            if (items == 2)
+                block_merge_passes64<2>(sv, run0, span);
+            else if (items == 4)
+                block_merge_passes64<4>(sv, run0, span);
+            else
+                block_merge_passes64<8>(sv, run0, span);
             packed = __syncthreads_and(window_pairs_ok_ind(sk, sv, s.len, threadIdx.x,
                                                            SMALL_THREADS));
             if (!packed) block_sort_full(sk, sx, full_span);
