@@ -160,18 +160,20 @@ class Clocks:
 KB = 16  # key bytes per round
 
 # DRAM bytes (read + write) per string handled, from one ncu capture of a small
-# case of the same kernel (profiles/*.md); scaled by the strings a launch
-# handles to give `roofline.traffic` per launch.
+# case of the same kernel (10 M Zipf words for count and scatter); scaled by
+# the strings a launch handles to give `roofline.traffic` per launch.
 TRAFFIC_PER_STRING = {
-    "count": 16.8,    # profiles/count_scatter_zipf_words_10m.md
-    "scatter": 48.8,  # profiles/count_scatter_zipf_words_10m.md
+    "count": 16.8,
+    "scatter": 48.8,
 }
 
 
 def kernel_strings(st):
     """Strings each kernel handled during one sort (stats counters)."""
     return {
-        "gather": st.gather_elems, "count": st.partitioned, "scatter": st.partitioned,
+        "gather": st.gather_elems - st.gather_fused,
+        "count_gather": st.gather_fused, "count": st.partitioned - st.gather_fused,
+        "scatter": st.partitioned,
         "warp1": st.warp1_fresh + st.warp1_keyed, "warp8": st.warp8_fresh + st.warp8_keyed,
         "block": st.block_fresh + st.block_keyed,
     }
@@ -179,16 +181,18 @@ def kernel_strings(st):
 
 def kernel_bytes(st, w):
     """Algorithmic bytes each kernel must move for one sort, from the per-kernel
-    string counts: gather reads idx (4) + offset (w) + the key bytes and writes
-    the key (16); count reads keys (16); scatter reads and writes key+idx
+    string counts: the first partition level of a round gathers while it
+    counts: it reads idx (4) + offset (w) + the key bytes and writes the key
+    (16); later levels' count reads keys (16); scatter reads and writes key+idx
     (2x20); on-chip sorts read idx (4) + offset (w) + key bytes when they
     gather themselves, or key+idx (20) otherwise, and write idx + lcp (8);
     equality buckets copy idx (8) and/or write lcp (4)."""
     def sort_bytes(fresh, keyed):
         return fresh * (4 + w + KB) + keyed * (KB + 4) + (fresh + keyed) * 8
     return {
-        "gather": st.gather_elems * (4 + w + KB + KB),
-        "count": st.partitioned * KB,
+        "gather": (st.gather_elems - st.gather_fused) * (4 + w + KB + KB),
+        "count_gather": st.gather_fused * (4 + w + KB + KB),
+        "count": (st.partitioned - st.gather_fused) * KB,
         "scatter": st.partitioned * 2 * (KB + 4),
         "warp1": sort_bytes(st.warp1_fresh, st.warp1_keyed),
         "warp8": sort_bytes(st.warp8_fresh, st.warp8_keyed),

@@ -209,6 +209,8 @@ typedef struct {
     uint64_t warp1_fresh, warp1_keyed, warp8_fresh, warp8_keyed, block_fresh, block_keyed;
     uint64_t equal_moved, equal_final;
     uint64_t boundaries;
+    uint64_t gather_fused; /* of gather_elems: keys gathered by the first
+                              partition level's count kernel (rounds >= 1) */
 } ssort_stats;
 
 int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);

@@ -63,12 +63,15 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
     if (round_no < SSORT_MAX_ROUNDS) stats.live[round_no] = h_ctr->live_next;
     uint32_t n_large = h_ctr->n_large;
     Seg *lcur = ws.L, *lnext = ws.L2;
-    if (n_large) {
-        // Keys of the large segments at this depth.
+    // Keys of the large segments at this depth.  In round 0 the indices are
+    // the identity, so a separate gather streams the arena in order; later
+    // rounds read it at random, and the count kernel of the first partition
+    // level gathers the keys itself so that those reads overlap its work.
+    const bool fused_gather = round_no > 0;
+    if (n_large && !fused_gather) {
         LAUNCH(this, "seg_tiles",
                launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));
-        LAUNCH(this, "gather",
-               launch_gather(a, lcur, n_large, ws.tile_base, g8, st));
+        LAUNCH(this, "gather", launch_gather(a, lcur, n_large, ws.tile_base, g8, st));
     }
     uint32_t levels_this_round = 0;
     while (n_large) {
@@ -78,18 +81,16 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
         if (++levels_this_round > 4096)
             return fail(SSORT_EINTERNAL, "partition levels exceeded 4096");
         stats.partition_levels++;
+        const bool first = fused_gather && levels_this_round == 1;
         LAUNCH(this, "sample",
-               launch_sample(a, lcur, n_large, ws.spl, ws.nspl,
-                             ws.tbl, ws.ntiles, ws.cm_size,
-                             st));
+               launch_sample(a, lcur, n_large, ws.spl, ws.nspl, ws.tbl, ws.ntiles, ws.cm_size,
+                             first, st));
         LAUNCH(this, "scan_pair",
                launch_scan_pair(ws.ntiles, ws.tile_base, ws.cm_size, ws.cm_base, n_large,
                                 st));
-        LAUNCH(this, "count",
-               launch_count(a, lcur, n_large, ws.tile_base,
-                            ws.spl, ws.nspl,
-                            ws.tbl, ws.cm_base,
-                            ws.cm, g2, st));
+        LAUNCH(this, first ? "count_gather" : "count",
+               launch_count(a, lcur, n_large, ws.tile_base, ws.spl, ws.nspl, ws.tbl, ws.cm_base,
+                            ws.cm, first, g2, st));
         SS_TRY(scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
                     ws.cm_base + n_large));
         LAUNCH(this, "scatter",
@@ -116,6 +117,7 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
     stats.small_segments += h_ctr->n_w1 + h_ctr->n_w8 + h_ctr->n_small;
     stats.partitioned += h_ctr->partitioned;
     stats.gather_elems += h_ctr->gather_elems;
+    if (fused_gather) stats.gather_fused += h_ctr->gather_elems;
     stats.warp1_fresh += h_ctr->warp1_fresh;
     stats.warp1_keyed += h_ctr->warp1_keyed;
     stats.warp8_fresh += h_ctr->warp8_fresh;

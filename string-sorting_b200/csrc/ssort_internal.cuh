@@ -228,12 +228,15 @@ void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint3
 uint32_t scan_partials_needed(uint32_t n);
 void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                    int grid, cudaStream_t st);
+// from_arena / gather: first partition level of a round, whose keys the
+// count kernel gathers from the arena (the sample reads its strings there).
 void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl,
                    uint32_t *nspl, uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size,
-                   cudaStream_t st);
+                   bool from_arena, cudaStream_t st);
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                   const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
-                  const uint32_t *cm_base, uint32_t *cm, int grid, cudaStream_t st);
+                  const uint32_t *cm_base, uint32_t *cm, bool gather, int grid,
+                  cudaStream_t st);
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                     const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
                     const uint32_t *cm_base, const uint32_t *cm_scan, int grid,

@@ -980,7 +980,7 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
 __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg *__restrict__ L,
                                                            ulonglong2 *spl, uint32_t *nspl,
                                                            uint16_t *tbl, uint32_t *ntiles,
-                                                           uint32_t *cm_size) {
+                                                           uint32_t *cm_size, bool from_arena) {
     // smp: SAMPLES_MAX keys; sv: their packed sort keys (padded layout)
     extern __shared__ __align__(16) unsigned char sample_smem[];
     ulonglong2 *smp = reinterpret_cast<ulonglong2 *>(sample_smem);
@@ -997,9 +997,17 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
     uint32_t S = next_pow2(8 * (k + 1));
     if (S < 256) S = 256;
     if (S > (uint32_t)SAMPLES_MAX) S = SAMPLES_MAX;
+    // On the first partition level of a round the segment's keys are not in
+    // the key buffer yet (the count kernel gathers them): read the sampled
+    // strings straight from the arena.
     for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
         const uint32_t r = hash32(s.start * 0x9E3779B1u + i * 0x85EBCA77u + s.len);
-        smp[i] = K[(uint32_t)(((uint64_t)r * s.len) >> 32)];
+        const uint32_t e = (uint32_t)(((uint64_t)r * s.len) >> 32);
+        smp[i] = from_arena
+                     ? from_key(load_key(a.arena, a.arena_bytes,
+                                         string_offset(a.offs, a.off_width,
+                                                       a.idx[0][s.start + e]) + s.depth))
+                     : K[e];
     }
     __syncthreads();
     // Order the samples by packed keys (window after the samples' common
@@ -1171,6 +1179,10 @@ __device__ __forceinline__ void load_splitters(PartSmem &sm, const ulonglong2 *_
     }
 }
 
+// GATHER (first partition level of a round): the keys are loaded from the
+// arena through idx and offsets and stored to the key buffer here, so the
+// key gather's random arena reads overlap the classification work.
+template <bool GATHER>
 __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg *__restrict__ L,
                                                         uint32_t nL,
                                                         const uint32_t *__restrict__ tile_base,
@@ -1204,12 +1216,34 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
         const uint32_t tl = t - tile_base[si];
         const uint32_t nt = tile_base[si + 1] - tile_base[si];
         const uint32_t lo = tl * PART_TILE + w * SUB;
-        const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
         Key kk[PART_ITEMS];
+        if (GATHER) {
+            // round-start segments live in buffer 0
+            const uint32_t *I = a.idx[0] + s.start;
+            ulonglong2 *KW = a.key[0] + s.start;
+            uint64_t off[PART_ITEMS];
 #pragma unroll
-        for (int c = 0; c < PART_ITEMS; ++c) {
-            const uint32_t e = lo + c * 32 + lane;
-            kk[c] = e < s.len ? to_key(K[e]) : key_max();
+            for (int c = 0; c < PART_ITEMS; ++c) {
+                const uint32_t e = lo + c * 32 + lane;
+                off[c] = e < s.len ? string_offset(a.offs, a.off_width, I[e]) + s.depth : 0;
+            }
+#pragma unroll
+            for (int c = 0; c < PART_ITEMS; ++c) {
+                const uint32_t e = lo + c * 32 + lane;
+                if (e < s.len) {
+                    kk[c] = load_key(a.arena, a.arena_bytes, off[c]);
+                    KW[e] = from_key(kk[c]);
+                } else {
+                    kk[c] = key_max();
+                }
+            }
+        } else {
+            const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
+#pragma unroll
+            for (int c = 0; c < PART_ITEMS; ++c) {
+                const uint32_t e = lo + c * 32 + lane;
+                kk[c] = e < s.len ? to_key(K[e]) : key_max();
+            }
         }
         // Bucket and rank among the warp's earlier keys of the same bucket
         // (keys are visited in position order: the scatter stays stable).
@@ -1983,7 +2017,8 @@ void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t 
 }
 
 void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl, uint32_t *nspl,
-                   uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size, cudaStream_t st) {
+                   uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size, bool from_arena,
+                   cudaStream_t st) {
     if (!nL) return;
     static bool attr = false;
     const int smem = SAMPLES_MAX * sizeof(ulonglong2) +
@@ -1992,21 +2027,27 @@ void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl
         cudaFuncSetAttribute(k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    k_sample<<<nL, SAMPLE_THREADS, smem, st>>>(a, L, spl, nspl, tbl, ntiles, cm_size);
+    k_sample<<<nL, SAMPLE_THREADS, smem, st>>>(a, L, spl, nspl, tbl, ntiles, cm_size, from_arena);
 }
 
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                   const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
-                  const uint32_t *cm_base, uint32_t *cm, int grid, cudaStream_t st) {
+                  const uint32_t *cm_base, uint32_t *cm, bool gather, int grid, cudaStream_t st) {
     if (!nL) return;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_count<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(PartSmem));
+        cudaFuncSetAttribute(k_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(PartSmem));
         attr = true;
     }
-    k_count<<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl, tbl,
-                                                          cm_base, cm);
+    if (gather)
+        k_count<true><<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl,
+                                                                    tbl, cm_base, cm);
+    else
+        k_count<false><<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl,
+                                                                     nspl, tbl, cm_base, cm);
 }
 
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,

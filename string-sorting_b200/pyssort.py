@@ -61,6 +61,7 @@ class Stats(ctypes.Structure):
         ("equal_moved", ctypes.c_uint64),
         ("equal_final", ctypes.c_uint64),
         ("boundaries", ctypes.c_uint64),
+        ("gather_fused", ctypes.c_uint64),
     ]
 
     def as_dict(self):
