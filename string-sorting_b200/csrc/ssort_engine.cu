@@ -57,8 +57,8 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
     const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
     SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
     LAUNCH(this, "classify",
-           launch_classify(cur, n_cur, ws.W1, ws.W8, ws.S, ws.L, dc,
-                           st));
+           launch_classify(cur, n_cur, ws.W1, ws.W8, SmallLists{{ws.S, ws.S2, ws.S3}}, ws.L,
+                           dc, st));
     SS_TRY(sync_counters());
     if (round_no < SSORT_MAX_ROUNDS) stats.live[round_no] = h_ctr->live_next;
     uint32_t n_large = h_ctr->n_large;
@@ -101,7 +101,7 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
         LAUNCH(this, "emit",
                launch_emit(a, lcur, n_large, ws.tile_base,
                            ws.nspl, ws.cm_base,
-                           ws.cm, ws.W1, ws.W8, ws.S, lnext,
+                           ws.cm, ws.W1, ws.W8, SmallLists{{ws.S, ws.S2, ws.S3}}, lnext,
                            ws.E, ws.B, nxt, dc, st));
         SS_TRY(sync_counters());
         n_large = h_ctr->n_large_next;
@@ -110,11 +110,25 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
     }
     LAUNCH(this, "warp1", launch_warp1(a, ws.W1, nxt, dc, g8, st));
     LAUNCH(this, "warp8", launch_warp8(a, ws.W8, nxt, dc, g8, st));
-    LAUNCH(this, "block", launch_block(a, ws.S, nxt, dc, g8, st));
+    {
+        // CTA-sort size classes: groups of 64, 128, 256 threads per segment.
+        // The counts are current: the host read them after the last
+        // classification or partition level.
+        Seg *lists[3] = {ws.S, ws.S2, ws.S3};
+        const uint32_t counts[3] = {h_ctr->n_small, h_ctr->n_small2, h_ctr->n_small3};
+        for (int k = 0; k < 3; ++k) {
+            if (!counts[k]) continue;
+            const uint32_t per_cta = (uint32_t)SMALL_THREADS / (64u << k);
+            const int grid = (int)std::min<uint32_t>((uint32_t)g8,
+                                                     (counts[k] + per_cta - 1) / per_cta);
+            LAUNCH(this, "block", launch_block(a, lists[k], k, nxt, dc, grid, st));
+        }
+    }
     LAUNCH(this, "equal", launch_equal(a, ws.E, nxt, dc, g8, st));
     LAUNCH(this, "boundary", launch_boundary(a, ws.B, dc, g4, st));
     SS_TRY(sync_counters());
-    stats.small_segments += h_ctr->n_w1 + h_ctr->n_w8 + h_ctr->n_small;
+    stats.small_segments +=
+        h_ctr->n_w1 + h_ctr->n_w8 + h_ctr->n_small + h_ctr->n_small2 + h_ctr->n_small3;
     stats.partitioned += h_ctr->partitioned;
     stats.gather_elems += h_ctr->gather_elems;
     if (fused_gather) stats.gather_fused += h_ctr->gather_elems;

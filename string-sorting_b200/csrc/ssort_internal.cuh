@@ -42,6 +42,11 @@ constexpr int WARP8_CAP = 256;
 constexpr int SMALL_CAP = 2048;
 constexpr int SMALL_THREADS = 256;
 constexpr int SMALL_ITEMS = SMALL_CAP / SMALL_THREADS;  // 8
+// The CTA sort splits its segments into three size classes, sorted by groups
+// of 64, 128 and 256 threads (8 strings per thread): <= BLOCK_CAP1,
+// <= BLOCK_CAP2 and <= SMALL_CAP strings.
+constexpr int BLOCK_CAP1 = 512;
+constexpr int BLOCK_CAP2 = 1024;
 
 // Sample partitioning of large segments.
 constexpr int KMAX = 511;               // splitters per segment and pass
@@ -75,6 +80,12 @@ struct Counters {
     unsigned long long warp1_fresh, warp1_keyed, warp8_fresh, warp8_keyed, block_fresh,
         block_keyed;
     unsigned long long equal_moved, equal_final;  // equality-bucket copies / lcp fills
+    uint32_t n_small2, n_small3;  // CTA-sort segments of the 2nd and 3rd size class
+};
+
+// The CTA-sort segment lists, one per size class (n_small, n_small2, n_small3).
+struct SmallLists {
+    Seg *s[3];
 };
 
 struct SortArgs {
@@ -103,7 +114,7 @@ constexpr uint32_t scan_partials_for(uint64_t n) {
 }
 
 struct WsLayout {
-    size_t idx1, key0, key1, lcp, bkt, R, N, W1, W8, S, E, B, L, L2, spl, nspl, tbl, ntiles,
+    size_t idx1, key0, key1, lcp, bkt, R, N, W1, W8, S, S2, S3, E, B, L, L2, spl, nspl, tbl, ntiles,
         cm_size, cm_base, tile_base, tmp, cm, partials, ctr;
     size_t cm_cap, total;
 };
@@ -128,6 +139,8 @@ constexpr WsLayout ws_layout(uint64_t n) {
     o.W1 = take(half * sizeof(Seg));
     o.W8 = take((n / (WARP1_CAP + 1) + 2) * sizeof(Seg));
     o.S = take((n / (WARP8_CAP + 1) + 2) * sizeof(Seg));
+    o.S2 = take((n / (BLOCK_CAP1 + 1) + 2) * sizeof(Seg));
+    o.S3 = take((n / (BLOCK_CAP2 + 1) + 2) * sizeof(Seg));
     // equality work items: buckets of >= 2 strings, one item per EQ_TILE
     o.E = take((half + n / EQ_TILE + 2) * sizeof(Seg));
     o.B = take((n + 2) * 8);
@@ -153,7 +166,7 @@ constexpr WsLayout ws_layout(uint64_t n) {
 struct Workspace {
     uint32_t *idx1, *lcp, *nspl, *ntiles, *cm_size, *cm_base, *tile_base, *tmp, *cm, *partials;
     ulonglong2 *key0, *key1, *spl;
-    Seg *R, *N, *W1, *W8, *S, *E, *L, *L2;
+    Seg *R, *N, *W1, *W8, *S, *S2, *S3, *E, *L, *L2;
     uint2 *B;
     uint16_t *tbl;
     uint32_t *bkt;
@@ -173,6 +186,8 @@ inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
     w.W1 = (Seg *)(base + o.W1);
     w.W8 = (Seg *)(base + o.W8);
     w.S = (Seg *)(base + o.S);
+    w.S2 = (Seg *)(base + o.S2);
+    w.S3 = (Seg *)(base + o.S3);
     w.E = (Seg *)(base + o.E);
     w.B = (uint2 *)(base + o.B);
     w.L = (Seg *)(base + o.L);
@@ -194,8 +209,8 @@ inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
 
 // ---- launchers (ssort_kernels.cu) ----------------------------------------
 void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st);
-void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L, Counters *c,
-                     cudaStream_t st);
+void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, SmallLists S, Seg *L,
+                     Counters *c, cudaStream_t st);
 void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
                         cudaStream_t st);
 // Batches: one round-0 segment per instance; instance-local result indices.
@@ -243,14 +258,15 @@ void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t
                     cudaStream_t st);
 void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                  const uint32_t *nspl, const uint32_t *cm_base, const uint32_t *cm_scan,
-                 Seg *W1, Seg *W8, Seg *S, Seg *L2, Seg *E, uint2 *B, Seg *N, Counters *c,
-                 cudaStream_t st);
+                 Seg *W1, Seg *W8, SmallLists S, Seg *L2, Seg *E, uint2 *B, Seg *N,
+                 Counters *c, cudaStream_t st);
 // On-chip segment sorts; list lengths are read from the counters on the device.
 void launch_warp1(const SortArgs &a, const Seg *W1, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
 void launch_warp8(const SortArgs &a, const Seg *W8, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
-void launch_block(const SortArgs &a, const Seg *S, Seg *N, Counters *c, int grid,
+// cls: size class 0, 1, 2 (segment list S holds that class)
+void launch_block(const SortArgs &a, const Seg *S, int cls, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
 void launch_equal(const SortArgs &a, const Seg *E, Seg *N, Counters *c, int grid,
                   cudaStream_t st);

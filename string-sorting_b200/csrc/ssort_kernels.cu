@@ -541,7 +541,21 @@ __global__ void k_iota(uint32_t *idx, uint32_t n) {
         idx[i] = i;
 }
 
-__global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *W1, Seg *W8, Seg *S,
+// Appends o (when sm) to the CTA-sort list of its size class; warp-collective.
+__device__ __forceinline__ void append_small(const SmallLists &S, Counters *c, bool sm,
+                                             const Seg &o) {
+    const bool c0 = sm && o.len <= (uint32_t)BLOCK_CAP1;
+    const bool c1 = sm && !c0 && o.len <= (uint32_t)BLOCK_CAP2;
+    const bool c2 = sm && !c0 && !c1;
+    uint32_t slot = warp_append(&c->n_small, c0);
+    if (c0) S.s[0][slot] = o;
+    slot = warp_append(&c->n_small2, c1);
+    if (c1) S.s[1][slot] = o;
+    slot = warp_append(&c->n_small3, c2);
+    if (c2) S.s[2][slot] = o;
+}
+
+__global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *W1, Seg *W8, SmallLists S,
                            Seg *L, Counters *c) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool v = i < nR;
@@ -554,8 +568,7 @@ __global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *W1, Seg 
     if (w1) W1[slot] = s;
     slot = warp_append(&c->n_w8, w8);
     if (w8) W8[slot] = s;
-    slot = warp_append(&c->n_small, sm);
-    if (sm) S[slot] = s;
+    append_small(S, c, sm, s);
     slot = warp_append(&c->n_large, lg);
     if (lg) L[slot] = s;
     const unsigned long long live = warp_sum(v ? s.len : 0);
@@ -1403,8 +1416,8 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
 // ---- bucket emission: one CTA per partitioned segment ----------------------
 __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__restrict__ tile_base,
                        const uint32_t *__restrict__ nspl, const uint32_t *__restrict__ cm_base,
-                       const uint32_t *__restrict__ cm_scan, Seg *W1, Seg *W8, Seg *S, Seg *L2,
-                       Seg *E, uint2 *B, Seg *N, Counters *c) {
+                       const uint32_t *__restrict__ cm_scan, Seg *W1, Seg *W8, SmallLists S,
+                       Seg *L2, Seg *E, uint2 *B, Seg *N, Counters *c) {
     const uint32_t si = blockIdx.x;
     const Seg s = L[si];
     const uint32_t u = nspl[si] & 0xFFFF, nb = 2 * u + 1;
@@ -1466,8 +1479,7 @@ __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__
         if (w1) W1[slot] = o;
         slot = warp_append(&c->n_w8, w8);
         if (w8) W8[slot] = o;
-        slot = warp_append(&c->n_small, sm);
-        if (sm) S[slot] = o;
+        append_small(S, c, sm, o);
         slot = warp_append(&c->n_large_next, lg);
         if (lg) L2[slot] = o;
     }
@@ -1672,20 +1684,45 @@ __global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg
     }
 }
 
-// ---- segments of 257..SMALL_CAP strings: one CTA ---------------------------
+// ---- segments of 257..SMALL_CAP strings: groups of threads -----------------
+// A CTA of SMALL_THREADS threads is split into groups of GT threads (2, 4 or
+// 8 warps); each group sorts one segment of up to GT * SMALL_ITEMS strings at a
+// time and synchronises on its own named barrier.  Segments are bucketed by
+// size so that every thread holds 5..8 strings: small segments do not leave
+// warps idle at CTA-wide barriers, and one SM overlaps the loads and sorts of
+// up to 12 segments.
 constexpr int SMALL_PAD = SMALL_CAP + SMALL_CAP / 8;
 constexpr size_t BLOCK_SMEM = SMALL_PAD * (sizeof(ulonglong2) + sizeof(uint32_t) + sizeof(uint64_t));
+constexpr uint32_t BLOCK_RUN = 32 * SMALL_ITEMS;  // one warp's run of packed keys
 
-// Full-comparator sort of the span (multiple of RUN) records at padded
-// positions 0..span-1: warp runs of RUN, then pairwise merge-path merges.
-__device__ __noinline__ void block_sort_full(ulonglong2 *sk, uint32_t *sx, uint32_t span) {
-    constexpr uint32_t RUN = 32 * SMALL_ITEMS;
-    const uint32_t nruns = span / RUN;
-    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (w < nruns) warp_sort_run<SMALL_ITEMS>(sk, sx, w * RUN, lane);
-    __syncthreads();
-    for (uint32_t run = RUN; run < span; run <<= 1) {
-        const uint32_t o = threadIdx.x * SMALL_ITEMS;
+// Barrier among the GT threads of group gi: named barrier 1 + gi (0 is
+// __syncthreads).  Immediate ids, so that a CTA claims only the barriers it
+// uses (at most 5) and the SM's barriers do not limit occupancy.
+template <int GT>
+__device__ __forceinline__ void group_sync(uint32_t gi) {
+    constexpr int G = SMALL_THREADS / GT;
+    if (G == 1 || gi == 0)
+        asm volatile("bar.sync 1, %0;" ::"n"(GT) : "memory");
+    else if (G == 2 || gi == 1)
+        asm volatile("bar.sync 2, %0;" ::"n"(GT) : "memory");
+    else if (gi == 2)
+        asm volatile("bar.sync 3, %0;" ::"n"(GT) : "memory");
+    else
+        asm volatile("bar.sync 4, %0;" ::"n"(GT) : "memory");
+}
+
+// Full-comparator sort of the span (multiple of BLOCK_RUN) records at padded
+// positions 0..span-1 by the GT threads of a group (thread t): warp runs, then
+// pairwise merge-path merges.
+template <int GT>
+__device__ __noinline__ void group_sort_full(ulonglong2 *sk, uint32_t *sx, uint32_t span,
+                                             uint32_t t, uint32_t gi) {
+    const uint32_t nruns = span / BLOCK_RUN;
+    const uint32_t lane = t & 31, gw = t >> 5;
+    if (gw < nruns) warp_sort_run<SMALL_ITEMS>(sk, sx, gw * BLOCK_RUN, lane);
+    group_sync<GT>(gi);
+    for (uint32_t run = BLOCK_RUN; run < span; run <<= 1) {
+        const uint32_t o = t * SMALL_ITEMS;
         Key ok[SMALL_ITEMS];
         uint32_t ox[SMALL_ITEMS];
         const bool active = o < span;
@@ -1722,7 +1759,7 @@ __device__ __noinline__ void block_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
                 }
             }
         }
-        __syncthreads();
+        group_sync<GT>(gi);
         if (active) {
 #pragma unroll
             for (int i = 0; i < SMALL_ITEMS; ++i) {
@@ -1730,85 +1767,90 @@ __device__ __noinline__ void block_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
                 sx[pad(o + i)] = ox[i];
             }
         }
-        __syncthreads();
+        group_sync<GT>(gi);
     }
 }
 
-// Pairwise merge-path merges of the sorted runs of length run0 in sv[0..span)
-// (span = runs * run0, padded positions) until one run is left; MI outputs
-// per thread and pass (run0 is a multiple of MI, span <= MI * SMALL_THREADS).
-template <int MI>
-__device__ __forceinline__ void block_merge_passes64(uint64_t *sv, uint32_t run0, uint32_t span) {
-    for (uint32_t run = run0; run < span; run <<= 1) {
-        {
-            const uint32_t o = threadIdx.x * MI;
-            uint64_t ov[MI];
-            const bool active = o < span;
-            if (active) {
-                const uint32_t a0 = o / (2 * run) * (2 * run);
-                const uint32_t b0 = a0 + run;
-                const uint32_t la = min(run, span - a0);
-                const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
-                const uint32_t d = o - a0;
-                uint32_t ia = merge_split64(sv, a0, la, b0, lb, d);
-                uint32_t ib = d - ia;
+// Pairwise merge-path merges of the sorted packed-key runs of BLOCK_RUN in
+// sv[0..span) until one run is left; SMALL_ITEMS outputs per thread and pass.
+template <int GT>
+__device__ __forceinline__ void group_merge_passes64(uint64_t *sv, uint32_t span, uint32_t t,
+                                                     uint32_t gi) {
+    for (uint32_t run = BLOCK_RUN; run < span; run <<= 1) {
+        const uint32_t o = t * SMALL_ITEMS;
+        uint64_t ov[SMALL_ITEMS];
+        const bool active = o < span;
+        if (active) {
+            const uint32_t a0 = o / (2 * run) * (2 * run);
+            const uint32_t b0 = a0 + run;
+            const uint32_t la = min(run, span - a0);
+            const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
+            const uint32_t d = o - a0;
+            uint32_t ia = merge_split64(sv, a0, la, b0, lb, d);
+            uint32_t ib = d - ia;
 #pragma unroll
-                for (int i = 0; i < MI; ++i) {
-                    const uint64_t va = ia < la ? sv[pad(a0 + ia)] : ~0ull;
-                    const uint64_t vb = ib < lb ? sv[pad(b0 + ib)] : ~0ull;
-                    const bool take_a = ib >= lb || (ia < la && va < vb);
-                    ov[i] = take_a ? va : vb;
-                    ia += take_a;
-                    ib += !take_a;
-                }
+            for (int i = 0; i < SMALL_ITEMS; ++i) {
+                const uint64_t va = ia < la ? sv[pad(a0 + ia)] : ~0ull;
+                const uint64_t vb = ib < lb ? sv[pad(b0 + ib)] : ~0ull;
+                const bool take_a = ib >= lb || (ia < la && va < vb);
+                ov[i] = take_a ? va : vb;
+                ia += take_a;
+                ib += !take_a;
             }
-            __syncthreads();
-            if (active) {
-#pragma unroll
-                for (int i = 0; i < MI; ++i) sv[pad(o + i)] = ov[i];
-            }
-            __syncthreads();
         }
+        group_sync<GT>(gi);
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < SMALL_ITEMS; ++i) sv[pad(o + i)] = ov[i];
+        }
+        group_sync<GT>(gi);
     }
 }
 
-__global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
-                                                            Seg *N, Counters *c) {
+// The CTAs cta0 .. cta0 + ncta - 1 of the launch sort the segments of one
+// size class (list S of nS segments) with groups of GT threads.
+template <int GT>
+__device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__restrict__ S,
+                                            uint32_t nS, uint32_t cta0, uint32_t ncta, Seg *N,
+                                            Counters *c) {
+    constexpr uint32_t G = SMALL_THREADS / GT;          // groups per CTA
+    constexpr uint32_t CAP = GT * SMALL_ITEMS;          // strings per group
+    constexpr uint32_t PADC = CAP + CAP / 8;            // padded slots per group
+    static_assert(G * PADC == SMALL_PAD, "group slots");
     extern __shared__ __align__(16) unsigned char block_smem[];
-    ulonglong2 *sk = reinterpret_cast<ulonglong2 *>(block_smem);
-    uint64_t *sv = reinterpret_cast<uint64_t *>(sk + SMALL_PAD);
-    uint32_t *sx = reinterpret_cast<uint32_t *>(sv + SMALL_PAD);
     __shared__ uint64_t red[2][SMALL_THREADS / 32];
-    constexpr uint32_t FULL_RUN = 32 * SMALL_ITEMS;
-    const uint32_t nS = c->n_small;
-    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __shared__ int ok_flag[G];
+    const uint32_t gi = threadIdx.x / GT, t = threadIdx.x % GT;
+    const uint32_t lane = threadIdx.x & 31, gw = t >> 5, w = threadIdx.x >> 5;
+    ulonglong2 *sk_all = reinterpret_cast<ulonglong2 *>(block_smem);
+    uint64_t *sv_all = reinterpret_cast<uint64_t *>(sk_all + SMALL_PAD);
+    uint32_t *sx_all = reinterpret_cast<uint32_t *>(sv_all + SMALL_PAD);
+    ulonglong2 *sk = sk_all + gi * PADC;
+    uint64_t *sv = sv_all + gi * PADC;
+    uint32_t *sx = sx_all + gi * PADC;
     unsigned long long fresh = 0, keyed = 0;
-    for (uint32_t g = blockIdx.x; g < nS; g += gridDim.x) {
+    for (uint32_t g = (blockIdx.x - cta0) * G + gi; g < nS; g += ncta * G) {
         const Seg s = S[g];
         if (s.flags & SEG_KEYS)
             keyed += s.len;
         else
             fresh += s.len;
-        // Runs of 64/128/256 packed keys so that most of the 8 warps get one.
-        const uint32_t per = (s.len + SMALL_THREADS - 1) / SMALL_THREADS;  // 2..8
-        const uint32_t items = per <= 2 ? 2u : (per <= 4 ? 4u : 8u);
-        const uint32_t run0 = 32 * items;
-        const uint32_t nruns = (s.len + run0 - 1) / run0;
-        const uint32_t span = nruns * run0;
-        const uint32_t full_span = (s.len + FULL_RUN - 1) / FULL_RUN * FULL_RUN;
-        for (uint32_t e = threadIdx.x; e < full_span; e += SMALL_THREADS) {
+        const uint32_t nruns = (s.len + BLOCK_RUN - 1) / BLOCK_RUN;
+        const uint32_t span = nruns * BLOCK_RUN;
+        for (uint32_t e = t; e < span; e += GT) {
             Key k = key_max();
             uint32_t id = IDX_MAX;
             if (e < s.len) load_elem(a, s, e, k, id);
             sk[pad(e)] = from_key(k);
             sx[pad(e)] = id;
         }
-        __syncthreads();
+        if (t == 0) ok_flag[gi] = 1;
+        group_sync<GT>(gi);
         // f: first bit in which the keys differ.
         {
             const Key k0 = to_key(sk[pad(0)]);
             uint64_t dh = 0, dl = 0;
-            for (uint32_t e = threadIdx.x; e < s.len; e += SMALL_THREADS) {
+            for (uint32_t e = t; e < s.len; e += GT) {
                 const Key k = to_key(sk[pad(e)]);
                 dh |= k.hi ^ k0.hi;
                 dl |= k.lo ^ k0.lo;
@@ -1823,48 +1865,44 @@ __global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Se
                 red[1][w] = dl;
             }
         }
-        __syncthreads();
+        group_sync<GT>(gi);
         uint64_t dh = 0, dl = 0;
 #pragma unroll
-        for (int q = 0; q < SMALL_THREADS / 32; ++q) {
-            dh |= red[0][q];
-            dl |= red[1][q];
+        for (uint32_t q = 0; q < GT / 32; ++q) {
+            dh |= red[0][gi * (GT / 32) + q];
+            dl |= red[1][gi * (GT / 32) + q];
         }
         bool packed = false;
         if (dh | dl) {
             const uint32_t f = clz128(dh, dl);
-            if (w < nruns) {
-                if (items == 2)
-                    warp_run_packed<2>(sk, sv, w * run0, s.len, f, lane);
-                else if (items == 4)
-                    warp_run_packed<4>(sk, sv, w * run0, s.len, f, lane);
-                else
-                    warp_run_packed<8>(sk, sv, w * run0, s.len, f, lane);
-            }
-            __syncthreads();
-            // Each thread writes `items` outputs per pass, so a segment of
-            // span keys keeps span / items threads busy (not span / 8).
-            if (items == 2)
-                block_merge_passes64<2>(sv, run0, span);
-            else if (items == 4)
-                block_merge_passes64<4>(sv, run0, span);
-            else
-                block_merge_passes64<8>(sv, run0, span);
-            packed = __syncthreads_and(window_pairs_ok_ind(sk, sv, s.len, threadIdx.x,
-                                                           SMALL_THREADS));
-            if (!packed) block_sort_full(sk, sx, full_span);
+            if (gw < nruns) warp_run_packed<SMALL_ITEMS>(sk, sv, gw * BLOCK_RUN, s.len, f, lane);
+            group_sync<GT>(gi);
+            group_merge_passes64<GT>(sv, span, t, gi);
+            if (!window_pairs_ok_ind(sk, sv, s.len, t, GT)) ok_flag[gi] = 0;
+            group_sync<GT>(gi);
+            packed = ok_flag[gi] != 0;
+            if (!packed) group_sort_full<GT>(sk, sx, span, t, gi);
         }
-        __syncthreads();
+        group_sync<GT>(gi);
         if (packed)
-            finish_segment<true>(a, s, sk, sx, sv, threadIdx.x, SMALL_THREADS, N, c);
+            finish_segment<true>(a, s, sk, sx, sv, t, GT, N, c);
         else
-            finish_segment<false>(a, s, sk, sx, sv, threadIdx.x, SMALL_THREADS, N, c);
-        __syncthreads();
+            finish_segment<false>(a, s, sk, sx, sv, t, GT, N, c);
+        group_sync<GT>(gi);
     }
-    if (threadIdx.x == 0 && (fresh | keyed)) {
+    if (t == 0 && (fresh | keyed)) {
         atomicAdd(&c->block_fresh, fresh);
         atomicAdd(&c->block_keyed, keyed);
     }
+}
+
+// One size class per launch (a single launch for all three inlines all
+// three bodies and spills more; measured slower).
+template <int GT>
+__global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
+                                                            const uint32_t *n_list, Seg *N,
+                                                            Counters *c) {
+    block_class<GT>(a, S, *n_list, 0, gridDim.x, N, c);
 }
 
 // ---- equality buckets: work items of up to EQ_TILE strings ------------------
@@ -1919,8 +1957,8 @@ void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st) {
     k_iota<<<g ? g : 1, 256, 0, st>>>(idx, n);
 }
 
-void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, Seg *S, Seg *L, Counters *c,
-                     cudaStream_t st) {
+void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, SmallLists S, Seg *L,
+                     Counters *c, cudaStream_t st) {
     if (!nR) return;
     k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, W1, W8, S, L, c);
 }
@@ -2066,8 +2104,8 @@ void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t
 
 void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                  const uint32_t *nspl, const uint32_t *cm_base, const uint32_t *cm_scan,
-                 Seg *W1, Seg *W8, Seg *S, Seg *L2, Seg *E, uint2 *B, Seg *N, Counters *c,
-                 cudaStream_t st) {
+                 Seg *W1, Seg *W8, SmallLists S, Seg *L2, Seg *E, uint2 *B, Seg *N,
+                 Counters *c, cudaStream_t st) {
     if (!nL) return;
     k_emit<<<nL, 256, 0, st>>>(a, L, tile_base, nspl, cm_base, cm_scan, W1, W8, S, L2, E, B, N,
                                c);
@@ -2088,15 +2126,24 @@ void launch_warp8(const SortArgs &a, const Seg *W8, Seg *N, Counters *c, int gri
     k_warp8<<<grid, WARP_THREADS, W8_SMEM, st>>>(a, W8, N, c);
 }
 
-void launch_block(const SortArgs &a, const Seg *S, Seg *N, Counters *c, int grid,
+void launch_block(const SortArgs &a, const Seg *S, int cls, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_block<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)BLOCK_SMEM);
+        cudaFuncSetAttribute(k_block<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)BLOCK_SMEM);
+        cudaFuncSetAttribute(k_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)BLOCK_SMEM);
         attr = true;
     }
-    k_block<<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, N, c);
+    if (cls == 0)
+        k_block<64><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, &c->n_small, N, c);
+    else if (cls == 1)
+        k_block<128><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, &c->n_small2, N, c);
+    else
+        k_block<256><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, &c->n_small3, N, c);
 }
 
 void launch_equal(const SortArgs &a, const Seg *E, Seg *N, Counters *c, int grid,
