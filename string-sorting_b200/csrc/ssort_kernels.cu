@@ -1090,25 +1090,37 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
         }
         __syncthreads();
     }
-    // Candidates at ranks (j+1)*S/(k+1), padded with the all-ones key, sorted
-    // by full key with a bitonic network over SAMPLE_THREADS slots.
+    // Candidates at ranks (j+1)*S/(k+1), padded with the all-ones key.  They
+    // are in packed-key order, which is full-key order unless two windows
+    // tie; only then a bitonic network over the next power of two >= k slots
+    // sorts them by full key.
     {
         const uint32_t j = threadIdx.x;
         cands[j] = j < k ? smp[sv[pad(((j + 1) * S) / (k + 1))] & 0xFFF] : from_key(key_max());
     }
     __syncthreads();
-    for (uint32_t kk = 2; kk <= (uint32_t)SAMPLE_THREADS; kk <<= 1) {
-        for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
-            const uint32_t i = threadIdx.x, l = i ^ jj;
-            Key x = to_key(cands[i]), y = to_key(cands[l]);
-            const bool lower = l > i;
-            const bool asc = (i & kk) == 0;
-            // the lower slot keeps the min when ascending, the max otherwise
-            const bool take = lower ? (asc ? key_lt(y, x) : key_lt(x, y))
-                                    : (asc ? key_lt(x, y) : key_lt(y, x));
-            __syncthreads();
-            if (take) cands[i] = from_key(y);
-            __syncthreads();
+    const bool out_of_order = threadIdx.x + 1 < k &&
+                              key_lt(to_key(cands[threadIdx.x + 1]), to_key(cands[threadIdx.x]));
+    if (__syncthreads_or(out_of_order)) {
+        const uint32_t kp = next_pow2(k);
+        for (uint32_t kk = 2; kk <= kp; kk <<= 1) {
+            for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+                const uint32_t i = threadIdx.x, l = i ^ jj;
+                bool take = false;
+                Key y{0, 0};
+                if (i < kp) {
+                    const Key x = to_key(cands[i]);
+                    y = to_key(cands[l]);
+                    const bool lower = l > i;
+                    const bool asc = (i & kk) == 0;
+                    // the lower slot keeps the min when ascending, the max otherwise
+                    take = lower ? (asc ? key_lt(y, x) : key_lt(x, y))
+                                 : (asc ? key_lt(x, y) : key_lt(y, x));
+                }
+                __syncthreads();
+                if (take) cands[i] = from_key(y);
+                __syncthreads();
+            }
         }
     }
     // Survivors: the distinct candidates, compacted in order.
@@ -1308,7 +1320,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
 // tile is first laid out in shared memory in output order (its bucket runs
 // back to back), so consecutive threads store to consecutive addresses within
 // every run.
-constexpr int SCATTER_THREADS = 256;
+constexpr int SCATTER_THREADS = 256;  // 512 x 8 items measured slower
 constexpr int SCATTER_ITEMS = PART_TILE / SCATTER_THREADS;  // 16
 struct ScatterSmem {
     ulonglong2 key[PART_TILE];
@@ -1498,6 +1510,117 @@ __device__ __forceinline__ void load_elem(const SortArgs &a, const Seg &s, uint3
             : load_key(a.arena, a.arena_bytes, string_offset(a.offs, a.off_width, id) + s.depth);
 }
 
+// Sorts one segment of at most W strings held by the W lanes of one aligned
+// lane group (W = 8 or 32; lane li of the group holds string li).  Every
+// lane of the warp calls this with its group's segment (len 0 for idle
+// groups): the shuffles, ballots and the next-round append are
+// warp-collective.
+template <int W>
+__device__ __forceinline__ void warp1_group(const SortArgs &a, const Seg &s, uint32_t lane,
+                                            Seg *N, Counters *c) {
+    const uint32_t li = lane & (W - 1), base = lane & ~(uint32_t)(W - 1);
+    const bool v = li < s.len;
+    uint32_t id = IDX_MAX;
+    Key k = key_max();
+    if (v) load_elem(a, s, li, k, id);
+    // Bits in which the group's keys differ.
+    Key k0;
+    k0.hi = __shfl_sync(0xffffffffu, k.hi, base);
+    k0.lo = __shfl_sync(0xffffffffu, k.lo, base);
+    uint64_t dh = v ? (k.hi ^ k0.hi) : 0, dl = v ? (k.lo ^ k0.lo) : 0;
+#pragma unroll
+    for (int d = W / 2; d > 0; d >>= 1) {
+        dh |= __shfl_xor_sync(0xffffffffu, dh, d);
+        dl |= __shfl_xor_sync(0xffffffffu, dl, d);
+    }
+    // Packed 64-bit keys (window after the common prefix, source lane), a
+    // bitonic sort inside the group (the last stage ascending for every
+    // group), then each record moves to its rank.  Groups whose keys are all
+    // equal sort by lane alone, which keeps them in place.
+    const bool diff = (dh | dl) != 0;
+    const uint32_t f = diff ? clz128(dh, dl) : 0u;
+    bool bad = false;
+    if (__any_sync(0xffffffffu, diff)) {  // else every group's keys are all equal
+        uint64_t x = !v ? ~0ull : (diff ? sort_key(k, f, lane) : (uint64_t)lane);
+#pragma unroll
+        for (int kk = 2; kk <= W; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                const uint64_t y = __shfl_xor_sync(0xffffffffu, x, j);
+                const bool up = kk == W || (lane & kk) == 0;
+                const bool keep_min = ((lane & j) == 0) == up;
+                x = keep_min ? (y < x ? y : x) : (y < x ? x : y);
+            }
+        }
+        const uint32_t src = v ? (uint32_t)(x & 31) : lane;
+        Key kn;
+        kn.hi = __shfl_sync(0xffffffffu, k.hi, src);
+        kn.lo = __shfl_sync(0xffffffffu, k.lo, src);
+        const uint32_t idn = __shfl_sync(0xffffffffu, id, src);
+        k = kn;
+        id = idn;
+        // Pairs with equal windows must also be in full-key order.
+        Key kp;
+        kp.hi = __shfl_up_sync(0xffffffffu, k.hi, 1);
+        kp.lo = __shfl_up_sync(0xffffffffu, k.lo, 1);
+        bad = v && diff && li > 0 &&
+              (window64(kp, f) >> POS_BITS) == (window64(k, f) >> POS_BITS) && key_lt(k, kp);
+    }
+    if (__any_sync(0xffffffffu, bad)) {
+        // Full (key, index) comparator over every group (rare).
+#pragma unroll
+        for (int kk = 2; kk <= W; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                Key ok;
+                ok.hi = __shfl_xor_sync(0xffffffffu, k.hi, j);
+                ok.lo = __shfl_xor_sync(0xffffffffu, k.lo, j);
+                const uint32_t oi = __shfl_xor_sync(0xffffffffu, id, j);
+                const bool up = kk == W || (lane & kk) == 0;
+                const bool keep_min = ((lane & j) == 0) == up;
+                const bool take = keep_min ? pair_lt(ok, oi, k, id) : pair_lt(k, id, ok, oi);
+                if (take) {
+                    k = ok;
+                    id = oi;
+                }
+            }
+        }
+    }
+    Key prev, next;
+    prev.hi = __shfl_up_sync(0xffffffffu, k.hi, 1);
+    prev.lo = __shfl_up_sync(0xffffffffu, k.lo, 1);
+    next.hi = __shfl_down_sync(0xffffffffu, k.hi, 1);
+    next.lo = __shfl_down_sync(0xffffffffu, k.lo, 1);
+    const bool head = v && (li == 0 || !key_eq(prev, k));
+    const uint32_t heads = __ballot_sync(0xffffffffu, head);
+    bool want = false;
+    uint32_t h = lane;
+    if (v) {
+        const uint32_t p = s.start + li;
+        a.idx[0][p] = id;
+        if (li == 0 || li == s.len - 1) a.key[0][p] = from_key(k);
+        if (li > 0) {
+            if (!key_eq(prev, k))
+                a.lcp[p] = s.depth + key_lcp(prev, k);
+            else if (key_is_end(k))
+                a.lcp[p] = s.depth + key_len(k);
+        }
+        const bool tail = li == s.len - 1 || !key_eq(next, k);
+        if (tail && !head && !key_is_end(k)) {
+            const uint32_t m = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+            h = 31 - __clz(heads & m);  // the run's head: at or after the group's lane 0
+            want = true;
+        }
+    }
+    emit_next_warp(N, c, want, s.start + (h - base), lane - h + 1, s.depth + KEY_BYTES);
+}
+
+// Segments of <= WARP1_CAP strings.  First pass: a warp takes W1_PACK
+// consecutive list entries and sorts those of at most 8 strings together, one
+// per 8-lane group, so that their loads overlap.  Second pass: one warp per
+// remaining segment.
+constexpr uint32_t W1_PACK = 4;
+
 __global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *__restrict__ T,
                                                         Seg *N, Counters *c) {
     const uint32_t nT = c->n_w1;
@@ -1505,94 +1628,24 @@ __global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *_
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long fresh = 0, keyed = 0;
+    for (uint32_t g0 = warp0 * W1_PACK; g0 < nT; g0 += nwarps * W1_PACK) {
+        const uint32_t j = lane >> 3;
+        const Seg sj = g0 + j < nT ? T[g0 + j] : Seg{0, 0, 0, 0};
+        const bool small = sj.len <= 8;
+        if ((lane & 7) == 0) {
+            if (sj.flags & SEG_KEYS)
+                keyed += sj.len;
+            else
+                fresh += sj.len;
+        }
+        if (__any_sync(0xffffffffu, small && sj.len > 0))
+            warp1_group<8>(a, small ? sj : Seg{0, 0, 0, 0}, lane, N, c);
+    }
     for (uint32_t g = warp0; g < nT; g += nwarps) {
         const Seg s = T[g];
-        const bool v = lane < s.len;
-        if (s.flags & SEG_KEYS)
-            keyed += s.len;
-        else
-            fresh += s.len;
-        uint32_t id = IDX_MAX;
-        Key k = key_max();
-        if (v) load_elem(a, s, lane, k, id);
-        // Bits in which the segment's keys differ.
-        Key k0;
-        k0.hi = __shfl_sync(0xffffffffu, k.hi, 0);
-        k0.lo = __shfl_sync(0xffffffffu, k.lo, 0);
-        uint64_t dh = v ? (k.hi ^ k0.hi) : 0, dl = v ? (k.lo ^ k0.lo) : 0;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-            dh |= __shfl_xor_sync(0xffffffffu, dh, d);
-            dl |= __shfl_xor_sync(0xffffffffu, dl, d);
-        }
-        if (dh | dl) {
-            // Packed 64-bit keys, then move each record to its rank.
-            const uint32_t f = clz128(dh, dl);
-            uint64_t sv[1] = {v ? sort_key(k, f, lane) : ~0ull};
-            warp_bitonic64<1>(sv, lane);
-            const uint32_t src = v ? (uint32_t)(sv[0] & 31) : lane;
-            Key kn;
-            kn.hi = __shfl_sync(0xffffffffu, k.hi, src);
-            kn.lo = __shfl_sync(0xffffffffu, k.lo, src);
-            const uint32_t idn = __shfl_sync(0xffffffffu, id, src);
-            k = kn;
-            id = idn;
-            // Pairs with equal windows must also be in full-key order.
-            Key kp;
-            kp.hi = __shfl_up_sync(0xffffffffu, k.hi, 1);
-            kp.lo = __shfl_up_sync(0xffffffffu, k.lo, 1);
-            const bool bad = v && lane > 0 &&
-                             (window64(kp, f) >> POS_BITS) == (window64(k, f) >> POS_BITS) &&
-                             key_lt(k, kp);
-            if (__any_sync(0xffffffffu, bad)) {
-#pragma unroll
-                for (int kk = 2; kk <= 32; kk <<= 1) {
-#pragma unroll
-                    for (int j = kk >> 1; j > 0; j >>= 1) {
-                        Key ok;
-                        ok.hi = __shfl_xor_sync(0xffffffffu, k.hi, j);
-                        ok.lo = __shfl_xor_sync(0xffffffffu, k.lo, j);
-                        const uint32_t oi = __shfl_xor_sync(0xffffffffu, id, j);
-                        const bool keep_min = ((lane & j) == 0) == ((lane & kk) == 0);
-                        const bool take =
-                            keep_min ? pair_lt(ok, oi, k, id) : pair_lt(k, id, ok, oi);
-                        if (take) {
-                            k = ok;
-                            id = oi;
-                        }
-                    }
-                }
-            }
-        }
-        Key prev, next;
-        prev.hi = __shfl_up_sync(0xffffffffu, k.hi, 1);
-        prev.lo = __shfl_up_sync(0xffffffffu, k.lo, 1);
-        next.hi = __shfl_down_sync(0xffffffffu, k.hi, 1);
-        next.lo = __shfl_down_sync(0xffffffffu, k.lo, 1);
-        const bool head = v && (lane == 0 || !key_eq(prev, k));
-        const uint32_t heads = __ballot_sync(0xffffffffu, head);
-        bool want = false;
-        uint32_t h = 0;
-        if (v) {
-            const uint32_t p = s.start + lane;
-            a.idx[0][p] = id;
-            if (lane == 0 || lane == s.len - 1) a.key[0][p] = from_key(k);
-            if (lane > 0) {
-                if (!key_eq(prev, k))
-                    a.lcp[p] = s.depth + key_lcp(prev, k);
-                else if (key_is_end(k))
-                    a.lcp[p] = s.depth + key_len(k);
-            }
-            const bool tail = lane == s.len - 1 || !key_eq(next, k);
-            if (tail && !head && !key_is_end(k)) {
-                const uint32_t m = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
-                h = 31 - __clz(heads & m);
-                want = true;
-            }
-        }
-        emit_next_warp(N, c, want, s.start + h, lane - h + 1, s.depth + KEY_BYTES);
+        if (s.len > 8) warp1_group<32>(a, s, lane, N, c);
     }
-    if (lane == 0 && (fresh | keyed)) {
+    if ((lane & 7) == 0 && (fresh | keyed)) {  // each 8-lane group's leader
         atomicAdd(&c->warp1_fresh, fresh);
         atomicAdd(&c->warp1_keyed, keyed);
     }
