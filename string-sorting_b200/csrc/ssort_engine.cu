@@ -47,12 +47,76 @@ int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const ui
     return SSORT_OK;
 }
 
+// Marks, on the partition stream, the point after which the list entries
+// counted in h_ctr are ready for the on-chip sorts.
+int ssort_ctx::fork_small() {
+    if (overlap_round) SS_CUDA(cudaEventRecord(ev_fork, st));
+    return SSORT_OK;
+}
+
+// Launches the on-chip sorts (warp, CTA and equality-bucket work) for the
+// list entries appended since the last call, as counted in h_ctr.  They work
+// on positions that no later partition level of the round touches, and they
+// append next-round segments with atomics, so they may run concurrently with
+// the partition levels on the side stream.
+int ssort_ctx::launch_small(const SortArgs &a, Seg *nxt, SmallDone &d) {
+    const bool overlap = overlap_round;
+    cudaStream_t s2 = overlap ? side : st;
+    if (overlap) SS_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));  // recorded by fork_small
+    Counters *dc = ws.ctr;
+    // One pass of CTAs over the entries (no CTA loops over several): short
+    // CTAs let the scheduler give SMs back to the partition kernels.  The
+    // packed warp sort keeps a capped grid: its warps loop over entries.
+    auto grid = [&](uint32_t n, uint32_t per_cta) { return (int)((n + per_cta - 1) / per_cta); };
+    uint32_t n = h_ctr->n_w1 - d.w1;
+    LAUNCH(this, "warp1",
+           launch_warp1(a, ws.W1 + d.w1, n, nxt, dc, std::min(grid(n, 32), grid_for(8)), s2));
+    d.w1 += n;
+    n = h_ctr->n_w8 - d.w8;
+    LAUNCH(this, "warp8", launch_warp8(a, ws.W8 + d.w8, n, nxt, dc, grid(n, 8), s2));
+    d.w8 += n;
+    // CTA-sort size classes: groups of 64, 128, 256 threads per segment.
+    Seg *lists[3] = {ws.S, ws.S2, ws.S3};
+    const uint32_t counts[3] = {h_ctr->n_small, h_ctr->n_small2, h_ctr->n_small3};
+    for (int k = 0; k < 3; ++k) {
+        n = counts[k] - d.s[k];
+        const uint32_t per_cta = (uint32_t)SMALL_THREADS / (64u << k);
+        LAUNCH(this, "block",
+               launch_block(a, lists[k] + d.s[k], n, k, nxt, dc, grid(n, per_cta), s2));
+        d.s[k] += n;
+    }
+    n = h_ctr->n_equal - d.e;
+    LAUNCH(this, "equal", launch_equal(a, ws.E + d.e, n, nxt, dc, grid(n, 1), s2));
+    d.e += n;
+    return SSORT_OK;
+}
+
 // One refinement round over the n_cur segments in `cur`: classification,
 // key gather and sample partitioning of large segments, on-chip sorts,
 // equality buckets and boundary LCPs.  The next round's segments are
 // appended to `nxt`; their count is returned in n_next.
 int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint32_t &n_next,
                      uint32_t round_no) {
+    // Overlap the on-chip sorts with the partition in round 0 only: from
+    // round 1 on, the first partition level gathers keys at random, a
+    // latency-bound kernel that measured slower when it shares its SMs.
+    overlap_round = side && hp && !prof && round_no == 0;
+    if (!overlap_round) return round_body(a, cur, n_cur, nxt, n_next, round_no);
+    // Fork the round onto the high-priority stream and join it back.
+    cudaStream_t user = st;
+    SS_CUDA(cudaEventRecord(ev_round, user));
+    SS_CUDA(cudaStreamWaitEvent(hp, ev_round, 0));
+    st = hp;
+    const int rc = round_body(a, cur, n_cur, nxt, n_next, round_no);
+    st = user;
+    if (rc != SSORT_OK) return rc;
+    SS_CUDA(cudaEventRecord(ev_round, hp));
+    SS_CUDA(cudaStreamWaitEvent(user, ev_round, 0));
+    return SSORT_OK;
+}
+
+int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
+                          uint32_t &n_next, uint32_t round_no) {
     Counters *dc = ws.ctr;
     const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
     SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
@@ -61,6 +125,11 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
                            dc, st));
     SS_TRY(sync_counters());
     if (round_no < SSORT_MAX_ROUNDS) stats.live[round_no] = h_ctr->live_next;
+    // The on-chip sorts of the segments known after each host read of the
+    // counters are launched on the side stream after the next partition
+    // level is enqueued, so that the level's kernels get the SMs first.
+    SmallDone done;
+    SS_TRY(fork_small());
     uint32_t n_large = h_ctr->n_large;
     Seg *lcur = ws.L, *lnext = ws.L2;
     // Keys of the large segments at this depth.  In round 0 the indices are
@@ -103,28 +172,18 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
                            ws.nspl, ws.cm_base,
                            ws.cm, ws.W1, ws.W8, SmallLists{{ws.S, ws.S2, ws.S3}}, lnext,
                            ws.E, ws.B, nxt, dc, st));
+        SS_TRY(launch_small(a, nxt, done));  // segments known before this level
         SS_TRY(sync_counters());
+        SS_TRY(fork_small());
         n_large = h_ctr->n_large_next;
         SS_CUDA(cudaMemsetAsync(&dc->n_large_next, 0, 4, st));
         std::swap(lcur, lnext);
     }
-    LAUNCH(this, "warp1", launch_warp1(a, ws.W1, nxt, dc, g8, st));
-    LAUNCH(this, "warp8", launch_warp8(a, ws.W8, nxt, dc, g8, st));
-    {
-        // CTA-sort size classes: groups of 64, 128, 256 threads per segment.
-        // The counts are current: the host read them after the last
-        // classification or partition level.
-        Seg *lists[3] = {ws.S, ws.S2, ws.S3};
-        const uint32_t counts[3] = {h_ctr->n_small, h_ctr->n_small2, h_ctr->n_small3};
-        for (int k = 0; k < 3; ++k) {
-            if (!counts[k]) continue;
-            const uint32_t per_cta = (uint32_t)SMALL_THREADS / (64u << k);
-            const int grid = (int)std::min<uint32_t>((uint32_t)g8,
-                                                     (counts[k] + per_cta - 1) / per_cta);
-            LAUNCH(this, "block", launch_block(a, lists[k], k, nxt, dc, grid, st));
-        }
+    SS_TRY(launch_small(a, nxt, done));  // the rest
+    if (overlap_round) {
+        SS_CUDA(cudaEventRecord(ev_join, side));
+        SS_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     }
-    LAUNCH(this, "equal", launch_equal(a, ws.E, nxt, dc, g8, st));
     LAUNCH(this, "boundary", launch_boundary(a, ws.B, dc, g4, st));
     SS_TRY(sync_counters());
     stats.small_segments +=
@@ -226,6 +285,8 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
                       ninst);
     if (rc != SSORT_OK) {
         cudaStreamSynchronize(ctx->st);
+        if (ctx->side) cudaStreamSynchronize(ctx->side);
+        if (ctx->hp) cudaStreamSynchronize(ctx->hp);
         ctx->recs.clear();
         ctx->ev_used = 0;
         return rc;
@@ -301,6 +362,13 @@ int ssort_ctx_create(int device, ssort_ctx **out) {
     int rc = with_device(ctx, [&]() -> int {
         SS_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
         SS_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+        int least = 0, greatest = 0;
+        SS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        SS_CUDA(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, least));
+        SS_CUDA(cudaStreamCreateWithPriority(&ctx->hp, cudaStreamNonBlocking, greatest));
+        SS_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+        SS_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+        SS_CUDA(cudaEventCreateWithFlags(&ctx->ev_round, cudaEventDisableTiming));
         SS_CUDA(cudaEventCreate(&ctx->ev_start));
         SS_CUDA(cudaEventCreate(&ctx->ev_stop));
         ctx->st = ctx->own_stream;
@@ -327,6 +395,13 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
         for (auto e : ctx->ev_pool) cudaEventDestroy(e);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+        if (ctx->side) cudaStreamSynchronize(ctx->side);
+        if (ctx->hp) cudaStreamSynchronize(ctx->hp);
+        if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+        if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+        if (ctx->ev_round) cudaEventDestroy(ctx->ev_round);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->hp) cudaStreamDestroy(ctx->hp);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         return SSORT_OK;
     });

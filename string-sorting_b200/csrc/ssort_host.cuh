@@ -45,6 +45,16 @@ struct ssort_ctx {
     int num_sms = 148;
     cudaStream_t own_stream = nullptr;
     cudaStream_t st = nullptr;
+    // The on-chip sorts of a round run on `side` while the partition levels
+    // continue on `st` (fork/join through the two events).  Without a side
+    // stream, or while profiling, they run on `st`.
+    // Within a round the partition levels run on `hp` (highest priority,
+    // forked from and joined back into `st`) and the on-chip sorts on `side`
+    // (lowest priority), so that the CTA scheduler serves the partition's
+    // critical path first and the sorts fill the SMs it leaves idle.
+    cudaStream_t side = nullptr, hp = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_round = nullptr;
+    bool overlap_round = false;  // this round runs its on-chip sorts on `side`
 
     // workspace
     ssort::DBuf ws_buf;    // one block holding every scratch buffer (ws_layout)
@@ -151,6 +161,14 @@ struct ssort_ctx {
     int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
             uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
             uint32_t ninst = 0);
+    // List entries of the on-chip sorts already launched in this round.
+    struct SmallDone {
+        uint32_t w1 = 0, w8 = 0, s[3] = {0, 0, 0}, e = 0;
+    };
+    int fork_small();
+    int launch_small(const ssort::SortArgs &a, ssort::Seg *nxt, SmallDone &done);
+    int round_body(const ssort::SortArgs &a, ssort::Seg *cur, uint32_t n_cur, ssort::Seg *nxt,
+                   uint32_t &n_next, uint32_t round_no);
     int round(const ssort::SortArgs &a, ssort::Seg *cur, uint32_t n_cur, ssort::Seg *nxt,
               uint32_t &n_next,
               uint32_t round_no);

@@ -261,14 +261,16 @@ void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *t
                  Seg *W1, Seg *W8, SmallLists S, Seg *L2, Seg *E, uint2 *B, Seg *N,
                  Counters *c, cudaStream_t st);
 // On-chip segment sorts; list lengths are read from the counters on the device.
-void launch_warp1(const SortArgs &a, const Seg *W1, Seg *N, Counters *c, int grid,
+// The on-chip sorts take n list entries from the given list pointer (a range
+// of the list), so that they can run while the list is still being appended.
+void launch_warp1(const SortArgs &a, const Seg *W1, uint32_t n, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
-void launch_warp8(const SortArgs &a, const Seg *W8, Seg *N, Counters *c, int grid,
+void launch_warp8(const SortArgs &a, const Seg *W8, uint32_t n, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
 // cls: size class 0, 1, 2 (segment list S holds that class)
-void launch_block(const SortArgs &a, const Seg *S, int cls, Seg *N, Counters *c, int grid,
-                  cudaStream_t st);
-void launch_equal(const SortArgs &a, const Seg *E, Seg *N, Counters *c, int grid,
+void launch_block(const SortArgs &a, const Seg *S, uint32_t n, int cls, Seg *N, Counters *c,
+                  int grid, cudaStream_t st);
+void launch_equal(const SortArgs &a, const Seg *E, uint32_t n, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
 void launch_boundary(const SortArgs &a, const uint2 *B, Counters *c, int grid, cudaStream_t st);
 

@@ -1622,8 +1622,7 @@ __device__ __forceinline__ void warp1_group(const SortArgs &a, const Seg &s, uin
 constexpr uint32_t W1_PACK = 4;
 
 __global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *__restrict__ T,
-                                                        Seg *N, Counters *c) {
-    const uint32_t nT = c->n_w1;
+                                                        uint32_t nT, Seg *N, Counters *c) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1676,9 +1675,8 @@ constexpr size_t W8_SMEM = (size_t)W8_WARPS * W8_PAD * (sizeof(ulonglong2) + siz
                                                          sizeof(uint32_t));
 
 __global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg *__restrict__ T,
-                                                           Seg *N, Counters *c) {
+                                                           uint32_t nT, Seg *N, Counters *c) {
     extern __shared__ __align__(16) unsigned char w8_smem[];
-    const uint32_t nT = c->n_w8;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     ulonglong2 *sk = reinterpret_cast<ulonglong2 *>(w8_smem) + w * W8_PAD;
     uint64_t *sv = reinterpret_cast<uint64_t *>(reinterpret_cast<ulonglong2 *>(w8_smem) +
@@ -1953,14 +1951,12 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
 // three bodies and spills more; measured slower).
 template <int GT>
 __global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
-                                                            const uint32_t *n_list, Seg *N,
-                                                            Counters *c) {
-    block_class<GT>(a, S, *n_list, 0, gridDim.x, N, c);
+                                                            uint32_t nS, Seg *N, Counters *c) {
+    block_class<GT>(a, S, nS, 0, gridDim.x, N, c);
 }
 
 // ---- equality buckets: work items of up to EQ_TILE strings ------------------
-__global__ void k_equal(SortArgs a, const Seg *__restrict__ E, Seg *N, Counters *c) {
-    const uint32_t nE = c->n_equal;
+__global__ void k_equal(SortArgs a, const Seg *__restrict__ E, uint32_t nE, Seg *N, Counters *c) {
     unsigned long long moved = 0, fin = 0;
     for (uint32_t g = blockIdx.x; g < nE; g += gridDim.x) {
         const Seg s = E[g];
@@ -2164,23 +2160,26 @@ void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *t
                                c);
 }
 
-void launch_warp1(const SortArgs &a, const Seg *W1, Seg *N, Counters *c, int grid,
+void launch_warp1(const SortArgs &a, const Seg *W1, uint32_t n, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
-    k_warp1<<<grid, WARP_THREADS, 0, st>>>(a, W1, N, c);
+    if (!n) return;
+    k_warp1<<<grid, WARP_THREADS, 0, st>>>(a, W1, n, N, c);
 }
 
-void launch_warp8(const SortArgs &a, const Seg *W8, Seg *N, Counters *c, int grid,
+void launch_warp8(const SortArgs &a, const Seg *W8, uint32_t n, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
+    if (!n) return;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_warp8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W8_SMEM);
         attr = true;
     }
-    k_warp8<<<grid, WARP_THREADS, W8_SMEM, st>>>(a, W8, N, c);
+    k_warp8<<<grid, WARP_THREADS, W8_SMEM, st>>>(a, W8, n, N, c);
 }
 
-void launch_block(const SortArgs &a, const Seg *S, int cls, Seg *N, Counters *c, int grid,
-                  cudaStream_t st) {
+void launch_block(const SortArgs &a, const Seg *S, uint32_t n, int cls, Seg *N, Counters *c,
+                  int grid, cudaStream_t st) {
+    if (!n) return;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_block<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2192,16 +2191,17 @@ void launch_block(const SortArgs &a, const Seg *S, int cls, Seg *N, Counters *c,
         attr = true;
     }
     if (cls == 0)
-        k_block<64><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, &c->n_small, N, c);
+        k_block<64><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, n, N, c);
     else if (cls == 1)
-        k_block<128><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, &c->n_small2, N, c);
+        k_block<128><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, n, N, c);
     else
-        k_block<256><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, &c->n_small3, N, c);
+        k_block<256><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, n, N, c);
 }
 
-void launch_equal(const SortArgs &a, const Seg *E, Seg *N, Counters *c, int grid,
+void launch_equal(const SortArgs &a, const Seg *E, uint32_t n, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
-    k_equal<<<grid, 256, 0, st>>>(a, E, N, c);
+    if (!n) return;
+    k_equal<<<grid, 256, 0, st>>>(a, E, n, N, c);
 }
 
 void launch_boundary(const SortArgs &a, const uint2 *B, Counters *c, int grid, cudaStream_t st) {
