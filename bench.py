@@ -159,12 +159,19 @@ class Clocks:
 # ---- algorithmic bytes -----------------------------------------------------------
 KB = 16  # key bytes per round
 
-# DRAM bytes (read + write) per string handled, from one ncu capture of a small
-# case of the same kernel (10 M Zipf words for count and scatter); scaled by
-# the strings a launch handles to give `roofline.traffic` per launch.
+# DRAM bytes (read + write) per string handled, from one ncu capture of every
+# launch of three sorts of 10 M URLs (dram__bytes_read/write summed per kernel
+# and divided by the strings the kernel handled); scaled by the strings a
+# launch handles to give `roofline.traffic` per launch.  Writes that stay in
+# L2 until a later kernel evicts them are not counted here.
 TRAFFIC_PER_STRING = {
-    "count": 16.8,
-    "scatter": 48.8,
+    "count_gather": 219.8,  # random offset + key reads (>= 32-byte sectors each)
+    "gather": 80.4,         # round 0: the arena streamed in order
+    "count": 17.9,
+    "scatter": 36.3,
+    "block": 57.2,
+    "warp8": 195.0,
+    "warp1": 261.0,
 }
 
 
