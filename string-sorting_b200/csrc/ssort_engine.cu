@@ -97,10 +97,13 @@ int ssort_ctx::launch_small(const SortArgs &a, Seg *nxt, SmallDone &d) {
 // appended to `nxt`; their count is returned in n_next.
 int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint32_t &n_next,
                      uint32_t round_no) {
-    // Overlap the on-chip sorts with the partition in round 0 only: from
-    // round 1 on, the first partition level gathers keys at random, a
-    // latency-bound kernel that measured slower when it shares its SMs.
-    overlap_round = side && hp && !prof && round_no == 0;
+    // A fresh round (round 0 of a sort, or by the caller's choice) streams
+    // the arena in index order with a separate gather and overlaps the
+    // on-chip sorts with the partition; a deep round gathers keys at random
+    // inside the first count and keeps one stream (the random gather is
+    // latency-bound and measured slower when it shares its SMs).
+    fresh_round = round_mode >= 0 ? round_mode == 0 : round_no == 0;
+    overlap_round = side && hp && !prof && fresh_round;
     if (!overlap_round) return round_body(a, cur, n_cur, nxt, n_next, round_no);
     // Fork the round onto the high-priority stream and join it back.
     cudaStream_t user = st;
@@ -136,7 +139,7 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     // the identity, so a separate gather streams the arena in order; later
     // rounds read it at random, and the count kernel of the first partition
     // level gathers the keys itself so that those reads overlap its work.
-    const bool fused_gather = round_no > 0;
+    const bool fused_gather = !fresh_round;
     if (n_large && !fused_gather) {
         LAUNCH(this, "seg_tiles",
                launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));

@@ -55,6 +55,8 @@ struct ssort_ctx {
     cudaStream_t side = nullptr, hp = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_round = nullptr;
     bool overlap_round = false;  // this round runs its on-chip sorts on `side`
+    bool fresh_round = false;    // this round gathers round-0 style (see round())
+    int round_mode = -1;         // -1: fresh iff round_no == 0; 0: fresh; 1: deep
 
     // workspace
     ssort::DBuf ws_buf;    // one block holding every scratch buffer (ws_layout)

@@ -120,6 +120,8 @@ struct ssort_server {
     Seg *cur = nullptr, *nxt = nullptr;
     uint32_t n_cur = 0;
     uint64_t rounds = 0, requests_done = 0, strings_done = 0;
+    uint64_t joined_strings = 0;  // strings joined in this step
+    uint64_t prev_live = 0;       // strings live in the last round
     uint32_t max_active = 0;
     int error = SSORT_OK;
     std::string error_msg;
@@ -225,6 +227,7 @@ int ssort_server::join() {
                            (uint32_t)r->pos, r->n, r->region, r->arena_bytes, r->off_width, cur,
                            n_cur, ctx->st));
         if (r->n >= 2) ++n_cur;
+        joined_strings += r->n;
         r->state = SSORT_REQ_ACTIVE;
         active.push_back(r);
     }
@@ -304,11 +307,16 @@ int ssort_server::retire() {
 int ssort_server::step_locked() {
     SS_TRY(retire());
     SS_TRY(admit());
+    joined_strings = 0;
     SS_TRY(join());
     if (n_cur) {
         uint32_t n_next = 0;
+        // Mostly newly joined strings (identity indices, request bytes laid
+        // out in order in the pool): a fresh round; else a deep one.
+        ctx->round_mode = joined_strings * 2 >= prev_live ? 0 : 1;
         SS_TRY(ctx->round(args(), cur, n_cur, nxt, n_next, (uint32_t)std::min<uint64_t>(
                                                                 rounds, UINT32_MAX)));
+        prev_live = ctx->h_ctr->live_next;
         std::swap(cur, nxt);
         n_cur = n_next;
         ++rounds;
