@@ -224,12 +224,20 @@ void launch_text_starts(uint8_t *text, uint64_t len, uint8_t delim, const uint32
 void launch_iota_offs(void *offs, int off_width, uint64_t n, cudaStream_t st);
 void launch_sorted_offs(const uint32_t *perm, const void *offs, int off_width, uint64_t n,
                         uint64_t *out, cudaStream_t st);
-void launch_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, uint32_t pos_base, uint32_t n,
-                 uint64_t region_base, uint64_t arena_bytes, int off_width, Seg *R, uint32_t slot,
-                 cudaStream_t st);
+// One request joining or leaving the server's batch (see k_join / k_unbase).
+struct ReqJob {
+    uint64_t region_base, arena_bytes;
+    uint32_t pos, n;
+    uint32_t first;  // positions of the jobs before this one
+    uint32_t slot;   // segment slot in the round list (requests of >= 2 strings)
+    uint32_t off_width, pad;
+};
+void launch_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, const ReqJob *jobs,
+                 uint32_t njobs, uint32_t total, Seg *R, cudaStream_t st);
 void launch_mark(const Seg *R, uint32_t nR, const uint32_t *base, uint32_t nact, uint32_t *flag,
                  cudaStream_t st);
-void launch_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n, cudaStream_t st);
+void launch_unbase(uint32_t *perm, const ReqJob *jobs, uint32_t njobs, uint32_t total,
+                   cudaStream_t st);
 void launch_localize(uint32_t *perm, uint32_t n, const uint32_t *inst_start, uint32_t ninst,
                      cudaStream_t st);
 // Single-CTA scans of short per-segment arrays (out*[n] = totals).

@@ -610,27 +610,47 @@ __global__ void k_localize(uint32_t *perm, uint32_t n, const uint32_t *__restric
 }
 
 // ---- request server: joining and retiring requests between rounds ----------
-// Joins one admitted request at positions [pos_base, pos_base + n) whose bytes
-// sit at region_base in the pool arena.  Its offsets arrive either as uint64
-// in place in goffs or as uint32 staged in lcp at its positions; each becomes
-// a pool offset.  An offset at or past the request's own arena_bytes is
-// clamped to arena_bytes, where the server stores a NUL byte: the same empty
-// string the single-request sort reads past the end of its arena.  Positions
-// get their identity index, lcp of the first position becomes 0, and the
-// request's positions become one depth-0 segment at R[slot].
-__global__ void k_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, uint32_t pos_base,
-                       uint32_t n, uint64_t region_base, uint64_t arena_bytes, int off_width,
-                       Seg *R, uint32_t slot) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += gridDim.x * blockDim.x) {
-        const uint32_t p = pos_base + i;
-        uint64_t o = off_width == 4 ? (uint64_t)lcp[p] : goffs[p];
-        if (o > arena_bytes) o = arena_bytes;
-        goffs[p] = region_base + o;
-        perm[p] = p;
-        if (i == 0) lcp[p] = 0;
+// The requests of one step are described by ReqJob records; a flat index q
+// over all their positions (jobs[j].first = positions of the jobs before j)
+// finds its job by binary search.
+__device__ __forceinline__ uint32_t find_job(const ReqJob *__restrict__ jobs, uint32_t njobs,
+                                             uint32_t q) {
+    uint32_t lo = 0, hi = njobs;  // largest j with jobs[j].first <= q
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (jobs[mid].first <= q)
+            lo = mid;
+        else
+            hi = mid;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && n >= 2) R[slot] = Seg{pos_base, n, 0, 0};
+    return lo;
+}
+
+// Joins admitted requests: request j occupies positions [pos, pos + n) and its
+// bytes sit at region_base in the pool arena.  Its offsets arrive either as
+// uint64 in place in goffs or as uint32 staged in lcp at its positions; each
+// becomes a pool offset.  An offset at or past the request's own arena_bytes
+// is clamped to arena_bytes, where the server stores a NUL byte: the same
+// empty string the single-request sort reads past the end of its arena.
+// Positions get their identity index, lcp of the first position becomes 0,
+// and a request of two or more strings becomes one depth-0 segment at
+// R[slot].
+__global__ void k_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm,
+                       const ReqJob *__restrict__ jobs, uint32_t njobs, uint32_t total, Seg *R) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += gridDim.x * blockDim.x) {
+        const ReqJob jb = jobs[find_job(jobs, njobs, q)];
+        const uint32_t i = q - jb.first;
+        const uint32_t p = jb.pos + i;
+        uint64_t o = jb.off_width == 4 ? (uint64_t)lcp[p] : goffs[p];
+        if (o > jb.arena_bytes) o = jb.arena_bytes;
+        goffs[p] = jb.region_base + o;
+        perm[p] = p;
+        if (i == 0) {
+            lcp[p] = 0;
+            if (jb.n >= 2) R[jb.slot] = Seg{jb.pos, jb.n, 0, 0};
+        }
+    }
 }
 
 // flag[j] = 1 for every active request j that still owns a segment of R;
@@ -652,11 +672,14 @@ __global__ void k_mark(const Seg *__restrict__ R, uint32_t nR, const uint32_t *_
     }
 }
 
-// Global positions of one finished request -> indices within the request.
-__global__ void k_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += gridDim.x * blockDim.x)
-        perm[pos_base + i] -= pos_base;
+// Global positions of finished requests -> indices within each request.
+__global__ void k_unbase(uint32_t *perm, const ReqJob *__restrict__ jobs, uint32_t njobs,
+                         uint32_t total) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += gridDim.x * blockDim.x) {
+        const ReqJob jb = jobs[find_job(jobs, njobs, q)];
+        perm[jb.pos + (q - jb.first)] -= jb.pos;
+    }
 }
 
 // ---- text inputs: string starts in a delimited text ---------------------------
@@ -2024,12 +2047,11 @@ void launch_localize(uint32_t *perm, uint32_t n, const uint32_t *inst_start, uin
     k_localize<<<g ? g : 1, 256, 0, st>>>(perm, n, inst_start, ninst);
 }
 
-void launch_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, uint32_t pos_base, uint32_t n,
-                 uint64_t region_base, uint64_t arena_bytes, int off_width, Seg *R, uint32_t slot,
-                 cudaStream_t st) {
-    const uint32_t g = cdiv(n, 256) < 148 * 8 ? cdiv(n, 256) : 148 * 8;
-    k_join<<<g ? g : 1, 256, 0, st>>>(goffs, lcp, perm, pos_base, n, region_base, arena_bytes,
-                                      off_width, R, slot);
+void launch_join(uint64_t *goffs, uint32_t *lcp, uint32_t *perm, const ReqJob *jobs,
+                 uint32_t njobs, uint32_t total, Seg *R, cudaStream_t st) {
+    if (!njobs || !total) return;
+    const uint32_t g = cdiv(total, 256) < 148 * 8 ? cdiv(total, 256) : 148 * 8;
+    k_join<<<g, 256, 0, st>>>(goffs, lcp, perm, jobs, njobs, total, R);
 }
 
 void launch_mark(const Seg *R, uint32_t nR, const uint32_t *base, uint32_t nact, uint32_t *flag,
@@ -2039,10 +2061,11 @@ void launch_mark(const Seg *R, uint32_t nR, const uint32_t *base, uint32_t nact,
     k_mark<<<g, 256, 0, st>>>(R, nR, base, nact, flag);
 }
 
-void launch_unbase(uint32_t *perm, uint32_t pos_base, uint32_t n, cudaStream_t st) {
-    if (!n) return;
-    const uint32_t g = cdiv(n, 256) < 148 * 8 ? cdiv(n, 256) : 148 * 8;
-    k_unbase<<<g, 256, 0, st>>>(perm, pos_base, n);
+void launch_unbase(uint32_t *perm, const ReqJob *jobs, uint32_t njobs, uint32_t total,
+                   cudaStream_t st) {
+    if (!njobs || !total) return;
+    const uint32_t g = cdiv(total, 256) < 148 * 8 ? cdiv(total, 256) : 148 * 8;
+    k_unbase<<<g, 256, 0, st>>>(perm, jobs, njobs, total);
 }
 
 uint64_t text_tiles(uint64_t len) { return (len + TEXT_TILE - 1) / TEXT_TILE; }

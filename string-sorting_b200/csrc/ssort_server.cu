@@ -108,8 +108,11 @@ struct ssort_server {
     cudaStream_t h2d = nullptr, d2h = nullptr;  // copy-in and copy-out streams
     uint64_t budget = 0;
     uint32_t max_strings = 0;
-    DBuf pool, goffs, perm, bases, flags;
+    DBuf pool, goffs, perm, bases, flags, d_join, d_done;
     uint32_t *h_bases = nullptr, *h_flags = nullptr;
+    ReqJob *h_join = nullptr, *h_done = nullptr;  // pinned job tables
+    cudaEvent_t ev_join_jobs = nullptr, ev_done_jobs = nullptr, ev_unbased = nullptr;
+    bool join_jobs_pending = false, done_jobs_pending = false;
     RangeAlloc arena_alloc, pos_alloc;
     std::deque<Request *> queue;
     std::vector<Request *> loading, active, draining;
@@ -162,7 +165,7 @@ struct ssort_server {
 
     int admit();
     int join();
-    int finish(Request *r);
+    int finish(const std::vector<Request *> &done);
     int detect();
     int retire();
     int step_locked();
@@ -209,11 +212,20 @@ int ssort_server::admit() {
     return SSORT_OK;
 }
 
-// Requests whose copies have landed join the segment list; with no round in
-// progress every loading request joins and the compute stream waits for it.
+// Waits until the previous host-to-device copy out of a job table has run,
+// so that the pinned table can be refilled.
+static int jobs_free(cudaEvent_t ev, bool &pending) {
+    if (pending) SS_CUDA(cudaEventSynchronize(ev));
+    pending = false;
+    return SSORT_OK;
+}
+
+// Requests whose copies have landed join the segment list (one launch for
+// all of them); with no round in progress every loading request joins and
+// the compute stream waits for its copies.
 int ssort_server::join() {
     const bool idle = n_cur == 0 && active.empty();
-    std::vector<Request *> still;
+    std::vector<Request *> still, joined;
     for (Request *r : loading) {
         cudaError_t q = cudaEventQuery(r->ev);
         if (q != cudaSuccess && q != cudaErrorNotReady) return cuda_fail(q, "copy-in event");
@@ -222,35 +234,75 @@ int ssort_server::join() {
             continue;
         }
         SS_CUDA(cudaStreamWaitEvent(ctx->st, r->ev, 0));
-        LAUNCH(ctx, "join",
-               launch_join((uint64_t *)goffs.p, ctx->ws.lcp, (uint32_t *)perm.p,
-                           (uint32_t)r->pos, r->n, r->region, r->arena_bytes, r->off_width, cur,
-                           n_cur, ctx->st));
-        if (r->n >= 2) ++n_cur;
+        joined.push_back(r);
+    }
+    loading.swap(still);
+    if (joined.empty()) return SSORT_OK;
+    SS_TRY(jobs_free(ev_join_jobs, join_jobs_pending));
+    uint32_t total = 0;
+    for (size_t k = 0; k < joined.size(); ++k) {
+        Request *r = joined[k];
+        ReqJob &jb = h_join[k];
+        jb.region_base = r->region;
+        jb.arena_bytes = r->arena_bytes;
+        jb.pos = (uint32_t)r->pos;
+        jb.n = r->n;
+        jb.first = total;
+        jb.slot = r->n >= 2 ? n_cur++ : 0u;
+        jb.off_width = (uint32_t)r->off_width;
+        jb.pad = 0;
+        total += r->n;
         joined_strings += r->n;
         r->state = SSORT_REQ_ACTIVE;
         active.push_back(r);
     }
-    loading.swap(still);
+    const uint32_t nj = (uint32_t)joined.size();
+    SS_CUDA(cudaMemcpyAsync(d_join.p, h_join, nj * sizeof(ReqJob), cudaMemcpyHostToDevice,
+                            ctx->st));
+    SS_CUDA(cudaEventRecord(ev_join_jobs, ctx->st));
+    join_jobs_pending = true;
+    LAUNCH(ctx, "join",
+           launch_join((uint64_t *)goffs.p, ctx->ws.lcp, (uint32_t *)perm.p,
+                       (const ReqJob *)d_join.p, nj, total, cur, ctx->st));
     max_active = std::max<uint32_t>(max_active, (uint32_t)active.size());
     return SSORT_OK;
 }
 
-// Request-local indices, then the copy-out on the device-to-host stream.
-int ssort_server::finish(Request *r) {
-    LAUNCH(ctx, "unbase", launch_unbase((uint32_t *)perm.p, (uint32_t)r->pos, r->n, ctx->st));
-    SS_CUDA(cudaEventRecord(r->ev, ctx->st));
-    SS_CUDA(cudaStreamWaitEvent(d2h, r->ev, 0));
-    if (r->n) {
-        SS_CUDA(cudaMemcpyAsync(r->perm_out, (uint32_t *)perm.p + r->pos, (size_t)r->n * 4,
-                                cudaMemcpyDefault, d2h));
-        if (r->lcp_out)
-            SS_CUDA(cudaMemcpyAsync(r->lcp_out, ctx->ws.lcp + r->pos, (size_t)r->n * 4,
-                                    cudaMemcpyDefault, d2h));
+// Request-local indices for all finished requests (one launch), then each
+// request's copy-out on the device-to-host stream.
+int ssort_server::finish(const std::vector<Request *> &done) {
+    if (done.empty()) return SSORT_OK;
+    SS_TRY(jobs_free(ev_done_jobs, done_jobs_pending));
+    uint32_t total = 0;
+    for (size_t k = 0; k < done.size(); ++k) {
+        ReqJob &jb = h_done[k];
+        jb = ReqJob{};
+        jb.pos = (uint32_t)done[k]->pos;
+        jb.n = done[k]->n;
+        jb.first = total;
+        total += done[k]->n;
     }
-    SS_CUDA(cudaEventRecord(r->ev, d2h));
-    r->state = SSORT_REQ_DRAINING;
-    draining.push_back(r);
+    const uint32_t nd = (uint32_t)done.size();
+    SS_CUDA(cudaMemcpyAsync(d_done.p, h_done, nd * sizeof(ReqJob), cudaMemcpyHostToDevice,
+                            ctx->st));
+    SS_CUDA(cudaEventRecord(ev_done_jobs, ctx->st));
+    done_jobs_pending = true;
+    LAUNCH(ctx, "unbase",
+           launch_unbase((uint32_t *)perm.p, (const ReqJob *)d_done.p, nd, total, ctx->st));
+    SS_CUDA(cudaEventRecord(ev_unbased, ctx->st));
+    SS_CUDA(cudaStreamWaitEvent(d2h, ev_unbased, 0));
+    for (Request *r : done) {
+        if (r->n) {
+            SS_CUDA(cudaMemcpyAsync(r->perm_out, (uint32_t *)perm.p + r->pos, (size_t)r->n * 4,
+                                    cudaMemcpyDefault, d2h));
+            if (r->lcp_out)
+                SS_CUDA(cudaMemcpyAsync(r->lcp_out, ctx->ws.lcp + r->pos, (size_t)r->n * 4,
+                                        cudaMemcpyDefault, d2h));
+        }
+        SS_CUDA(cudaEventRecord(r->ev, d2h));
+        r->state = SSORT_REQ_DRAINING;
+        draining.push_back(r);
+    }
     return SSORT_OK;
 }
 
@@ -276,8 +328,7 @@ int ssort_server::detect() {
         for (uint32_t j = 0; j < nact; ++j) (h_flags[j] ? keep : done).push_back(active[j]);
         active.swap(keep);
     }
-    for (Request *r : done) SS_TRY(finish(r));
-    return SSORT_OK;
+    return finish(done);
 }
 
 // Requests whose copy-out has completed release their pool region and
@@ -337,10 +388,15 @@ void server_free(ssort_server *srv) {
             if (srv->h2d) cudaStreamSynchronize(srv->h2d);
             if (srv->d2h) cudaStreamSynchronize(srv->d2h);
             cudaStreamSynchronize(srv->ctx->st);
-            for (DBuf *b : {&srv->pool, &srv->goffs, &srv->perm, &srv->bases, &srv->flags})
+            for (DBuf *b : {&srv->pool, &srv->goffs, &srv->perm, &srv->bases, &srv->flags,
+                            &srv->d_join, &srv->d_done})
                 if (b->p) cudaFree(b->p);
             if (srv->h_bases) cudaFreeHost(srv->h_bases);
             if (srv->h_flags) cudaFreeHost(srv->h_flags);
+            if (srv->h_join) cudaFreeHost(srv->h_join);
+            if (srv->h_done) cudaFreeHost(srv->h_done);
+            for (cudaEvent_t e : {srv->ev_join_jobs, srv->ev_done_jobs, srv->ev_unbased})
+                if (e) cudaEventDestroy(e);
             for (auto &kv : srv->by_id) {
                 if (kv.second->ev) cudaEventDestroy(kv.second->ev);
                 delete kv.second;
@@ -384,6 +440,15 @@ int ssort_server_create(int device, uint64_t arena_budget_bytes, uint64_t max_st
         SS_TRY(ctx->ensure(srv->flags, (size_t)MAX_SLOTS * 4));
         SS_CUDA(cudaHostAlloc((void **)&srv->h_bases, (size_t)MAX_SLOTS * 4, cudaHostAllocDefault));
         SS_CUDA(cudaHostAlloc((void **)&srv->h_flags, (size_t)MAX_SLOTS * 4, cudaHostAllocDefault));
+        SS_TRY(ctx->ensure(srv->d_join, (size_t)MAX_SLOTS * sizeof(ReqJob)));
+        SS_TRY(ctx->ensure(srv->d_done, (size_t)MAX_SLOTS * sizeof(ReqJob)));
+        SS_CUDA(cudaHostAlloc((void **)&srv->h_join, (size_t)MAX_SLOTS * sizeof(ReqJob),
+                              cudaHostAllocDefault));
+        SS_CUDA(cudaHostAlloc((void **)&srv->h_done, (size_t)MAX_SLOTS * sizeof(ReqJob),
+                              cudaHostAllocDefault));
+        SS_CUDA(cudaEventCreateWithFlags(&srv->ev_join_jobs, cudaEventDisableTiming));
+        SS_CUDA(cudaEventCreateWithFlags(&srv->ev_done_jobs, cudaEventDisableTiming));
+        SS_CUDA(cudaEventCreateWithFlags(&srv->ev_unbased, cudaEventDisableTiming));
         return SSORT_OK;
     });
     if (rc != SSORT_OK) {
@@ -491,7 +556,9 @@ int ssort_server_get_info(ssort_server *srv, ssort_server_info *out) {
     i.arena_budget = srv->budget;
     i.max_strings = srv->max_strings;
     size_t held = srv->ctx->ws_buf.cap;
-    for (DBuf *b : {&srv->pool, &srv->goffs, &srv->perm, &srv->bases, &srv->flags}) held += b->cap;
+    for (DBuf *b : {&srv->pool, &srv->goffs, &srv->perm, &srv->bases, &srv->flags, &srv->d_join,
+                    &srv->d_done})
+        held += b->cap;
     i.device_bytes = held;
     *out = i;
     return SSORT_OK;
