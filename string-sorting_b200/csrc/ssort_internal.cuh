@@ -211,8 +211,6 @@ inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
 void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st);
 void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, SmallLists S, Seg *L,
                      Counters *c, cudaStream_t st);
-void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
-                        cudaStream_t st);
 // Batches: one round-0 segment per instance; instance-local result indices.
 void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
                        Counters *c, cudaStream_t st);

@@ -198,21 +198,12 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
     return v;
 }
 
-// Bucket of `key` among u sorted distinct splitters s[0..u) padded with the
-// all-ones key to kp2-1 entries: range bucket 2j holds s[j-1] < key < s[j],
-// equality bucket 2j+1 holds key == s[j].
-__device__ __forceinline__ uint32_t classify(const ulonglong2 *s, uint32_t kp2, uint32_t u,
-                                             const Key &key) {
-    uint32_t lo = 0;
-    for (uint32_t step = kp2 >> 1; step > 0; step >>= 1)
-        if (key_lt(to_key(s[lo + step - 1]), key)) lo += step;
-    return (lo < u && key_eq(to_key(s[lo]), key)) ? 2 * lo + 1 : 2 * lo;
-}
-
-// The same bucket through the lookup table T: splitters share their first f
-// bits; T[w] counts the splitters whose next TBL_BITS bits are below w, so a
-// key strictly between the first and last splitter (and hence sharing those
-// f bits) only needs a search among the splitters with its own window.
+// Bucket of `key` among u sorted distinct splitters s[0..u): range bucket 2j
+// holds s[j-1] < key < s[j], equality bucket 2j+1 holds key == s[j].  Found
+// through the lookup table T: splitters share their first f bits; T[w] counts
+// the splitters whose next TBL_BITS bits are below w, so a key strictly
+// between the first and last splitter (and hence sharing those f bits) only
+// needs a search among the splitters with its own window.
 __device__ __forceinline__ uint64_t window64(const Key &k, uint32_t f);
 
 __device__ __forceinline__ uint32_t window_bits(const Key &k, uint32_t f) {
@@ -860,12 +851,6 @@ __global__ void __launch_bounds__(SMALL_SCAN_THREADS) k_seg_tiles(const Seg *__r
         c += t;
     }
     if (threadIdx.x == 0) out[n] = c;
-}
-
-__global__ void k_tile_counts(const Seg *__restrict__ segs, uint32_t n, uint32_t tile,
-                              uint32_t *out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = (segs[i].len + tile - 1) / tile;
 }
 
 // ---- exclusive scan (u32), three phases ----------------------------------
@@ -2102,12 +2087,6 @@ void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, 
 
 void launch_seg_tiles(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out, cudaStream_t st) {
     k_seg_tiles<<<1, SMALL_SCAN_THREADS, 0, st>>>(segs, n, tile, out);
-}
-
-void launch_tile_counts(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out,
-                        cudaStream_t st) {
-    if (!n) return;
-    k_tile_counts<<<cdiv(n, 256), 256, 0, st>>>(segs, n, tile, out);
 }
 
 uint32_t scan_partials_needed(uint32_t n) { return cdiv(n ? n : 1, SCAN_CHUNK) + 1; }
