@@ -1702,12 +1702,25 @@ __global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg
         else
             fresh += s.len;
         const uint32_t P = next_pow2(s.len);
-        for (uint32_t e = lane; e < P; e += 32) {
-            Key k = key_max();
-            uint32_t id = IDX_MAX;
-            if (e < s.len) load_elem(a, s, e, k, id);
-            sk[pad(e)] = from_key(k);
-            sx[pad(e)] = id;
+        {
+            // All loads first (P <= 8 * 32), then the shared-memory stores.
+            Key kk[8];
+            uint32_t ii[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const uint32_t e = lane + c * 32;
+                kk[c] = key_max();
+                ii[c] = IDX_MAX;
+                if (e < s.len) load_elem(a, s, e, kk[c], ii[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const uint32_t e = lane + c * 32;
+                if (e < P) {
+                    sk[pad(e)] = from_key(kk[c]);
+                    sx[pad(e)] = ii[c];
+                }
+            }
         }
         __syncwarp();
         const uint32_t f = warp_diff_bit(sk, s.len, lane);
@@ -1896,12 +1909,26 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
             fresh += s.len;
         const uint32_t nruns = (s.len + BLOCK_RUN - 1) / BLOCK_RUN;
         const uint32_t span = nruns * BLOCK_RUN;
-        for (uint32_t e = t; e < span; e += GT) {
-            Key k = key_max();
-            uint32_t id = IDX_MAX;
-            if (e < s.len) load_elem(a, s, e, k, id);
-            sk[pad(e)] = from_key(k);
-            sx[pad(e)] = id;
+        {
+            // All of a thread's loads first (span <= SMALL_ITEMS * GT), so
+            // that they are in flight together, then the shared-memory stores.
+            Key kk[SMALL_ITEMS];
+            uint32_t ii[SMALL_ITEMS];
+#pragma unroll
+            for (int c = 0; c < SMALL_ITEMS; ++c) {
+                const uint32_t e = t + c * GT;
+                kk[c] = key_max();
+                ii[c] = IDX_MAX;
+                if (e < s.len) load_elem(a, s, e, kk[c], ii[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < SMALL_ITEMS; ++c) {
+                const uint32_t e = t + c * GT;
+                if (e < span) {
+                    sk[pad(e)] = from_key(kk[c]);
+                    sx[pad(e)] = ii[c];
+                }
+            }
         }
         if (t == 0) ok_flag[gi] = 1;
         group_sync<GT>(gi);
