@@ -233,6 +233,23 @@ def sort_algorithmic_bytes(live8, n, w):
 
 
 # ---- our arm ---------------------------------------------------------------------
+def max_over_ranks(dist, x, device):
+    """The largest of every rank's x (every rank calls this with its own);
+    x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, steps, world, seconds):
+    """Whole-job throughput of replicas: every rank processed units_per_rank
+    per step, and the job took the slowest rank's time."""
+    return units_per_rank * steps * world / seconds
+
+
 def run_ours(args, rank, world, local_rank, dist):
     import torch
     torch.cuda.set_device(local_rank)
@@ -285,10 +302,7 @@ def run_ours(args, rank, world, local_rank, dist):
     sorter.set_profiling(False)
     st = sorter.stats()
 
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, ms, f"cuda:{local_rank}")
 
     # ---- end to end through the host-buffer entry point (pinned buffers) ------
     e2e = None
@@ -308,11 +322,8 @@ def run_ours(args, rank, world, local_rank, dist):
         for _ in range(args.steps):
             sorter.sort_host(na, no, perm=pp, lcp=pl)
         e2e_s = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": n * args.steps * world / e2e_s, "unit": UNIT,
+        e2e_s = max_over_ranks(dist, e2e_s, f"cuda:{local_rank}")
+        e2e = {"value": job_rate(n, args.steps, world, e2e_s), "unit": UNIT,
                "h2d_bytes_per_step": int(ab + n * w), "d2h_bytes_per_step": int(n * 8),
                "ms_per_step": 1000 * e2e_s / args.steps,
                "api": "ssort_sort_host (pinned host buffers)"}
@@ -365,7 +376,7 @@ def run_ours(args, rank, world, local_rank, dist):
 
     lens_mean = ss.text_bytes / n - 1
     out = {
-        "metric": METRIC, "value": n * args.steps * world / (ms / 1e3), "unit": UNIT,
+        "metric": METRIC, "value": job_rate(n, args.steps, world, ms / 1e3), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8",
