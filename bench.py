@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
                     choices=sorted(pyssort.WORKLOADS) + ["batch_c4", "serve_c5"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run ssort_autotune on the input before timing (reported in `tuning`)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--target-bucket", type=int, default=0,
                     help="override the partition's wanted strings per range bucket")
@@ -270,6 +272,8 @@ def run_ours(args, rank, world, local_rank, dist):
     def step():
         sorter.sort_device(d_arena, ab, d_offs, w, n, d_perm, d_lcp, stream=stream.cuda_stream)
 
+    tuning = sorter.autotune(d_arena, ab, d_offs, w, n) if args.autotune else None
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -387,7 +391,7 @@ def run_ours(args, rank, world, local_rank, dist):
                    "l2": f"inputs larger than L2 (arena {ab / 1e9:.2f} GB)"},
         "key_gbs": round(ss.text_bytes * args.steps * world / (ms / 1e3) / 1e9, 2),
         "roofline": roofline, "sort_roofline": sort_roof, "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": int(launches), "clocks": clocks.summary(),
+        "gpu_launches": int(launches), "clocks": clocks.summary(), "tuning": tuning,
         "stats": {k: v for k, v in st.as_dict().items()}, "kernels": per_kernel,
     }
     return out

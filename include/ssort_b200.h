@@ -219,7 +219,38 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
  * the library; these override them for every later sort on the context). */
 #define SSORT_PARAM_TARGET_BUCKET 1 /* wanted strings per range bucket of a sample
                                        partition, 32..2048 (default 512) */
+#define SSORT_PARAM_WARP8_CAP 2     /* largest segment sorted by one warp, 64..256
+                                       (default 256); larger ones go to the CTA sort */
+#define SSORT_PARAM_OVERLAP 3       /* 1 (default): in round 0 the on-chip sorts run
+                                       on a side stream beside the partition; 0: one stream */
+#define SSORT_PARAM_FUSED_GATHER 4  /* 1 (default): from round 1 on, the first partition
+                                       level gathers the keys it counts; 0: separate gather */
 int ssort_set_param(ssort_ctx *ctx, int param, int64_t value);
+
+/*
+ * Autotuning (no counterpart in the reference).  Times sorts of the given
+ * device input under candidate parameter values, one parameter at a time:
+ * target bucket {256, 512, 1024}, one-warp cutoff {64, 128, 256}, fused
+ * gather {1, 0}, overlap {1, 0}; each candidate is sorted twice and kept when
+ * its faster run beats the current best by at least 1 %.  The winners are
+ * set on the context and recorded for the input's size class (floor(log2 n))
+ * and entropy class (Shannon entropy of the first 8 key bytes of a 4096-string
+ * sample: < 2, < 4, >= 4 bits per byte); later sorts on this context whose
+ * input falls in a recorded class use that class's values (when a size class
+ * has values for more than one entropy class, one sample pass finds the
+ * class).  Results are identical under every parameter value.
+ */
+typedef struct {
+    uint32_t size_class;    /* floor(log2 n) */
+    uint32_t entropy_class; /* 0, 1, 2 (see above) */
+    double entropy_bits;    /* bits per byte of the sample */
+    int64_t target_bucket, warp8_cap, overlap, fused_gather; /* chosen values */
+    double default_ms;      /* device time of one sort with the values before tuning */
+    double tuned_ms;        /* with the chosen values */
+    uint32_t trials;        /* sorts timed */
+} ssort_tuning;
+int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                   const void *d_offs, int off_width, uint64_t n, ssort_tuning *out);
 
 /* Kernel-level timing: when enabled, each kernel launch of a sort is bracketed
  * by CUDA events and its time is accumulated per kernel name. */

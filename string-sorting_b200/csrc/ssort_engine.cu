@@ -6,6 +6,7 @@
 #include "ssort_host.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -39,6 +40,29 @@ int ssort_ctx::reserve(uint32_t n) {
     if (!h_ctr) {
         SS_CUDA(cudaHostAlloc((void **)&h_ctr, sizeof(Counters), cudaHostAllocDefault));
     }
+    return SSORT_OK;
+}
+
+// Shannon entropy (bits per byte) of the first 8 key bytes of up to 4096
+// strings spread over the input.
+int ssort_ctx::sample_entropy(const uint8_t *arena_p, uint64_t arena_bytes, const void *offs_p,
+                              int off_width, uint32_t n, double &bits) {
+    SS_TRY(ensure(hist_buf, 256 * 4));
+    if (!h_hist) SS_CUDA(cudaHostAlloc((void **)&h_hist, 256 * 4, cudaHostAllocDefault));
+    const uint32_t samples = std::min<uint32_t>(n, 4096);
+    LAUNCH(this, "byte_hist",
+           launch_byte_hist(arena_p, arena_bytes, offs_p, off_width, n, samples,
+                            (uint32_t *)hist_buf.p, st));
+    SS_CUDA(cudaMemcpyAsync(h_hist, hist_buf.p, 256 * 4, cudaMemcpyDeviceToHost, st));
+    SS_CUDA(cudaStreamSynchronize(st));
+    double total = 0, h = 0;
+    for (int b = 0; b < 256; ++b) total += h_hist[b];
+    for (int b = 0; b < 256; ++b)
+        if (h_hist[b]) {
+            const double p = h_hist[b] / total;
+            h -= p * std::log2(p);
+        }
+    bits = h;
     return SSORT_OK;
 }
 
@@ -103,7 +127,7 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
     // inside the first count and keeps one stream (the random gather is
     // latency-bound and measured slower when it shares its SMs).
     fresh_round = round_mode >= 0 ? round_mode == 0 : round_no == 0;
-    overlap_round = side && hp && !prof && fresh_round;
+    overlap_round = side && hp && !prof && overlap && fresh_round;
     if (!overlap_round) return round_body(a, cur, n_cur, nxt, n_next, round_no);
     // Fork the round onto the high-priority stream and join it back.
     cudaStream_t user = st;
@@ -124,8 +148,8 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
     SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
     LAUNCH(this, "classify",
-           launch_classify(cur, n_cur, ws.W1, ws.W8, SmallLists{{ws.S, ws.S2, ws.S3}}, ws.L,
-                           dc, st));
+           launch_classify(cur, n_cur, a.warp8_cap, ws.W1, ws.W8,
+                           SmallLists{{ws.S, ws.S2, ws.S3}}, ws.L, dc, st));
     SS_TRY(sync_counters());
     if (round_no < SSORT_MAX_ROUNDS) stats.live[round_no] = h_ctr->live_next;
     // The on-chip sorts of the segments known after each host read of the
@@ -139,7 +163,7 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     // the identity, so a separate gather streams the arena in order; later
     // rounds read it at random, and the count kernel of the first partition
     // level gathers the keys itself so that those reads overlap its work.
-    const bool fused_gather = !fresh_round;
+    const bool fused_gather = !fresh_round && this->fused_gather;
     if (n_large && !fused_gather) {
         LAUNCH(this, "seg_tiles",
                launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));
@@ -238,6 +262,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.lcp = d_lcp ? d_lcp : ws.lcp;
     a.bkt = ws.bkt;
     a.target_bucket = target_bucket;
+    a.warp8_cap = warp8_cap;
 
     Seg *cur = ws.R, *nxt = ws.N;
     Counters *dc = ws.ctr;
@@ -278,9 +303,41 @@ int validate_common(ssort_ctx *ctx, int off_width, uint64_t n) {
     return SSORT_OK;
 }
 
+uint32_t size_class(uint64_t n) { return n ? 63u - (uint32_t)__builtin_clzll(n) : 0u; }
+uint32_t entropy_class(double bits) { return bits < 2.0 ? 0u : (bits < 4.0 ? 1u : 2u); }
+
+// Applies autotuned values recorded for this input's size and entropy class.
+int apply_tuning(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                 const void *d_offs, int off_width, uint64_t n) {
+    if (ctx->tuned.empty() || ctx->tuning || n < 2) return SSORT_OK;
+    const uint32_t sc = size_class(n);
+    uint32_t classes = 0, only = 0;
+    for (uint32_t e = 0; e < 3; ++e)
+        if (ctx->tuned.count(sc * 4 + e)) {
+            ++classes;
+            only = e;
+        }
+    if (!classes) return SSORT_OK;
+    // One recorded entropy class for this size: use it without sampling.
+    uint32_t ec = only;
+    if (classes > 1) {
+        double bits = 0;
+        SS_TRY(ctx->sample_entropy(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, bits));
+        ec = entropy_class(bits);
+    }
+    auto it = ctx->tuned.find(sc * 4 + ec);
+    if (it == ctx->tuned.end()) return SSORT_OK;
+    ctx->target_bucket = it->second.target_bucket;
+    ctx->warp8_cap = it->second.warp8_cap;
+    ctx->overlap = it->second.overlap;
+    ctx->fused_gather = it->second.fused_gather;
+    return SSORT_OK;
+}
+
 int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                      const void *d_offs, int off_width, uint64_t n, uint32_t *d_perm,
                      uint32_t *d_lcp, const uint32_t *d_inst = nullptr, uint32_t ninst = 0) {
+    SS_TRY(apply_tuning(ctx, d_arena, arena_bytes, d_offs, off_width, n));
     ctx->stats = ssort_stats{};
     ctx->stats.n = n;
     SS_CUDA(cudaEventRecord(ctx->ev_start, ctx->st));
@@ -395,6 +452,8 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
         for (HBuf *b : {&ctx->h_offs, &ctx->h_arena, &ctx->h_perm})
             if (b->p) cudaFreeHost(b->p);
         if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
+        if (ctx->h_hist) cudaFreeHost(ctx->h_hist);
+        if (ctx->hist_buf.p) cudaFree(ctx->hist_buf.p);
         for (auto e : ctx->ev_pool) cudaEventDestroy(e);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
@@ -620,6 +679,19 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
             if (value < 32 || value > SMALL_CAP) return fail(SSORT_EINVAL, "target_bucket out of range");
             ctx->target_bucket = (uint32_t)value;
             return SSORT_OK;
+        case SSORT_PARAM_WARP8_CAP:
+            if (value < 64 || value > WARP8_CAP)
+                return fail(SSORT_EINVAL, "warp8_cap out of range (64..256)");
+            ctx->warp8_cap = (uint32_t)value;
+            return SSORT_OK;
+        case SSORT_PARAM_OVERLAP:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "overlap must be 0 or 1");
+            ctx->overlap = value != 0;
+            return SSORT_OK;
+        case SSORT_PARAM_FUSED_GATHER:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "fused_gather must be 0 or 1");
+            ctx->fused_gather = value != 0;
+            return SSORT_OK;
         default:
             return fail(SSORT_EINVAL, "unknown parameter");
     }
@@ -802,6 +874,98 @@ int ssort_sort_host_chunked(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena
     if (rc != SSORT_OK) return rc;
     return ssort_merge_runs(arena, arena_bytes, offs, off_width, n, run_start.data(),
                             (uint32_t)runs, perm, lcp, perm, lcp);
+}
+
+int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
+                   const void *d_offs, int off_width, uint64_t n, ssort_tuning *out) {
+    SS_TRY(validate_common(ctx, off_width, n));
+    if (!out) return fail(SSORT_EINVAL, "null output pointer");
+    if (n < 2) return fail(SSORT_EINVAL, "autotuning needs at least 2 strings");
+    if (!d_arena || !d_offs) return fail(SSORT_EINVAL, "null device buffer");
+    if (((uintptr_t)d_arena & 15) != 0)
+        return fail(SSORT_EINVAL, "arena must be 16-byte aligned");
+    *out = ssort_tuning{};
+    return with_device(ctx, [&]() -> int {
+        ctx->st = ctx->own_stream;
+        ctx->tuning = true;
+        const bool was_prof = ctx->prof;
+        ctx->prof = false;
+        auto restore = [&]() {
+            ctx->tuning = false;
+            ctx->prof = was_prof;
+        };
+        int rc = [&]() -> int {
+            SS_TRY(ctx->ensure(ctx->perm, n * 8));
+            uint32_t *d_perm = (uint32_t *)ctx->perm.p, *d_lcp = d_perm + n;
+            double bits = 0;
+            SS_TRY(ctx->sample_entropy(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n,
+                                       bits));
+            uint32_t trials = 0;
+            // Device time of the faster of two sorts under the current values.
+            auto time_it = [&](double &ms) -> int {
+                ms = 1e30;
+                for (int r = 0; r < 2; ++r) {
+                    SS_TRY(sort_device_impl(ctx, d_arena, arena_bytes, d_offs, off_width, n,
+                                            d_perm, d_lcp));
+                    ms = std::min(ms, ctx->stats.device_ms);
+                    ++trials;
+                }
+                return SSORT_OK;
+            };
+            SS_TRY(sort_device_impl(ctx, d_arena, arena_bytes, d_offs, off_width, n, d_perm,
+                                    d_lcp));  // allocations and first-launch costs
+            double best = 0;
+            SS_TRY(time_it(best));
+            const double base = best;
+            struct Knob {
+                int param;
+                std::vector<int64_t> values;
+            };
+            const Knob knobs[] = {{SSORT_PARAM_TARGET_BUCKET, {256, 512, 1024}},
+                                  {SSORT_PARAM_WARP8_CAP, {64, 128, 256}},
+                                  {SSORT_PARAM_FUSED_GATHER, {1, 0}},
+                                  {SSORT_PARAM_OVERLAP, {1, 0}}};
+            auto get = [&](int p) -> int64_t {
+                switch (p) {
+                    case SSORT_PARAM_TARGET_BUCKET: return ctx->target_bucket;
+                    case SSORT_PARAM_WARP8_CAP: return ctx->warp8_cap;
+                    case SSORT_PARAM_FUSED_GATHER: return ctx->fused_gather ? 1 : 0;
+                    default: return ctx->overlap ? 1 : 0;
+                }
+            };
+            for (const Knob &k : knobs) {
+                const int64_t start = get(k.param);  // already timed
+                int64_t keep = start;
+                for (int64_t v : k.values) {
+                    if (v == start) continue;
+                    SS_TRY(ssort_set_param(ctx, k.param, v));
+                    double ms = 0;
+                    SS_TRY(time_it(ms));
+                    if (ms < best * 0.99) {
+                        best = ms;
+                        keep = v;
+                    }
+                }
+                SS_TRY(ssort_set_param(ctx, k.param, keep));
+            }
+            const uint32_t sc = size_class(n), ec = entropy_class(bits);
+            ctx->tuned[sc * 4 + ec] = ssort_ctx::Tuned{ctx->target_bucket, ctx->warp8_cap,
+                                                       ctx->overlap, ctx->fused_gather};
+            out->size_class = sc;
+            out->entropy_class = ec;
+            out->entropy_bits = bits;
+            out->target_bucket = ctx->target_bucket;
+            out->warp8_cap = ctx->warp8_cap;
+            out->overlap = ctx->overlap ? 1 : 0;
+            out->fused_gather = ctx->fused_gather ? 1 : 0;
+            out->default_ms = base;
+            out->tuned_ms = best;
+            out->trials = trials;
+            return SSORT_OK;
+        }();
+        restore();
+        return rc;
+    });
 }
 
 int ssort_pinned_alloc(size_t bytes, void **out) {

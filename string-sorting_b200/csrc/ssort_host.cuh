@@ -71,7 +71,23 @@ struct ssort_ctx {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 
     bool prof = false;
-    uint32_t target_bucket = ssort::TARGET_BUCKET;  // tuning: wanted strings per range bucket
+    // tuning parameters (ssort_set_param, ssort_autotune)
+    uint32_t target_bucket = ssort::TARGET_BUCKET;  // wanted strings per range bucket
+    uint32_t warp8_cap = ssort::WARP8_CAP;          // largest one-warp segment
+    bool overlap = true;       // round-0 on-chip sorts on the side stream
+    bool fused_gather = true;  // rounds >= 1 gather inside the first count
+    // Autotuned values per (size class * 4 + entropy class), applied to later
+    // sorts of the same classes; not while the tuner itself runs.
+    struct Tuned {
+        uint32_t target_bucket, warp8_cap;
+        bool overlap, fused_gather;
+    };
+    std::map<uint32_t, Tuned> tuned;
+    bool tuning = false;
+    ssort::DBuf hist_buf;
+    uint32_t *h_hist = nullptr;
+    int sample_entropy(const uint8_t *arena, uint64_t arena_bytes, const void *offs,
+                       int off_width, uint32_t n, double &bits);
     struct Rec {
         const char *name;
         cudaEvent_t a, b;

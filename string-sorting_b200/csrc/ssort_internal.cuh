@@ -102,6 +102,7 @@ struct SortArgs {
     uint32_t *lcp;
     uint32_t *bkt;  // per position during a partition level: bucket << 12 | offset
     uint32_t target_bucket;  // wanted strings per range bucket of a partition
+    uint32_t warp8_cap;      // largest segment for the one-warp sort (64..WARP8_CAP)
 };
 
 // ---- device workspace ---------------------------------------------------------
@@ -138,7 +139,8 @@ constexpr WsLayout ws_layout(uint64_t n) {
     o.N = take(half * sizeof(Seg));
     o.W1 = take(half * sizeof(Seg));
     o.W8 = take((n / (WARP1_CAP + 1) + 2) * sizeof(Seg));
-    o.S = take((n / (WARP8_CAP + 1) + 2) * sizeof(Seg));
+    // class 0 starts above the one-warp cutoff, which may be lowered to 64
+    o.S = take((n / 65 + 2) * sizeof(Seg));
     o.S2 = take((n / (BLOCK_CAP1 + 1) + 2) * sizeof(Seg));
     o.S3 = take((n / (BLOCK_CAP2 + 1) + 2) * sizeof(Seg));
     // equality work items: buckets of >= 2 strings, one item per EQ_TILE
@@ -209,8 +211,11 @@ inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
 
 // ---- launchers (ssort_kernels.cu) ----------------------------------------
 void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st);
-void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, SmallLists S, Seg *L,
-                     Counters *c, cudaStream_t st);
+// 256-bin histogram of the first 8 key bytes of `samples` strings (tuning).
+void launch_byte_hist(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
+                      uint32_t n, uint32_t samples, uint32_t *hist, cudaStream_t st);
+void launch_classify(const Seg *R, uint32_t nR, uint32_t warp8_cap, Seg *W1, Seg *W8,
+                     SmallLists S, Seg *L, Counters *c, cudaStream_t st);
 // Batches: one round-0 segment per instance; instance-local result indices.
 void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
                        Counters *c, cudaStream_t st);

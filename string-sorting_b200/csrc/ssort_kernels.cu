@@ -546,13 +546,13 @@ __device__ __forceinline__ void append_small(const SmallLists &S, Counters *c, b
     if (c2) S.s[2][slot] = o;
 }
 
-__global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, Seg *W1, Seg *W8, SmallLists S,
-                           Seg *L, Counters *c) {
+__global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, uint32_t warp8_cap, Seg *W1,
+                           Seg *W8, SmallLists S, Seg *L, Counters *c) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool v = i < nR;
     const Seg s = v ? R[i] : Seg{0, 0, 0, 0};
     const bool w1 = v && s.len <= (uint32_t)WARP1_CAP;
-    const bool w8 = v && !w1 && s.len <= (uint32_t)WARP8_CAP;
+    const bool w8 = v && !w1 && s.len <= warp8_cap;
     const bool sm = v && !w1 && !w8 && s.len <= (uint32_t)SMALL_CAP;
     const bool lg = v && !w1 && !w8 && !sm;
     uint32_t slot = warp_append(&c->n_w1, w1);
@@ -783,6 +783,25 @@ __global__ void k_sorted_offs(const uint32_t *__restrict__ perm, const void *off
         out[k] = off_width == 8 ? static_cast<const uint64_t *>(offs)[i]
                                 : static_cast<const uint32_t *>(offs)[i];
     }
+}
+
+// ---- tuning: byte histogram of a sample of keys -----------------------------
+// hist[b] += occurrences of byte value b among the first 8 key bytes of
+// `samples` strings spread evenly over the n input strings (one CTA).
+__global__ void k_byte_hist(const uint8_t *__restrict__ arena, uint64_t arena_bytes,
+                            const void *offs, int off_width, uint32_t n, uint32_t samples,
+                            uint32_t *hist) {
+    __shared__ uint32_t h[256];
+    for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < samples; i += blockDim.x) {
+        const uint32_t id = (uint32_t)((uint64_t)i * n / samples);
+        const Key k = load_key(arena, arena_bytes, string_offset(offs, off_width, id));
+#pragma unroll
+        for (int b = 0; b < 8; ++b) atomicAdd(&h[(k.hi >> (56 - 8 * b)) & 0xFF], 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = h[b];
 }
 
 // ---- single-CTA exclusive scans of short per-segment arrays -----------------
@@ -1492,7 +1511,7 @@ __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__
         const Seg o{p, len, s.depth, flags};
         const bool rng = multi && !(b & 1);
         const bool w1 = rng && len <= (uint32_t)WARP1_CAP;
-        const bool w8 = rng && !w1 && len <= (uint32_t)WARP8_CAP;
+        const bool w8 = rng && !w1 && len <= a.warp8_cap;
         const bool sm = rng && !w1 && !w8 && len <= (uint32_t)SMALL_CAP;
         const bool lg = rng && !w1 && !w8 && !sm;
         slot = warp_append(&c->n_w1, w1);
@@ -2041,10 +2060,10 @@ void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st) {
     k_iota<<<g ? g : 1, 256, 0, st>>>(idx, n);
 }
 
-void launch_classify(const Seg *R, uint32_t nR, Seg *W1, Seg *W8, SmallLists S, Seg *L,
-                     Counters *c, cudaStream_t st) {
+void launch_classify(const Seg *R, uint32_t nR, uint32_t warp8_cap, Seg *W1, Seg *W8,
+                     SmallLists S, Seg *L, Counters *c, cudaStream_t st) {
     if (!nR) return;
-    k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, W1, W8, S, L, c);
+    k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, warp8_cap, W1, W8, S, L, c);
 }
 
 void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
@@ -2105,6 +2124,11 @@ void launch_sorted_offs(const uint32_t *perm, const void *offs, int off_width, u
                         uint64_t *out, cudaStream_t st) {
     const uint64_t g = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
     k_sorted_offs<<<(unsigned)(g ? g : 1), 256, 0, st>>>(perm, offs, off_width, n, out);
+}
+
+void launch_byte_hist(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
+                      uint32_t n, uint32_t samples, uint32_t *hist, cudaStream_t st) {
+    k_byte_hist<<<1, 256, 0, st>>>(arena, arena_bytes, offs, off_width, n, samples, hist);
 }
 
 void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,

@@ -160,6 +160,7 @@ struct ssort_server {
         a.lcp = ctx->ws.lcp;
         a.bkt = ctx->ws.bkt;
         a.target_bucket = ctx->target_bucket;
+        a.warp8_cap = ctx->warp8_cap;
         return a;
     }
 

@@ -26,13 +26,16 @@ EXPORTS = (
     "ssort_server_create", "ssort_server_destroy", "ssort_server_submit", "ssort_server_step",
     "ssort_server_poll", "ssort_server_drain", "ssort_server_get_info",
     "ssort_text_offsets_device", "ssort_sort_text_host", "ssort_pinned_alloc",
-    "ssort_pinned_free", "ssort_merge_runs", "ssort_sort_host_chunked",
+    "ssort_pinned_free", "ssort_merge_runs", "ssort_sort_host_chunked", "ssort_autotune",
 )
 # text input modes (sortstring's default line mode, --raw, --suffix-sorting)
 TEXT_LINES, TEXT_RAW, TEXT_SUFFIXES = 0, 1, 2
 # request states reported by ssort_server_poll
 REQ_QUEUED, REQ_LOADING, REQ_ACTIVE, REQ_DRAINING, REQ_DONE = range(5)
 SSORT_PARAM_TARGET_BUCKET = 1
+SSORT_PARAM_WARP8_CAP = 2
+SSORT_PARAM_OVERLAP = 3
+SSORT_PARAM_FUSED_GATHER = 4
 
 
 class SsortError(RuntimeError):
@@ -91,6 +94,24 @@ class ServerInfo(ctypes.Structure):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("size_class", ctypes.c_uint32),
+        ("entropy_class", ctypes.c_uint32),
+        ("entropy_bits", ctypes.c_double),
+        ("target_bucket", ctypes.c_int64),
+        ("warp8_cap", ctypes.c_int64),
+        ("overlap", ctypes.c_int64),
+        ("fused_gather", ctypes.c_int64),
+        ("default_ms", ctypes.c_double),
+        ("tuned_ms", ctypes.c_double),
+        ("trials", ctypes.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib = None
 _wlib = None
 
@@ -141,6 +162,7 @@ def lib():
         L.ssort_merge_runs.argtypes = [vp, u64, vp, i32, u64, vp, ctypes.c_uint32, vp, vp, vp,
                                        vp]
         L.ssort_sort_host_chunked.argtypes = [vp, vp, u64, vp, i32, u64, u64, vp, vp]
+        L.ssort_autotune.argtypes = [vp, vp, u64, vp, i32, u64, ctypes.POINTER(Tuning)]
         L.ssort_pinned_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
         L.ssort_pinned_free.argtypes = [vp]
         L.ssort_pinned_free.restype = None
@@ -301,6 +323,16 @@ class Sorter:
 
     def set_param(self, param, value):
         _check(lib().ssort_set_param(self._ctx, int(param), int(value)))
+
+    def autotune(self, d_arena, arena_bytes, d_offs, off_width, n):
+        """Tune the context's parameters on a device-resident input
+        (ssort_autotune); returns the chosen values and timings."""
+        def p(x):
+            return x if isinstance(x, int) or x is None else x.data_ptr()
+        t = Tuning()
+        _check(lib().ssort_autotune(self._ctx, p(d_arena), int(arena_bytes), p(d_offs),
+                                    int(off_width), int(n), ctypes.byref(t)))
+        return t.as_dict()
 
     def set_profiling(self, on):
         _check(lib().ssort_set_profiling(self._ctx, 1 if on else 0))

@@ -1,0 +1,79 @@
+"""Tuning parameters and the autotuner: every parameter value gives the same
+perm and LCP (checked against the default and the oracle), out-of-range
+values are rejected, and ssort_autotune picks values from its candidate sets,
+records them, and later sorts of the same class stay bit-exact."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import cases
+import pyoracle
+import pyssort
+
+pytestmark = pytest.mark.gpu
+
+SETTINGS = [
+    (pyssort.SSORT_PARAM_WARP8_CAP, 64),
+    (pyssort.SSORT_PARAM_WARP8_CAP, 128),
+    (pyssort.SSORT_PARAM_OVERLAP, 0),
+    (pyssort.SSORT_PARAM_FUSED_GATHER, 0),
+    (pyssort.SSORT_PARAM_TARGET_BUCKET, 128),
+    (pyssort.SSORT_PARAM_TARGET_BUCKET, 1024),
+]
+
+
+@pytest.mark.parametrize("param,value", SETTINGS)
+def test_parameter_values_keep_results(golden, param, value):
+    with pyssort.Sorter(0) as s:
+        s.set_param(param, value)
+        for name in ("desc_numbers_200000", "long_prefix_10000", "high_bytes_5000",
+                     "ut_runs30_8001", "one_letter_20000"):
+            arena, offs = cases.arena_of(cases.CASES[name]())
+            p, l = s.sort_host(arena, offs)
+            assert hashlib.sha256(np.ascontiguousarray(p, "<u4").tobytes()).hexdigest() == \
+                golden[name]["perm_sha256"], name
+            assert hashlib.sha256(np.ascontiguousarray(l, "<u4").tobytes()).hexdigest() == \
+                golden[name]["lcp_sha256"], name
+        ss = pyssort.gen_urls(300_000, seed=61)
+        p, l = s.sort_host(ss.arena, ss.offs)
+        rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+        assert np.array_equal(p, rp) and np.array_equal(l, rl)
+
+
+def test_out_of_range_parameters_are_rejected():
+    with pyssort.Sorter(0) as s:
+        for param, value in [(pyssort.SSORT_PARAM_WARP8_CAP, 32),
+                             (pyssort.SSORT_PARAM_WARP8_CAP, 512),
+                             (pyssort.SSORT_PARAM_OVERLAP, 2),
+                             (pyssort.SSORT_PARAM_FUSED_GATHER, -1),
+                             (pyssort.SSORT_PARAM_TARGET_BUCKET, 4096),
+                             (99, 1)]:
+            with pytest.raises(pyssort.SsortError) as e:
+                s.set_param(param, value)
+            assert e.value.status == -1
+
+
+def test_autotune_then_sort_stays_exact():
+    torch = pytest.importorskip("torch")
+    ss = pyssort.gen_urls(1_000_000, seed=62)
+    d_arena = torch.from_numpy(ss.arena).cuda()
+    d_offs = torch.from_numpy(ss.offs.view(np.int64)).cuda()
+    with pyssort.Sorter(0) as s:
+        t = s.autotune(d_arena, ss.arena.nbytes, d_offs, 8, ss.n)
+        assert t["size_class"] == 19  # floor(log2(1e6))
+        assert t["entropy_class"] in (0, 1, 2)
+        assert 0 < t["entropy_bits"] <= 8
+        assert t["target_bucket"] in (256, 512, 1024)
+        assert t["warp8_cap"] in (64, 128, 256)
+        assert t["overlap"] in (0, 1) and t["fused_gather"] in (0, 1)
+        assert t["tuned_ms"] <= t["default_ms"]
+        assert t["trials"] == 2 + 2 * (2 + 2 + 1 + 1)  # base, then every other candidate
+        # a later sort of the same class uses the recorded values
+        d_perm = torch.empty(ss.n, dtype=torch.int32, device="cuda")
+        d_lcp = torch.empty(ss.n, dtype=torch.int32, device="cuda")
+        s.sort_device(d_arena, ss.arena.nbytes, d_offs, 8, ss.n, d_perm, d_lcp)
+        torch.cuda.synchronize()
+        rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+        assert np.array_equal(d_perm.cpu().numpy().view(np.uint32), rp)
+        assert np.array_equal(d_lcp.cpu().numpy().view(np.uint32), rl)
