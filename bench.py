@@ -66,13 +66,13 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--target-bucket", type=int, default=0,
                     help="override the partition's wanted strings per range bucket")
-    ap.add_argument("--serve-requests", type=int, default=1000,
+    ap.add_argument("--serve-requests", type=int, default=2000,
                     help="requests per arrival rate of the serve_c5 sweep")
     ap.add_argument("--serve-rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--serve-pool", type=int, default=64,
                     help="distinct requests the serve_c5 stream draws from")
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
-    ap.add_argument("--serve-max-strings", type=int, default=1 << 26)
+    ap.add_argument("--serve-max-strings", type=int, default=1 << 27)
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the workload's string count (profiling runs only; "
                          "the reported workload is the full one at 1.0)")
