@@ -35,8 +35,9 @@ struct Seg {
 };
 
 // Segments of at most WARP1_CAP strings are sorted by one warp with one string
-// per lane, at most WARP8_CAP by one warp with 8 strings per lane, at most
-// SMALL_CAP by one CTA; larger ones are split by sample partitioning first.
+// per lane, at most WARP8_CAP (or the runtime cutoff below it) by one warp
+// with up to 8 strings per lane, at most SMALL_CAP by a thread group of a CTA;
+// larger ones are split by sample partitioning first.
 constexpr int WARP1_CAP = 32;
 constexpr int WARP8_CAP = 256;
 constexpr int SMALL_CAP = 2048;

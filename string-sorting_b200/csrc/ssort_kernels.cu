@@ -6,10 +6,11 @@
 // multi-byte form of the reference's get_char, src/util/get_char.h:42-89, built
 // with unsigned shifts; the reference's int-promoted 64-bit form sign-extends
 // bytes >= 0x80, :82, and is not reproduced).  Each segment is then sorted by
-// (key, index): segments of <= 32 strings by one warp in registers, <= 256 by
-// one warp with 8 strings per lane, <= SMALL_CAP by one CTA, larger ones are
-// first split by sample partitioning into range buckets and equality buckets
-// with a stable scatter.  Equal runs whose key holds no NUL (the reference's
+// (key, index): segments of <= 32 strings by one warp in registers (four
+// segments of <= 8 per warp), <= 256 by one warp with up to 8 strings per
+// lane, <= SMALL_CAP by a group of 64, 128 or 256 threads of a CTA (by size),
+// larger ones are first split by sample partitioning into range buckets and
+// equality buckets with a stable scatter.  Equal runs whose key holds no NUL (the reference's
 // is_end test, src/util/get_char.h:162-175, and its bucket-skip rule,
 // src/msd_ce.cpp:402) become the next round's segments at depth+16; every
 // other adjacent pair gets its LCP here.
