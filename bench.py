@@ -702,6 +702,48 @@ def time_cpu_sort(ss, m):
     return time.perf_counter() - t0, "port"
 
 
+def instance_sample(workload, budget):
+    """The first instances of the batched or served workload's list, up to
+    about `budget` strings (the reference arm's bounded sample)."""
+    if workload == "batch_c4":
+        params = pyssort.batch_instance_params(20000, 5, key_byte_limit=1.5e9)
+        seed = 4
+    else:
+        params = pyssort.batch_instance_params(64, 6, lo=1000, hi=5_000_000)
+        seed = 7
+    take, total = [], 0
+    for p in params:
+        if take and total + p[0] > budget:
+            break
+        take.append(p)
+        total += p[0]
+    return pyssort.gen_instances(take, seed=seed)
+
+
+def time_cpu_instances(ss):
+    """Seconds for sorting every instance of ss one after another with the
+    reference's msd_CE6 (or the oracle port).  Returns (seconds, kind)."""
+    L = _ref_lib()
+    total, kind = 0.0, "reference" if L is not None else "port"
+    P = None if L is not None else _port_lib()
+    for i in range(len(ss.inst_start) - 1):
+        lo, hi = int(ss.inst_start[i]), int(ss.inst_start[i + 1])
+        if hi - lo < 2:
+            continue
+        op = ss.offs.ctypes.data + 8 * lo
+        if L is not None:
+            t = L.ref_time_sort(b"msd_CE6", ss.arena.ctypes.data, op, hi - lo)
+            if t < 0:
+                raise RuntimeError("reference sort failed")
+            total += t
+        else:
+            perm = np.empty(hi - lo, dtype=np.uint32)
+            t0 = time.perf_counter()
+            P.oracle_sort_arena(ss.arena.ctypes.data, op, 8, hi - lo, perm.ctypes.data, None)
+            total += time.perf_counter() - t0
+    return total, kind
+
+
 def cpu_baseline(workload, ss, reps=3):
     m = min(ss.n, CPU_SAMPLE.get(workload, 2_000_000))
     ts = []
@@ -720,14 +762,24 @@ def cpu_baseline(workload, ss, reps=3):
 def run_reference(args, rank):
     if rank != 0:
         return None
-    ss = pyssort.WORKLOADS[args.workload](args.scale)
-    m = min(ss.n, CPU_SAMPLE.get(args.workload, 2_000_000))
+    if args.workload in ("batch_c4", "serve_c5"):
+        # independent instances, sorted one after another on one core
+        ss = instance_sample(args.workload, 2_000_000)
+        m = ss.n
+        sample = (f"the first {len(ss.inst_start) - 1} instances ({m:,} strings) of the "
+                  f"{args.workload} list per step, each sorted alone")
+        timer = lambda: time_cpu_instances(ss)  # noqa: E731
+    else:
+        ss = pyssort.WORKLOADS[args.workload](args.scale)
+        m = min(ss.n, CPU_SAMPLE.get(args.workload, 2_000_000))
+        sample = f"first {m:,} strings of {args.workload} per step"
+        timer = lambda: time_cpu_sort(ss, m)  # noqa: E731
     for _ in range(args.warmup):
-        time_cpu_sort(ss, m)
+        timer()
     total = 0.0
     kind = None
     for _ in range(args.steps):
-        t, kind = time_cpu_sort(ss, m)
+        t, kind = timer()
         total += t
     v = m * args.steps / total
     return {
@@ -740,7 +792,7 @@ def run_reference(args, rank):
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
                          "routine": "msd_CE6 (single-threaded by design: function-static "
                                     "bucket arrays, src/msd_ce.cpp:392)",
-                         "sample": f"first {m:,} strings of {args.workload} per step",
+                         "sample": sample,
                          "host": {"cpu": cpu_model(), "nproc": os.cpu_count()}},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

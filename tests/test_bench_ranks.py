@@ -45,3 +45,13 @@ def test_single_process_and_job_rate():
     assert bench.max_over_ranks(None, 1.5, "cpu") == 1.5
     # two replicas of 50M strings, 10 steps, slowest rank 2 s
     assert bench.job_rate(50_000_000, 10, 2, 2.0) == pytest.approx(5e8)
+
+
+@pytest.mark.parametrize("workload", ["batch_c4", "serve_c5"])
+def test_reference_arm_times_instances_alone(workload):
+    """The CPU reference arm of the batched and served workloads sorts a
+    bounded prefix of their instance list, instance by instance."""
+    ss = bench.instance_sample(workload, 20_000)
+    assert len(ss.inst_start) >= 2 and ss.n == int(ss.inst_start[-1])
+    t, kind = bench.time_cpu_instances(ss)
+    assert t > 0 and kind in ("reference", "port")
