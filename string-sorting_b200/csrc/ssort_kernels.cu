@@ -14,6 +14,8 @@
 // is_end test, src/util/get_char.h:162-175, and its bucket-skip rule,
 // src/msd_ce.cpp:402) become the next round's segments at depth+16; every
 // other adjacent pair gets its LCP here.
+#include <atomic>
+
 #include "ssort_internal.cuh"
 
 namespace ssort {
@@ -2056,6 +2058,35 @@ __global__ void k_boundary(SortArgs a, const uint2 *__restrict__ B, Counters *c)
 // ---- launchers --------------------------------------------------------------
 static inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
+// Opt-in to more than 48 KB of dynamic shared memory for the kernels that use
+// it.  The attribute belongs to the function in the current device's context,
+// so it is set once per device (bit d of the mask), for all kernels at once;
+// two threads that race here both set the same values, which is harmless.
+static constexpr int SAMPLE_SMEM =
+    SAMPLES_MAX * sizeof(ulonglong2) + (SAMPLES_MAX + SAMPLES_MAX / 8) * sizeof(uint64_t);
+static void set_smem_attrs() {
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return;  // the launch reports it
+    const uint64_t bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+    cudaFuncSetAttribute(k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, SAMPLE_SMEM);
+    cudaFuncSetAttribute(k_count<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PartSmem));
+    cudaFuncSetAttribute(k_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PartSmem));
+    cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(ScatterSmem));
+    cudaFuncSetAttribute(k_warp8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W8_SMEM);
+    cudaFuncSetAttribute(k_block<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    done.fetch_or(bit, std::memory_order_release);
+}
+
 void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st) {
     const uint32_t g = cdiv(n, 256) < 148 * 16 ? cdiv(n, 256) : 148 * 16;
     k_iota<<<g ? g : 1, 256, 0, st>>>(idx, n);
@@ -2161,28 +2192,16 @@ void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl
                    uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size, bool from_arena,
                    cudaStream_t st) {
     if (!nL) return;
-    static bool attr = false;
-    const int smem = SAMPLES_MAX * sizeof(ulonglong2) +
-                     (SAMPLES_MAX + SAMPLES_MAX / 8) * sizeof(uint64_t);
-    if (!attr) {
-        cudaFuncSetAttribute(k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
-    }
-    k_sample<<<nL, SAMPLE_THREADS, smem, st>>>(a, L, spl, nspl, tbl, ntiles, cm_size, from_arena);
+    set_smem_attrs();
+    k_sample<<<nL, SAMPLE_THREADS, SAMPLE_SMEM, st>>>(a, L, spl, nspl, tbl, ntiles, cm_size,
+                                                      from_arena);
 }
 
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                   const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
                   const uint32_t *cm_base, uint32_t *cm, bool gather, int grid, cudaStream_t st) {
     if (!nL) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_count<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(PartSmem));
-        cudaFuncSetAttribute(k_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(PartSmem));
-        attr = true;
-    }
+    set_smem_attrs();
     if (gather)
         k_count<true><<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl,
                                                                     tbl, cm_base, cm);
@@ -2195,12 +2214,7 @@ void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t
                     const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
                     const uint32_t *cm_base, const uint32_t *cm_scan, int grid, cudaStream_t st) {
     if (!nL) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(ScatterSmem));
-        attr = true;
-    }
+    set_smem_attrs();
     k_scatter<<<grid, SCATTER_THREADS, sizeof(ScatterSmem), st>>>(a, L, nL, tile_base, nspl,
                                                                   cm_base, cm_scan);
 }
@@ -2223,27 +2237,14 @@ void launch_warp1(const SortArgs &a, const Seg *W1, uint32_t n, Seg *N, Counters
 void launch_warp8(const SortArgs &a, const Seg *W8, uint32_t n, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
     if (!n) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_warp8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W8_SMEM);
-        attr = true;
-    }
+    set_smem_attrs();
     k_warp8<<<grid, WARP_THREADS, W8_SMEM, st>>>(a, W8, n, N, c);
 }
 
 void launch_block(const SortArgs &a, const Seg *S, uint32_t n, int cls, Seg *N, Counters *c,
                   int grid, cudaStream_t st) {
     if (!n) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_block<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)BLOCK_SMEM);
-        cudaFuncSetAttribute(k_block<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)BLOCK_SMEM);
-        cudaFuncSetAttribute(k_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)BLOCK_SMEM);
-        attr = true;
-    }
+    set_smem_attrs();
     if (cls == 0)
         k_block<64><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, n, N, c);
     else if (cls == 1)
