@@ -71,6 +71,25 @@ def test_device_api_with_torch_stream(sorter):
     assert np.array_equal(perm, ref_perm) and np.array_equal(lcp, ref_lcp)
 
 
+@pytest.mark.parametrize("name", ["ut_runs30_8001", "dup_heavy_100000", "long_prefix_10000",
+                                  "all_empty_100"])
+def test_permutation_without_lcp_output(name, golden, sorter):
+    """A NULL lcp pointer (host and device entry points) gives the same
+    permutation; the LCP is then kept in library scratch."""
+    torch = pytest.importorskip("torch")
+    arena, offs = cases.arena_of(cases.CASES[name]())
+    perm, none = sorter.sort_host(arena, offs, with_lcp=False)
+    assert none is None
+    assert digest(perm) == golden[name]["perm_sha256"]
+    n = len(offs)
+    d_arena = torch.from_numpy(arena).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    sorter.sort_device(d_arena, arena.nbytes, d_offs, 8, n, d_perm, None)
+    torch.cuda.synchronize()
+    assert digest(d_perm.cpu().numpy().view(np.uint32)) == golden[name]["perm_sha256"]
+
+
 def test_pointer_array_form(sorter):
     strings = cases.high_bytes(3000, 33) + cases.ut_bb_a_bbb(50)
     out, lcp = sorter.sort_strings(strings, with_lcp=True)
