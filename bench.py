@@ -2,7 +2,8 @@
 """Benchmark of the B200 MSD radix string sort (one JSON line on rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload urls_50m|zipf_words_100m|uniform_1m|batch_c4|serve_c5]
+                  [--workload urls_50m|zipf_words_100m|uniform_1m|batch_c4|serve_c5|
+                              text_urls_50m|suffixes_160m]
 
 A step is one complete sort of the workload (perm + LCP) from inputs resident
 in HBM.  `value` is strings/s over the whole job; `e2e` repeats the
@@ -35,7 +36,8 @@ import pyssort  # noqa: E402
 METRIC = "sort throughput (strings/s)"
 UNIT = "strings/s"
 DEFAULT_WORKLOAD = "urls_50m"
-CPU_SAMPLE = {"urls_50m": 4_000_000, "zipf_words_100m": 8_000_000, "uniform_1m": 1_000_000}
+CPU_SAMPLE = {"urls_50m": 4_000_000, "zipf_words_100m": 8_000_000, "uniform_1m": 1_000_000,
+              "text_urls_50m": 4_000_000, "suffixes_160m": 16_000_000}
 DESCRIPTIONS = {
     "urls_50m": "50,000,000 URLs: 'http://' + Zipf(1.1) host of 4,096 (8-24 [a-z]) + 1-6 "
                 "'/'-segments of 3-12 [a-z0-9]; seed 2; uint64 offsets",
@@ -45,6 +47,13 @@ DESCRIPTIONS = {
     "batch_c4": "independent instances, counts log-uniform in [100, 2,000,000], alphabet "
                 "{4 from 'A', 26 from 'a', 95 from ' '}, length U[1, L], L in {8, 32, 128}; "
                 "the instance list stops at 1.5e9 expected key bytes; seeds 5 (list), 4 (strings)",
+    "text_urls_50m": "the urls_50m strings as one text file: resident steps find the starts of "
+                     "the NUL-delimited (--raw) text on the GPU, then sort; e2e sorts the "
+                     "'\\n'-delimited file (default mode) from pinned host memory; uint32 offsets",
+    "suffixes_160m": "every suffix (--suffix-sorting) of a 160,000,000-byte text: Zipf(1.0) "
+                     "words (as zipf_words_100m, seed 8) separated by spaces, overwritten by "
+                     "2,000 copies of earlier passages of log-uniform length in [32, 4096] "
+                     "bytes; uint32 offsets",
     "serve_c5": "Poisson request stream swept over 1k-50k req/s; request string counts "
                 "log-uniform in [1,000, 5,000,000], strings as batch_c4; requests drawn from a "
                 "pool of distinct requests in pinned host memory; uint32 offsets; 120 GB arena "
@@ -59,11 +68,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
-                    choices=sorted(pyssort.WORKLOADS) + ["batch_c4", "serve_c5"])
+                    choices=sorted(pyssort.WORKLOADS) + ["batch_c4", "serve_c5",
+                                                         "text_urls_50m", "suffixes_160m"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--autotune", action="store_true",
                     help="run ssort_autotune on the input before timing (reported in `tuning`)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--warp1-deep", type=int, default=None,
+                    help="in-warp refinement steps of the one-per-lane sort (library default "
+                         "when absent)")
     ap.add_argument("--target-bucket", type=int, default=0,
                     help="override the partition's wanted strings per range bucket")
     ap.add_argument("--serve-requests", type=int, default=2000,
@@ -218,13 +231,11 @@ def intrinsic_live(lcp, n):
     import numpy as np
     l = np.asarray(lcp, dtype=np.int64)
     m = np.maximum(l, np.append(l[1:], 0))
-    top = int(m.max()) if n else 0
-    live = [n]
-    d = 8
-    while d <= top:
-        live.append(int(np.count_nonzero(m >= d)))
-        d += 8
-    return live
+    if not n:
+        return [0]
+    # m >= 8r exactly when m // 8 >= r: one histogram, then suffix sums
+    ge = np.cumsum(np.bincount(m // 8)[::-1])[::-1]
+    return [n] + [int(x) for x in ge[1:]]
 
 
 def sort_algorithmic_bytes(live8, n, w):
@@ -266,6 +277,8 @@ def run_ours(args, rank, world, local_rank, dist):
     sorter = pyssort.Sorter(local_rank)
     if args.target_bucket:
         sorter.set_param(pyssort.SSORT_PARAM_TARGET_BUCKET, args.target_bucket)
+    if args.warp1_deep is not None:
+        sorter.set_param(pyssort.SSORT_PARAM_WARP1_DEEP, args.warp1_deep)
     stream = torch.cuda.Stream(device=local_rank)
     ab = ss.arena.nbytes
 
@@ -404,6 +417,178 @@ def run_ours(args, rank, world, local_rank, dist):
         "stats": {k: v for k, v in st.as_dict().items()}, "kernels": per_kernel,
     }
     return out
+
+
+# ---- text inputs: string starts found on the GPU, then the sort --------------------
+TEXT_WORKLOADS = ("text_urls_50m", "suffixes_160m")
+
+
+def text_workload(name, scale):
+    """(text followed by 16 zero bytes, text length, mode of the device-resident
+    steps, mode of the host-buffer steps, a function giving the text with the
+    host mode's delimiters, number of strings, a function giving the uint64
+    starts of the first m strings) for a text workload."""
+    if name == "text_urls_50m":
+        ss = pyssort.gen_urls(int(50_000_000 * scale), 4096, 1.1, 2)
+        tlen = ss.text_bytes
+
+        def lines():
+            t = ss.arena[:tlen].copy()
+            t[t == 0] = ord("\n")
+            return t
+        return (ss.arena, tlen, pyssort.TEXT_RAW, pyssort.TEXT_LINES, lines, ss.n,
+                lambda m: ss.offs[:m])
+    tlen = int(160_000_000 * scale)
+    text = pyssort.gen_repeat_text(tlen, n_repeats=max(1, int(2000 * scale)), seed=8)
+    return (text, tlen, pyssort.TEXT_SUFFIXES, pyssort.TEXT_SUFFIXES, lambda: text[:tlen], tlen,
+            lambda m: np.arange(m, dtype=np.uint64))
+
+
+def run_text(args, rank, world, local_rank, dist):
+    """Whole-text sorts: a step finds the string starts of a resident text
+    (ssort_text_offsets_device) and sorts them (ssort_sort_device); e2e is
+    ssort_sort_text_host on the text in pinned host memory (copy in, find,
+    sort, sorted starts out)."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    text, tlen, mode, host_mode, host_text, n, starts_of = text_workload(args.workload, args.scale)
+    w = 4  # both texts are shorter than 2^32 bytes
+    d_text = torch.from_numpy(text).to(dev)
+    d_offs = torch.empty(n, dtype=torch.int32, device=dev)
+    d_perm = torch.empty(n, dtype=torch.int32, device=dev)
+    d_lcp = torch.empty(n, dtype=torch.int32, device=dev)
+    sorter = pyssort.Sorter(local_rank)
+    if args.warp1_deep is not None:
+        sorter.set_param(pyssort.SSORT_PARAM_WARP1_DEEP, args.warp1_deep)
+    stream = torch.cuda.Stream(device=local_rank)
+
+    def step():
+        m = sorter.text_offsets_device(d_text, tlen, mode, d_offs, w, n,
+                                       stream=stream.cuda_stream)
+        sorter.sort_device(d_text, tlen + 16, d_offs, w, m, d_perm, d_lcp,
+                           stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        dist.barrier()
+    sorter.set_profiling(True)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    ktimes = sorter.kernel_times()
+    sorter.set_profiling(False)
+    st = sorter.stats()
+    ms = max_over_ranks(dist, ms, dev)
+
+    e2e = None
+    if not args.no_e2e:
+        h_text = torch.empty(tlen, dtype=torch.uint8, pin_memory=True)
+        h_text.numpy()[:] = host_text()
+        h_out = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        ht, ho = h_text.numpy(), h_out.numpy().view(np.uint64)
+        sorter.sort_text(ht, host_mode, with_lcp=False, out=ho)  # warm the staging buffers
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sorter.sort_text(ht, host_mode, with_lcp=False, out=ho)
+        e2e_s = max_over_ranks(dist, time.perf_counter() - t0, dev)
+        e2e = {"value": job_rate(n, args.steps, world, e2e_s), "unit": UNIT,
+               "h2d_bytes_per_step": int(tlen), "d2h_bytes_per_step": int(n * 8),
+               "ms_per_step": 1000 * e2e_s / args.steps,
+               "api": "ssort_sort_text_host (pinned host text), sorted string starts read back"}
+    clocks.stop()
+    if rank != 0:
+        return None
+
+    peak, peak_kind = peaks()
+    kb = kernel_bytes(st, w)
+    # text scan: count reads the text; starts reads it again and writes the
+    # offsets; suffix mode writes the offsets only
+    kb.update({"text_count": tlen, "text_starts": tlen + n * w, "iota_offs": n * w})
+    per_kernel = {}
+    for name, (kms, launches) in ktimes.items():
+        entry = {"ms_total": round(kms, 4), "launches": int(launches),
+                 "ms_per_step": round(kms / args.steps, 4)}
+        if name in kb and kms > 0:
+            entry["algorithmic_bytes_per_step"] = int(kb[name])
+            entry["gbs"] = round(kb[name] * args.steps / (kms / 1e3) / 1e9, 1)
+        per_kernel[name] = entry
+    timed = {k: v for k, v in per_kernel.items() if "gbs" in v}
+    dom = max(timed, key=lambda k: timed[k]["ms_total"]) if timed else None
+    roofline = None
+    if dom:
+        d = per_kernel[dom]
+        per_launch_bytes = kb[dom] * args.steps / d["launches"]
+        per_launch_s = d["ms_total"] / 1e3 / d["launches"]
+        ach = per_launch_bytes / per_launch_s / 1e9
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
+                    "traffic": None, "algorithmic_bytes_per_launch": int(per_launch_bytes),
+                    "launch_ms": round(per_launch_s * 1e3, 4)}
+    lcp = d_lcp.cpu().numpy().view(np.uint32)
+    live8 = intrinsic_live(lcp, n)
+    sort_bytes = sort_algorithmic_bytes(live8, n, w)
+    sort_s = ms / 1e3 / args.steps
+    sort_roof = {"bound": "hbm", "algorithmic_bytes_per_sort": int(sort_bytes),
+                 "achieved": round(sort_bytes / sort_s / 1e9, 1), "peak": peak,
+                 "frac": round(sort_bytes / sort_s / 1e9 / peak, 4),
+                 "live_per_8byte_round_first16": live8[:16], "rounds_8byte": len(live8),
+                 "formula": "sum_r m_r*(4+W+8+24) + n*8, m_r from the LCP array"}
+    launches = sum(v["launches"] * (3 if k == "scan" else 1) for k, v in per_kernel.items())
+    cpu = None
+    if not args.no_cpu and world == 1:
+        cpu = cpu_baseline(args.workload, TextSample(text, starts_of, n))
+    return {
+        "metric": METRIC, "value": job_rate(n, args.steps, world, ms / 1e3), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
+        "config": {"workload": args.workload, "description": DESCRIPTIONS[args.workload],
+                   "n_strings": n, "text_bytes": tlen, "offset_width": w,
+                   "max_lcp": int(lcp.max()) if n else 0,
+                   "mean_lcp": round(float(lcp.mean()), 2) if n else 0,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": f"inputs larger than L2 (text {tlen / 1e9:.2f} GB, offsets "
+                         f"{n * w / 1e9:.2f} GB)"},
+        "key_gbs": round(tlen * args.steps * world / (ms / 1e3) / 1e9, 2),
+        "roofline": roofline, "sort_roofline": sort_roof, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(launches), "clocks": clocks.summary(),
+        "stats": {k: v for k, v in st.as_dict().items()}, "kernels": per_kernel,
+    }
+
+
+class TextSample:
+    """The first strings of a text workload in the form the CPU timers read:
+    the padded text as the arena and the strings' starts as uint64 offsets."""
+
+    def __init__(self, text, starts_of, n):
+        self.arena = text
+        self.n = n
+        self._starts_of = starts_of
+        self.offs = None
+
+    def first(self, m):
+        self.offs = np.ascontiguousarray(self._starts_of(m), dtype=np.uint64)
+        return self
 
 
 def run_batch(args):
@@ -755,6 +940,8 @@ def time_cpu_instances(ss):
 
 def cpu_baseline(workload, ss, reps=3):
     m = min(ss.n, CPU_SAMPLE.get(workload, 2_000_000))
+    if isinstance(ss, TextSample):
+        ss.first(m)
     ts = []
     kind = None
     for _ in range(reps):
@@ -778,6 +965,12 @@ def run_reference(args, rank):
         sample = (f"the first {len(ss.inst_start) - 1} instances ({m:,} strings) of the "
                   f"{args.workload} list per step, each sorted alone")
         timer = lambda: time_cpu_instances(ss)  # noqa: E731
+    elif args.workload in TEXT_WORKLOADS:
+        text, _, _, _, _, n, starts_of = text_workload(args.workload, args.scale)
+        m = min(n, CPU_SAMPLE[args.workload])
+        ss = TextSample(text, starts_of, n).first(m)
+        sample = f"first {m:,} strings of {args.workload} per step (pointers into the whole text)"
+        timer = lambda: time_cpu_sort(ss, m)  # noqa: E731
     else:
         ss = pyssort.WORKLOADS[args.workload](args.scale)
         m = min(ss.n, CPU_SAMPLE.get(args.workload, 2_000_000))
@@ -833,7 +1026,8 @@ def main():
                                  device_id=torch.device(f"cuda:{local_rank}"))
         dist = tdist
     try:
-        out = run_ours(args, rank, world, local_rank, dist)
+        fn = run_text if args.workload in TEXT_WORKLOADS else run_ours
+        out = fn(args, rank, world, local_rank, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -211,6 +211,9 @@ typedef struct {
     uint64_t boundaries;
     uint64_t gather_fused; /* of gather_elems: keys gathered by the first
                               partition level's count kernel (rounds >= 1) */
+    uint64_t warp1_deep;   /* strings re-sorted by the one-per-lane warp sort on
+                              their next 16 bytes within the same round
+                              (SSORT_PARAM_WARP1_DEEP), summed over steps */
 } ssort_stats;
 
 int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
@@ -225,6 +228,10 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                        on a side stream beside the partition; 0: one stream */
 #define SSORT_PARAM_FUSED_GATHER 4  /* 1 (default): from round 1 on, the first partition
                                        level gathers the keys it counts; 0: separate gather */
+#define SSORT_PARAM_WARP1_DEEP 5    /* 0..4096 (default 64): 16-byte steps the warp that
+                                       sorts a segment of <= 32 strings takes on its own
+                                       runs of equal keys before handing what is left to
+                                       the next round; 0: every run waits for the next round */
 int ssort_set_param(ssort_ctx *ctx, int param, int64_t value);
 
 /*

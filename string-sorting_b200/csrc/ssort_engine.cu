@@ -219,6 +219,7 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     stats.gather_elems += h_ctr->gather_elems;
     if (fused_gather) stats.gather_fused += h_ctr->gather_elems;
     stats.warp1_fresh += h_ctr->warp1_fresh;
+    stats.warp1_deep += h_ctr->warp1_deep;
     stats.warp1_keyed += h_ctr->warp1_keyed;
     stats.warp8_fresh += h_ctr->warp8_fresh;
     stats.warp8_keyed += h_ctr->warp8_keyed;
@@ -263,6 +264,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.bkt = ws.bkt;
     a.target_bucket = target_bucket;
     a.warp8_cap = warp8_cap;
+    a.warp1_deep = warp1_deep;
 
     Seg *cur = ws.R, *nxt = ws.N;
     Counters *dc = ws.ctr;
@@ -691,6 +693,11 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
         case SSORT_PARAM_FUSED_GATHER:
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "fused_gather must be 0 or 1");
             ctx->fused_gather = value != 0;
+            return SSORT_OK;
+        case SSORT_PARAM_WARP1_DEEP:
+            if (value < 0 || value > WARP1_DEEP_MAX)
+                return fail(SSORT_EINVAL, "warp1_deep out of range (0..4096)");
+            ctx->warp1_deep = (uint32_t)value;
             return SSORT_OK;
         default:
             return fail(SSORT_EINVAL, "unknown parameter");

@@ -74,6 +74,7 @@ struct ssort_ctx {
     // tuning parameters (ssort_set_param, ssort_autotune)
     uint32_t target_bucket = ssort::TARGET_BUCKET;  // wanted strings per range bucket
     uint32_t warp8_cap = ssort::WARP8_CAP;          // largest one-warp segment
+    uint32_t warp1_deep = ssort::WARP1_DEEP;        // in-warp refinement steps
     bool overlap = true;       // round-0 on-chip sorts on the side stream
     bool fused_gather = true;  // rounds >= 1 gather inside the first count
     // Autotuned values per (size class * 4 + entropy class), applied to later

@@ -40,6 +40,8 @@ struct Seg {
 // larger ones are split by sample partitioning first.
 constexpr int WARP1_CAP = 32;
 constexpr int WARP8_CAP = 256;
+constexpr uint32_t WARP1_DEEP = 64;       // default in-warp refinement steps (16 bytes each)
+constexpr uint32_t WARP1_DEEP_MAX = 4096;
 constexpr int SMALL_CAP = 2048;
 constexpr int SMALL_THREADS = 256;
 constexpr int SMALL_ITEMS = SMALL_CAP / SMALL_THREADS;  // 8
@@ -82,6 +84,7 @@ struct Counters {
         block_keyed;
     unsigned long long equal_moved, equal_final;  // equality-bucket copies / lcp fills
     uint32_t n_small2, n_small3;  // CTA-sort segments of the 2nd and 3rd size class
+    unsigned long long warp1_deep;  // strings re-sorted by in-warp refinement steps
 };
 
 // The CTA-sort segment lists, one per size class (n_small, n_small2, n_small3).
@@ -104,6 +107,7 @@ struct SortArgs {
     uint32_t *bkt;  // per position during a partition level: bucket << 12 | offset
     uint32_t target_bucket;  // wanted strings per range bucket of a partition
     uint32_t warp8_cap;      // largest segment for the one-warp sort (64..WARP8_CAP)
+    uint32_t warp1_deep;     // in-warp refinement steps of the one-per-lane sort
 };
 
 // ---- device workspace ---------------------------------------------------------

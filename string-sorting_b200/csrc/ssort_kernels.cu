@@ -1540,14 +1540,176 @@ __device__ __forceinline__ void load_elem(const SortArgs &a, const Seg &s, uint3
             : load_key(a.arena, a.arena_bytes, string_offset(a.offs, a.off_width, id) + s.depth);
 }
 
+// Order of records in the in-warp refinement: run head first, then (key,
+// index).  Records outside runs carry their own lane as head.
+__device__ __forceinline__ bool run_lt(uint32_t h1, const Key &k1, uint32_t i1, uint32_t h2,
+                                       const Key &k2, uint32_t i2) {
+    return h1 != h2 ? h1 < h2 : pair_lt(k1, i1, k2, i2);
+}
+
+// Runs of exactly two strings, resolved by the whole warp: lane j compares the
+// two strings' 16-byte windows at depth + 16 j, so one step covers 512 bytes;
+// the first lane whose windows differ or end decides order and LCP (what a
+// lane past the end of a string reads is never used).  A pair still equal
+// after PAIR_CHUNKS steps stays a run, 512 * PAIR_CHUNKS bytes deeper.
+// `start` is the lane's group's segment start; a pair's members keep
+// ascending indices (their order when equal).  Warp-collective.
+constexpr uint32_t PAIR_CHUNKS = 16;
+
+template <int W>
+__device__ __forceinline__ void warp1_pairs(const uint8_t *__restrict__ arena,
+                                            uint64_t arena_bytes, const void *__restrict__ offs,
+                                            int off_width, uint32_t *__restrict__ idx0,
+                                            uint32_t *__restrict__ lcp, uint32_t start,
+                                            uint32_t lane, uint32_t id, bool &run, uint32_t &h,
+                                            uint32_t &depth, uint32_t &moved) {
+    const uint32_t li = lane & (W - 1);
+    const uint32_t nh1 = __shfl_down_sync(0xffffffffu, h, 1);
+    const uint32_t nh2 = __shfl_down_sync(0xffffffffu, h, 2);
+    const bool nr1 = __shfl_down_sync(0xffffffffu, (int)run, 1) != 0;
+    const bool nr2 = __shfl_down_sync(0xffffffffu, (int)run, 2) != 0;
+    const bool pair_head = run && h == lane && li + 1 < (uint32_t)W && nr1 && nh1 == h &&
+                           !(li + 2 < (uint32_t)W && nr2 && nh2 == h);
+    uint32_t pairs = __ballot_sync(0xffffffffu, pair_head);
+    while (pairs) {
+        const uint32_t p = __ffs(pairs) - 1;
+        pairs &= pairs - 1;
+        const uint32_t ia = __shfl_sync(0xffffffffu, id, p);
+        const uint32_t ib = __shfl_sync(0xffffffffu, id, p + 1);
+        const uint32_t d0 = __shfl_sync(0xffffffffu, depth, p);
+        const uint32_t pos = __shfl_sync(0xffffffffu, start, p) + (p & (W - 1));
+        const uint64_t oa = string_offset(offs, off_width, ia);
+        const uint64_t ob = string_offset(offs, off_width, ib);
+        uint32_t chunk = 0, found = 0;
+        for (; chunk < PAIR_CHUNKS; ++chunk) {
+            const uint64_t at = (uint64_t)d0 + chunk * (32u * KEY_BYTES) + lane * KEY_BYTES;
+            const Key ka = load_key(arena, arena_bytes, oa + at);
+            const Key kb = load_key(arena, arena_bytes, ob + at);
+            const bool same = key_eq(ka, kb);
+            const uint32_t stop = __ballot_sync(0xffffffffu, !same || key_is_end(ka));
+            if (stop) {
+                const uint32_t f = __ffs(stop) - 1;
+                if (lane == f) {
+                    const uint32_t base_d = (uint32_t)at;
+                    const bool swap = !same && key_lt(kb, ka);
+                    idx0[pos] = swap ? ib : ia;
+                    idx0[pos + 1] = swap ? ia : ib;
+                    lcp[pos + 1] = base_d + (same ? key_len(ka) : key_lcp(ka, kb));
+                }
+                found = 1;
+                break;
+            }
+        }
+        if (lane == p || lane == p + 1) {
+            if (found) {
+                run = false;
+                h = lane;
+            } else {
+                depth += PAIR_CHUNKS * 32u * KEY_BYTES;
+            }
+        }
+        if (lane == p) moved += 2 * (chunk + found);
+    }
+}
+
+// In-warp refinement of the runs a one-per-lane sort left (lanes with `run`,
+// h = the run's first lane, keys equal up to `depth`, id = the lane's record):
+// the members load their next 16 bytes, each run is re-sorted inside its own
+// lanes, the LCPs decided at this depth are written, and the runs of equal
+// keys that remain become the next step's runs; at most `steps` steps, then
+// what is left goes to the next round.  This is the next round's one-warp sort
+// of those runs done without a round trip: the same order and LCPs.  The keys
+// of the segment's first and last position, which the round's boundary pass
+// reads, stay as the first sort wrote them.  Returns the strings this lane
+// re-sorted.  Warp-collective.
+template <int W>
+__device__ __forceinline__ uint32_t warp1_deepen(const uint8_t *__restrict__ arena,
+                                              uint64_t arena_bytes, const void *__restrict__ offs,
+                                              int off_width, uint32_t *__restrict__ idx0,
+                                              uint32_t *__restrict__ lcp, uint32_t steps,
+                                              uint32_t start, uint32_t depth, uint32_t lane,
+                                              uint32_t id, bool run, uint32_t h, Seg *N,
+                                              Counters *c) {
+    const uint32_t li = lane & (W - 1), base = lane & ~(uint32_t)(W - 1);
+    const uint32_t m = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+    uint32_t moved = 0;
+    Key k = key_max();  // records outside runs are never compared by key
+    for (uint32_t it = 0; it < steps && __any_sync(0xffffffffu, run); ++it) {
+        warp1_pairs<W>(arena, arena_bytes, offs, off_width, idx0, lcp, start, lane, id, run, h,
+                       depth, moved);
+        if (!__any_sync(0xffffffffu, run)) break;
+        if (run) k = load_key(arena, arena_bytes, string_offset(offs, off_width, id) + depth);
+        moved += run;
+        // Sorting by (head, key, index) keeps every record outside a run in
+        // its lane and every run inside its own lanes.
+        uint32_t hh = run ? h : lane;
+        bool r = run;
+#pragma unroll
+        for (int kk = 2; kk <= W; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                Key ok;
+                ok.hi = __shfl_xor_sync(0xffffffffu, k.hi, j);
+                ok.lo = __shfl_xor_sync(0xffffffffu, k.lo, j);
+                const uint32_t oi = __shfl_xor_sync(0xffffffffu, id, j);
+                const uint32_t oh = __shfl_xor_sync(0xffffffffu, hh, j);
+                const bool orr = __shfl_xor_sync(0xffffffffu, (int)r, j) != 0;
+                const bool up = kk == W || (lane & kk) == 0;
+                const bool keep_min = ((lane & j) == 0) == up;
+                const bool take = keep_min ? run_lt(oh, ok, oi, hh, k, id)
+                                           : run_lt(hh, k, id, oh, ok, oi);
+                if (take) {
+                    k = ok;
+                    id = oi;
+                    hh = oh;
+                    r = orr;
+                }
+            }
+        }
+        Key prev, next;
+        prev.hi = __shfl_up_sync(0xffffffffu, k.hi, 1);
+        prev.lo = __shfl_up_sync(0xffffffffu, k.lo, 1);
+        next.hi = __shfl_down_sync(0xffffffffu, k.hi, 1);
+        next.lo = __shfl_down_sync(0xffffffffu, k.lo, 1);
+        const uint32_t ph = __shfl_up_sync(0xffffffffu, hh, 1);
+        const uint32_t nh = __shfl_down_sync(0xffffffffu, hh, 1);
+        // A run's head is one of its members' lanes, never another record's
+        // own lane, so equal heads mean the same run.
+        const bool same_prev = r && li > 0 && ph == hh;
+        const bool same_next = r && li + 1 < (uint32_t)W && nh == hh;
+        const bool eqp = same_prev && key_eq(prev, k);
+        const bool eqn = same_next && key_eq(next, k);
+        if (r) {
+            const uint32_t p = start + li;
+            idx0[p] = id;
+            if (same_prev) {
+                if (!eqp)
+                    lcp[p] = depth + key_lcp(prev, k);
+                else if (key_is_end(k))
+                    lcp[p] = depth + key_len(k);
+            }
+        }
+        run = r && !key_is_end(k) && (eqp || eqn);
+        const uint32_t heads = __ballot_sync(0xffffffffu, run && !eqp);
+        h = run ? 31 - __clz(heads & m) : lane;
+        depth += KEY_BYTES;
+    }
+    // What is still unresolved goes to the next round at the depth reached.
+    const uint32_t nh = __shfl_down_sync(0xffffffffu, h, 1);
+    const bool nrun = __shfl_down_sync(0xffffffffu, (int)run, 1) != 0;
+    const bool tail = run && !(li + 1 < (uint32_t)W && nrun && nh == h);
+    emit_next_warp(N, c, tail, start + (h - base), lane - h + 1, depth);
+    return moved;
+}
+
 // Sorts one segment of at most W strings held by the W lanes of one aligned
 // lane group (W = 8 or 32; lane li of the group holds string li).  Every
 // lane of the warp calls this with its group's segment (len 0 for idle
 // groups): the shuffles, ballots and the next-round append are
 // warp-collective.
 template <int W>
-__device__ __forceinline__ void warp1_group(const SortArgs &a, const Seg &s, uint32_t lane,
-                                            Seg *N, Counters *c) {
+__device__ __forceinline__ uint32_t warp1_group(const SortArgs &a, const Seg &s, uint32_t lane,
+                                                Seg *N, Counters *c) {
     const uint32_t li = lane & (W - 1), base = lane & ~(uint32_t)(W - 1);
     const bool v = li < s.len;
     uint32_t id = IDX_MAX;
@@ -1623,8 +1785,6 @@ __device__ __forceinline__ void warp1_group(const SortArgs &a, const Seg &s, uin
     next.lo = __shfl_down_sync(0xffffffffu, k.lo, 1);
     const bool head = v && (li == 0 || !key_eq(prev, k));
     const uint32_t heads = __ballot_sync(0xffffffffu, head);
-    bool want = false;
-    uint32_t h = lane;
     if (v) {
         const uint32_t p = s.start + li;
         a.idx[0][p] = id;
@@ -1635,14 +1795,20 @@ __device__ __forceinline__ void warp1_group(const SortArgs &a, const Seg &s, uin
             else if (key_is_end(k))
                 a.lcp[p] = s.depth + key_len(k);
         }
-        const bool tail = li == s.len - 1 || !key_eq(next, k);
-        if (tail && !head && !key_is_end(k)) {
-            const uint32_t m = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
-            h = 31 - __clz(heads & m);  // the run's head: at or after the group's lane 0
-            want = true;
-        }
     }
-    emit_next_warp(N, c, want, s.start + (h - base), lane - h + 1, s.depth + KEY_BYTES);
+    // Runs: maximal groups of at least two equal keys that do not end; h is
+    // the run's first lane (at or after the group's lane 0).
+    const bool eq_next = v && li + 1 < s.len && key_eq(next, k);
+    bool run = v && !key_is_end(k) && (!head || eq_next);
+    const uint32_t m = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+    uint32_t h = run ? 31 - __clz(heads & m) : lane;
+    if (a.warp1_deep && __any_sync(0xffffffffu, run))
+        return warp1_deepen<W>(a.arena, a.arena_bytes, a.offs, a.off_width, a.idx[0], a.lcp,
+                               a.warp1_deep, s.start, s.depth + KEY_BYTES, lane, id, run, h, N,
+                               c);
+    const bool tail = run && !eq_next;  // a run's last lane
+    emit_next_warp(N, c, tail, s.start + (h - base), lane - h + 1, s.depth + KEY_BYTES);
+    return 0;
 }
 
 // Segments of <= WARP1_CAP strings.  First pass: a warp takes W1_PACK
@@ -1656,7 +1822,7 @@ __global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *_
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    unsigned long long fresh = 0, keyed = 0;
+    unsigned long long fresh = 0, keyed = 0, deep = 0;
     for (uint32_t g0 = warp0 * W1_PACK; g0 < nT; g0 += nwarps * W1_PACK) {
         const uint32_t j = lane >> 3;
         const Seg sj = g0 + j < nT ? T[g0 + j] : Seg{0, 0, 0, 0};
@@ -1668,16 +1834,18 @@ __global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *_
                 fresh += sj.len;
         }
         if (__any_sync(0xffffffffu, small && sj.len > 0))
-            warp1_group<8>(a, small ? sj : Seg{0, 0, 0, 0}, lane, N, c);
+            deep += warp1_group<8>(a, small ? sj : Seg{0, 0, 0, 0}, lane, N, c);
     }
     for (uint32_t g = warp0; g < nT; g += nwarps) {
         const Seg s = T[g];
-        if (s.len > 8) warp1_group<32>(a, s, lane, N, c);
+        if (s.len > 8) deep += warp1_group<32>(a, s, lane, N, c);
     }
     if ((lane & 7) == 0 && (fresh | keyed)) {  // each 8-lane group's leader
         atomicAdd(&c->warp1_fresh, fresh);
         atomicAdd(&c->warp1_keyed, keyed);
     }
+    deep = warp_sum(deep);
+    if (lane == 0 && deep) atomicAdd(&c->warp1_deep, deep);
 }
 
 // Warp-wide OR of key ^ key0 over the records at padded positions 0..len-1.

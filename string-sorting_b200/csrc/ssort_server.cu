@@ -72,7 +72,6 @@ class RangeAlloc {
         free_[off] = size;
     }
     uint64_t used() const { return used_; }
-    uint64_t cap() const { return cap_; }
 
    private:
     std::map<uint64_t, uint64_t> free_;
@@ -161,6 +160,7 @@ struct ssort_server {
         a.bkt = ctx->ws.bkt;
         a.target_bucket = ctx->target_bucket;
         a.warp8_cap = ctx->warp8_cap;
+        a.warp1_deep = ctx->warp1_deep;
         return a;
     }
 

@@ -36,6 +36,7 @@ SSORT_PARAM_TARGET_BUCKET = 1
 SSORT_PARAM_WARP8_CAP = 2
 SSORT_PARAM_OVERLAP = 3
 SSORT_PARAM_FUSED_GATHER = 4
+SSORT_PARAM_WARP1_DEEP = 5
 
 
 class SsortError(RuntimeError):
@@ -65,6 +66,7 @@ class Stats(ctypes.Structure):
         ("equal_final", ctypes.c_uint64),
         ("boundaries", ctypes.c_uint64),
         ("gather_fused", ctypes.c_uint64),
+        ("warp1_deep", ctypes.c_uint64),
     ]
 
     def as_dict(self):
@@ -288,22 +290,28 @@ class Sorter:
                                              _ptr(lcp)))
         return perm, lcp
 
-    def sort_text(self, text, mode=TEXT_LINES, with_lcp=True):
+    def sort_text(self, text, mode=TEXT_LINES, with_lcp=True, out=None, lcp=None):
         """Sort the strings of a whole text (bytes or uint8 array) as sortstring
-        makes them; returns (sorted string starts as uint64 offsets, lcp)."""
+        makes them; returns (sorted string starts as uint64 offsets, lcp).
+        With `out` given (uint64, one entry per string, and `lcp` likewise when
+        with_lcp) the call writes there and skips the sizing call."""
         buf = np.frombuffer(text, dtype=np.uint8) if isinstance(text, (bytes, bytearray)) \
             else np.ascontiguousarray(text, dtype=np.uint8)
         L = lib()
         n = ctypes.c_uint64()
-        rc = L.ssort_sort_text_host(self._ctx, _ptr(buf), buf.nbytes, int(mode), None, None, 0,
-                                    ctypes.byref(n))
-        if rc != SSORT_OK and n.value == 0:
-            _check(rc)
-        out = np.empty(n.value, dtype=np.uint64)
-        lcp = np.empty(n.value, dtype=np.uint32) if with_lcp else None
+        if out is None:
+            rc = L.ssort_sort_text_host(self._ctx, _ptr(buf), buf.nbytes, int(mode), None, None,
+                                        0, ctypes.byref(n))
+            if rc != SSORT_OK and n.value == 0:
+                _check(rc)
+            out = np.empty(n.value, dtype=np.uint64)
+        if with_lcp and lcp is None:
+            lcp = np.empty(len(out), dtype=np.uint32)
+        if not with_lcp:
+            lcp = None
         _check(L.ssort_sort_text_host(self._ctx, _ptr(buf), buf.nbytes, int(mode), _ptr(out),
-                                      _ptr(lcp), n.value, ctypes.byref(n)))
-        return out, lcp
+                                      _ptr(lcp), len(out), ctypes.byref(n)))
+        return out[:n.value], lcp[:n.value] if lcp is not None else None
 
     def text_offsets_device(self, d_text, text_len, mode, d_offs, off_width, cap, stream=None):
         """String starts of a device-resident text (torch tensors or
@@ -545,6 +553,28 @@ def gen_urls(n, n_hosts=4096, zipf_s=1.1, seed=2):
 def gen_zipf_words(n, vocab=1_000_000, p_geom=0.15, max_len=24, zipf_s=1.0, seed=3):
     a, nb, o = _gen(wlib().ssw_gen_zipf_words, n, vocab, p_geom, max_len, zipf_s, seed)
     return StringSet(a, nb, o, n)
+
+
+def gen_repeat_text(nbytes, n_repeats=2000, min_rep=32, max_rep=4096, seed=8):
+    """A text of nbytes bytes for suffix sorting: Zipf(1.0) words (as
+    gen_zipf_words, seed `seed`) separated by single spaces, then n_repeats
+    passages of log-uniform length in [min_rep, max_rep] copied from a uniform
+    position to another (the long repeats of real corpora, which make suffix
+    LCPs deep).  Returns a uint8 array: the text followed by 16 zero bytes."""
+    words = gen_zipf_words(nbytes // 7 + 64, seed=seed)  # >= 8 bytes per word on average
+    if words.text_bytes < nbytes:
+        raise ValueError("word text shorter than requested")
+    text = np.zeros(nbytes + 16, dtype=np.uint8)
+    text[:nbytes] = words.arena[:nbytes]
+    body = text[:nbytes]
+    body[body == 0] = ord(" ")
+    rng = np.random.default_rng(seed)
+    lens = np.exp(rng.uniform(np.log(min_rep), np.log(max_rep), size=n_repeats)).astype(np.int64)
+    lens = np.minimum(lens, nbytes // 2)
+    for L in lens:
+        a, b = rng.integers(0, nbytes - L, size=2)
+        body[b:b + L] = body[a:a + L].copy()
+    return text
 
 
 class InstanceSet(StringSet):

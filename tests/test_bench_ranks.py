@@ -55,3 +55,32 @@ def test_reference_arm_times_instances_alone(workload):
     assert len(ss.inst_start) >= 2 and ss.n == int(ss.inst_start[-1])
     t, kind = bench.time_cpu_instances(ss)
     assert t > 0 and kind in ("reference", "port")
+
+
+def test_intrinsic_live_counts_strings_per_8_byte_round():
+    """Strings live at depth 8r: those sharing >= 8r bytes with a neighbour
+    (the definition, counted directly)."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        n = int(rng.integers(1, 500))
+        lcp = rng.integers(0, int(rng.integers(1, 200)), size=n).astype(np.uint32)
+        lcp[0] = 0
+        nb = np.maximum(lcp, np.append(lcp[1:], 0)).astype(np.int64)
+        want = [n] + [int((nb >= d).sum()) for d in range(8, int(nb.max()) + 1, 8)]
+        assert bench.intrinsic_live(lcp, n) == want
+    assert bench.intrinsic_live(np.zeros(0, np.uint32), 0) == [0]
+
+
+def test_text_workload_cpu_sample():
+    """The CPU timer of the suffix workload reads the first m suffixes of the
+    text (uint64 offsets 0..m-1 into it)."""
+    import numpy as np
+    text, tlen, mode, host_mode, host_text, n, starts_of = bench.text_workload(
+        "suffixes_160m", 0.001)
+    assert tlen == 160_000 and n == tlen and len(text) == tlen + 16
+    assert np.array_equal(host_text(), text[:tlen])
+    ss = bench.TextSample(text, starts_of, n).first(5000)
+    assert ss.offs.dtype == np.uint64 and list(ss.offs[:3]) == [0, 1, 2]
+    t, kind = bench.time_cpu_sort(ss, 5000)
+    assert t > 0 and kind in ("reference", "port")

@@ -20,6 +20,9 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_FUSED_GATHER, 0),
     (pyssort.SSORT_PARAM_TARGET_BUCKET, 128),
     (pyssort.SSORT_PARAM_TARGET_BUCKET, 1024),
+    (pyssort.SSORT_PARAM_WARP1_DEEP, 0),
+    (pyssort.SSORT_PARAM_WARP1_DEEP, 1),
+    (pyssort.SSORT_PARAM_WARP1_DEEP, 4096),
 ]
 
 
@@ -41,6 +44,29 @@ def test_parameter_values_keep_results(golden, param, value):
         assert np.array_equal(p, rp) and np.array_equal(l, rl)
 
 
+@pytest.mark.parametrize("deep", [0, 1, 2, 64, 4096])
+def test_in_warp_refinement_on_deep_suffixes(deep):
+    """Suffixes of a text with copied passages: runs of two or three strings
+    sharing hundreds of bytes, refined in the warp (up to `deep` 16-byte steps
+    per round, the rest in later rounds); results are the oracle's under every
+    step limit, including limits that leave runs for the next round."""
+    text = pyssort.gen_repeat_text(300_000, n_repeats=40, seed=12)
+    offs = np.arange(300_000, dtype=np.uint64)
+    rp, rl = pyoracle.oracle_sort(text, offs)
+    assert rl.max() > 500
+    with pyssort.Sorter(0) as s:
+        s.set_param(pyssort.SSORT_PARAM_WARP1_DEEP, deep)
+        p, l = s.sort_host(text, offs)
+        st = s.stats()
+    assert np.array_equal(p, rp) and np.array_equal(l, rl)
+    if deep == 0:
+        assert st.warp1_deep == 0
+    else:
+        assert st.warp1_deep > 0
+    if deep >= 64:
+        assert st.rounds < 20  # without the refinement: about max lcp / 16 rounds
+
+
 def test_out_of_range_parameters_are_rejected():
     with pyssort.Sorter(0) as s:
         for param, value in [(pyssort.SSORT_PARAM_WARP8_CAP, 32),
@@ -48,6 +74,8 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_OVERLAP, 2),
                              (pyssort.SSORT_PARAM_FUSED_GATHER, -1),
                              (pyssort.SSORT_PARAM_TARGET_BUCKET, 4096),
+                             (pyssort.SSORT_PARAM_WARP1_DEEP, -1),
+                             (pyssort.SSORT_PARAM_WARP1_DEEP, 4097),
                              (99, 1)]:
             with pytest.raises(pyssort.SsortError) as e:
                 s.set_param(param, value)

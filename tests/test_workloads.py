@@ -51,3 +51,19 @@ def test_offsets_ascending_and_nul_terminated():
     ends = np.append(z.offs[1:].astype(np.int64), z.text_bytes) - 1
     assert np.all(z.arena[ends] == 0)
     assert np.all(z.arena[z.text_bytes:z.text_bytes + 16] == 0)
+
+
+def test_repeat_text_shape_determinism_and_depth():
+    """The suffix-sorting text: deterministic, padded with 16 zero bytes, no
+    NUL inside, and its copied passages give suffix LCPs hundreds of bytes
+    deep (checked with the oracle on a small text)."""
+    import pyoracle
+    a = pyssort.gen_repeat_text(400_000, n_repeats=20, seed=8)
+    b = pyssort.gen_repeat_text(400_000, n_repeats=20, seed=8)
+    c = pyssort.gen_repeat_text(400_000, n_repeats=20, seed=9)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    assert len(a) == 400_016 and not a[400_000:].any()
+    assert np.count_nonzero(a[:400_000] == 0) == 0
+    assert set(np.unique(a[:400_000])) <= set(range(ord("a"), ord("z") + 1)) | {ord(" ")}
+    _, lcp = pyoracle.oracle_sort(a, np.arange(400_000, dtype=np.uint64))
+    assert lcp.max() > 500
