@@ -214,6 +214,10 @@ typedef struct {
     uint64_t warp1_deep;   /* strings re-sorted by the one-per-lane warp sort on
                               their next 16 bytes within the same round
                               (SSORT_PARAM_WARP1_DEEP), summed over steps */
+    uint64_t full_sorted;  /* strings of on-chip sorted segments whose packed
+                              64-bit keys could not order them (a run of more
+                              than 64 equal windows) and were re-sorted with
+                              the full key comparator */
 } ssort_stats;
 
 int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);

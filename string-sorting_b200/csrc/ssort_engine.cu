@@ -220,6 +220,7 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     if (fused_gather) stats.gather_fused += h_ctr->gather_elems;
     stats.warp1_fresh += h_ctr->warp1_fresh;
     stats.warp1_deep += h_ctr->warp1_deep;
+    stats.full_sorted += h_ctr->full_sorted;
     stats.warp1_keyed += h_ctr->warp1_keyed;
     stats.warp8_fresh += h_ctr->warp8_fresh;
     stats.warp8_keyed += h_ctr->warp8_keyed;

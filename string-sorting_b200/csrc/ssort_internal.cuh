@@ -85,6 +85,7 @@ struct Counters {
     unsigned long long equal_moved, equal_final;  // equality-bucket copies / lcp fills
     uint32_t n_small2, n_small3;  // CTA-sort segments of the 2nd and 3rd size class
     unsigned long long warp1_deep;  // strings re-sorted by in-warp refinement steps
+    unsigned long long full_sorted;  // strings of segments re-sorted by the full comparator
 };
 
 // The CTA-sort segment lists, one per size class (n_small, n_small2, n_small3).

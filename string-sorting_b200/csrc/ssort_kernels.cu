@@ -512,6 +512,56 @@ __device__ __forceinline__ bool window_pairs_ok_ind(const ulonglong2 *sk, const 
     return ok;
 }
 
+// Runs of equal windows after a packed sort hold their records in position
+// order.  window_runs_short: no run is longer than FIX_RUN_CAP (else the
+// caller sorts the whole segment with the full comparator).  sort_window_runs:
+// the thread that owns a run's first element puts the run into full (key,
+// position) order in place (insertion sort: equal keys keep position order).
+// Runs are disjoint and every entry of a run has the run's window bits, so
+// the neighbours another thread reads keep their windows while it sorts.
+constexpr uint32_t FIX_RUN_CAP = 64;
+
+__device__ __forceinline__ bool window_run_start(const uint64_t *sv, uint32_t len, uint32_t e) {
+    const uint64_t w = sv[pad(e)] >> POS_BITS;
+    return e + 1 < len && (sv[pad(e + 1)] >> POS_BITS) == w &&
+           (e == 0 || (sv[pad(e - 1)] >> POS_BITS) != w);
+}
+
+__device__ __forceinline__ bool window_runs_short(const uint64_t *sv, uint32_t len, uint32_t t,
+                                                  uint32_t threads) {
+    for (uint32_t e = t; e + 1 < len; e += threads) {
+        if (!window_run_start(sv, len, e)) continue;
+        const uint64_t w = sv[pad(e)] >> POS_BITS;
+        const uint32_t r = min(len, e + FIX_RUN_CAP + 1);
+        uint32_t q = e + 2;
+        while (q < r && (sv[pad(q)] >> POS_BITS) == w) ++q;
+        if (q - e > FIX_RUN_CAP) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void sort_window_runs(const ulonglong2 *sk, uint64_t *sv, uint32_t len,
+                                                 uint32_t t, uint32_t threads) {
+    for (uint32_t e = t; e + 1 < len; e += threads) {
+        if (!window_run_start(sv, len, e)) continue;
+        const uint64_t w = sv[pad(e)] >> POS_BITS;
+        uint32_t r = e + 2;
+        while (r < len && (sv[pad(r)] >> POS_BITS) == w) ++r;
+        for (uint32_t i = e + 1; i < r; ++i) {
+            const uint64_t v = sv[pad(i)];
+            const Key kv = to_key(sk[pad((uint32_t)(v & POS_MASK))]);
+            uint32_t j = i;
+            while (j > e) {
+                const uint64_t u = sv[pad(j - 1)];
+                if (!key_lt(kv, to_key(sk[pad((uint32_t)(u & POS_MASK))]))) break;
+                sv[pad(j)] = u;
+                --j;
+            }
+            sv[pad(j)] = v;
+        }
+    }
+}
+
 // One warp: packed keys of the records at slots base .. base + 32*ITEMS - 1
 // (positions >= len pad with all-ones), sorted, stored to sv.
 template <int ITEMS>
@@ -1884,7 +1934,7 @@ __global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg
                                                 W8_WARPS * W8_PAD) + w * W8_PAD;
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    unsigned long long fresh = 0, keyed = 0;
+    unsigned long long fresh = 0, keyed = 0, full = 0;
     for (uint32_t g = warp0; g < nT; g += nwarps) {
         const Seg s = T[g];
         if (s.flags & SEG_KEYS)
@@ -1925,6 +1975,11 @@ __global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg
             __syncwarp();
             packed = __all_sync(0xffffffffu, window_pairs_ok_ind(sk, sv, s.len, lane, 32));
             if (!packed) {
+                packed = __all_sync(0xffffffffu, window_runs_short(sv, s.len, lane, 32));
+                if (packed) sort_window_runs(sk, sv, s.len, lane, 32);
+            }
+            if (!packed) {
+                full += s.len;
                 if (P <= 64)
                     warp_sort_run<2>(sk, sx, 0, lane);
                 else if (P <= 128)
@@ -1943,6 +1998,7 @@ __global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg
     if (lane == 0 && (fresh | keyed)) {
         atomicAdd(&c->warp8_fresh, fresh);
         atomicAdd(&c->warp8_keyed, keyed);
+        if (full) atomicAdd(&c->full_sorted, full);
     }
 }
 
@@ -2081,7 +2137,7 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
     static_assert(G * PADC == SMALL_PAD, "group slots");
     extern __shared__ __align__(16) unsigned char block_smem[];
     __shared__ uint64_t red[2][SMALL_THREADS / 32];
-    __shared__ int ok_flag[G];
+    __shared__ int ok_flag[G], fix_flag[G];
     const uint32_t gi = threadIdx.x / GT, t = threadIdx.x % GT;
     const uint32_t lane = threadIdx.x & 31, gw = t >> 5, w = threadIdx.x >> 5;
     ulonglong2 *sk_all = reinterpret_cast<ulonglong2 *>(block_smem);
@@ -2090,7 +2146,7 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
     ulonglong2 *sk = sk_all + gi * PADC;
     uint64_t *sv = sv_all + gi * PADC;
     uint32_t *sx = sx_all + gi * PADC;
-    unsigned long long fresh = 0, keyed = 0;
+    unsigned long long fresh = 0, keyed = 0, full = 0;
     for (uint32_t g = (blockIdx.x - cta0) * G + gi; g < nS; g += ncta * G) {
         const Seg s = S[g];
         if (s.flags & SEG_KEYS)
@@ -2120,7 +2176,7 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
                 }
             }
         }
-        if (t == 0) ok_flag[gi] = 1;
+        if (t == 0) ok_flag[gi] = fix_flag[gi] = 1;
         group_sync<GT>(gi);
         // f: first bit in which the keys differ.
         {
@@ -2157,7 +2213,17 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
             if (!window_pairs_ok_ind(sk, sv, s.len, t, GT)) ok_flag[gi] = 0;
             group_sync<GT>(gi);
             packed = ok_flag[gi] != 0;
-            if (!packed) group_sort_full<GT>(sk, sx, span, t, gi);
+            if (!packed) {
+                if (!window_runs_short(sv, s.len, t, GT)) fix_flag[gi] = 0;
+                group_sync<GT>(gi);
+                packed = fix_flag[gi] != 0;
+                if (packed) {
+                    sort_window_runs(sk, sv, s.len, t, GT);
+                } else {
+                    if (t == 0) full += s.len;
+                    group_sort_full<GT>(sk, sx, span, t, gi);
+                }
+            }
         }
         group_sync<GT>(gi);
         if (packed)
@@ -2169,6 +2235,7 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
     if (t == 0 && (fresh | keyed)) {
         atomicAdd(&c->block_fresh, fresh);
         atomicAdd(&c->block_keyed, keyed);
+        if (full) atomicAdd(&c->full_sorted, full);
     }
 }
 

@@ -67,6 +67,7 @@ class Stats(ctypes.Structure):
         ("boundaries", ctypes.c_uint64),
         ("gather_fused", ctypes.c_uint64),
         ("warp1_deep", ctypes.c_uint64),
+        ("full_sorted", ctypes.c_uint64),
     ]
 
     def as_dict(self):

@@ -130,3 +130,32 @@ def test_full_size_properties(wl, sorter):
     perm, lcp = sorter.sort_host(ss.arena, ss.offs)
     bad, first = pyoracle.oracle_check(ss.arena, ss.offs, perm, lcp)
     assert bad == 0, f"{bad} violations, first at {first}"
+
+
+def _tied_window_strings(n, lead, alpha, seed):
+    """`lead` random bytes from the first `alpha` letters, then 8 equal bytes,
+    then 6 random letters: the keys differ first in byte 0, so the 53-bit
+    window after that bit ends inside the equal bytes and all strings with the
+    same lead bytes tie on it."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        out.append(bytes(rng.integers(97, 97 + alpha, size=lead, dtype=np.uint8)) + b"QQQQQQQQ" +
+                   bytes(rng.integers(97, 123, size=6, dtype=np.uint8)))
+    return out
+
+
+@pytest.mark.parametrize("n,lead,alpha,full", [(200, 2, 26, False), (1500, 2, 26, False),
+                                               (700, 2, 26, False), (1500, 1, 2, True),
+                                               (200, 1, 2, True)])
+def test_tied_packed_windows(sorter, n, lead, alpha, full):
+    """Segments of the one-warp (<= 256) and CTA (<= 2048) sorts whose packed
+    keys tie: runs of up to 64 tied records are put in order in place, longer
+    ones fall back to the full comparator; both give the oracle's order and
+    LCPs."""
+    strings = _tied_window_strings(n, lead, alpha, seed=n + lead)
+    arena, offs = cases.arena_of(strings)
+    perm, lcp = sorter.sort_host(arena, offs)
+    ref_perm, ref_lcp = pyoracle.oracle_sort(arena, offs)
+    assert np.array_equal(perm, ref_perm) and np.array_equal(lcp, ref_lcp)
+    assert (sorter.stats().full_sorted > 0) == full
