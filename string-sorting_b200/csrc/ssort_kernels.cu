@@ -731,36 +731,52 @@ __global__ void k_unbase(uint32_t *perm, const ReqJob *__restrict__ jobs, uint32
 // (src/sortstring.c:310-335): every delimiter byte ('\n', or NUL with --raw)
 // ends one string, the next string starts right after it, text after the last
 // delimiter is not a string, and '\n' delimiters are overwritten with NUL.
-// Each CTA covers TEXT_TILE bytes, 16 per thread.
+// Each CTA covers TEXT_TILE bytes: every thread TEXT_VEC consecutive 16-byte
+// chunks, loaded together before any is examined.
 constexpr int TEXT_THREADS = 256;
-constexpr uint64_t TEXT_TILE = TEXT_THREADS * 16;
+constexpr int TEXT_VEC = 4;
+constexpr uint64_t TEXT_TILE = TEXT_THREADS * 16 * TEXT_VEC;
 
-// Bit b of the result is set when text[base + b] == delim (positions at or
-// past len never match).
-__device__ __forceinline__ uint32_t delim_mask16(const uint8_t *__restrict__ text, uint64_t len,
-                                                 uint64_t base, uint8_t delim) {
-    uint32_t m = 0;
-    if (base + 16 <= len) {
-        const uint4 v = *reinterpret_cast<const uint4 *>(text + base);
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+// Bit b of a 4-byte word's result is set when byte b equals the delimiter.
+__device__ __forceinline__ uint32_t delim_bits4(uint32_t w, uint32_t d4) {
+    const uint32_t t = __vcmpeq4(w, d4) & 0x01010101u;
+    return (t | (t >> 7) | (t >> 14) | (t >> 21)) & 0xFu;
+}
+
+// m[c], bit b: text[base + 16 c + b] == delim (positions at or past len never
+// match); the thread's chunks start at base (a multiple of 16).
+__device__ __forceinline__ void delim_masks(const uint8_t *__restrict__ text, uint64_t len,
+                                            uint64_t base, uint8_t delim,
+                                            uint32_t (&m)[TEXT_VEC]) {
+    if (base + 16 * TEXT_VEC <= len) {
+        const uint32_t d4 = 0x01010101u * delim;
+        uint4 v[TEXT_VEC];
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int c = 0; c < TEXT_VEC; ++c) v[c] = reinterpret_cast<const uint4 *>(text + base)[c];
 #pragma unroll
-            for (int b = 0; b < 4; ++b)
-                if (((w[q] >> (8 * b)) & 0xFF) == delim) m |= 1u << (4 * q + b);
+        for (int c = 0; c < TEXT_VEC; ++c)
+            m[c] = delim_bits4(v[c].x, d4) | delim_bits4(v[c].y, d4) << 4 |
+                   delim_bits4(v[c].z, d4) << 8 | delim_bits4(v[c].w, d4) << 12;
     } else {
-        for (int b = 0; b < 16 && base + b < len; ++b)
-            if (text[base + b] == delim) m |= 1u << b;
+#pragma unroll
+        for (int c = 0; c < TEXT_VEC; ++c) {
+            m[c] = 0;
+            for (uint64_t b = 0; b < 16 && base + 16 * c + b < len; ++b)
+                if (text[base + 16 * c + b] == delim) m[c] |= 1u << b;
+        }
     }
-    return m;
 }
 
 __global__ void __launch_bounds__(TEXT_THREADS)
     k_text_count(const uint8_t *__restrict__ text, uint64_t len, uint8_t delim,
                  uint32_t *tile_cnt, unsigned long long *total) {
     __shared__ uint32_t warp_sums[TEXT_THREADS / 32];
-    const uint64_t base = blockIdx.x * TEXT_TILE + threadIdx.x * 16ull;
-    uint32_t c = __popc(delim_mask16(text, len, base, delim));
+    const uint64_t base = blockIdx.x * TEXT_TILE + threadIdx.x * (16ull * TEXT_VEC);
+    uint32_t m[TEXT_VEC];
+    delim_masks(text, len, base, delim, m);
+    uint32_t c = 0;
+#pragma unroll
+    for (int q = 0; q < TEXT_VEC; ++q) c += __popc(m[q]);
 #pragma unroll
     for (int d = 16; d; d >>= 1) c += __shfl_xor_sync(0xffffffffu, c, d);
     if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = c;
@@ -780,9 +796,12 @@ __global__ void __launch_bounds__(TEXT_THREADS)
                   uint64_t n, void *offs, int off_width) {
     __shared__ uint32_t warp_sums[TEXT_THREADS / 32];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint64_t base = blockIdx.x * TEXT_TILE + threadIdx.x * 16ull;
-    uint32_t m = delim_mask16(text, len, base, delim);
-    const uint32_t c = __popc(m);
+    const uint64_t base = blockIdx.x * TEXT_TILE + threadIdx.x * (16ull * TEXT_VEC);
+    uint32_t m[TEXT_VEC];
+    delim_masks(text, len, base, delim, m);
+    uint32_t c = 0;
+#pragma unroll
+    for (int q = 0; q < TEXT_VEC; ++q) c += __popc(m[q]);
     uint32_t v = c;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -794,18 +813,22 @@ __global__ void __launch_bounds__(TEXT_THREADS)
     uint32_t before = 0;
     for (uint32_t q = 0; q < w; ++q) before += warp_sums[q];
     uint64_t r = (uint64_t)tile_base[blockIdx.x] + before + v - c;
-    while (m) {
-        const int b = __ffs(m) - 1;
-        m &= m - 1;
-        const uint64_t i = base + b;
-        if (r + 1 < n) {
-            if (off_width == 8)
-                static_cast<uint64_t *>(offs)[r + 1] = i + 1;
-            else
-                static_cast<uint32_t *>(offs)[r + 1] = (uint32_t)(i + 1);
+#pragma unroll
+    for (int q = 0; q < TEXT_VEC; ++q) {
+        uint32_t mq = m[q];
+        while (mq) {
+            const int b = __ffs(mq) - 1;
+            mq &= mq - 1;
+            const uint64_t i = base + 16 * q + b;
+            if (r + 1 < n) {
+                if (off_width == 8)
+                    static_cast<uint64_t *>(offs)[r + 1] = i + 1;
+                else
+                    static_cast<uint32_t *>(offs)[r + 1] = (uint32_t)(i + 1);
+            }
+            if (delim) text[i] = 0;
+            ++r;
         }
-        if (delim) text[i] = 0;
-        ++r;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && n) {
         if (off_width == 8)
