@@ -93,3 +93,47 @@ def test_hundreds_of_rounds(sorter):
     assert np.array_equal(l, rl)
     assert int(l.max()) >= 4000
     assert sorter.stats().rounds > 200
+
+
+def _deep_families(seed):
+    """Small groups whose runs need many 16-byte steps, each family behind
+    its own first byte; the last string is an unterminated copy of the one
+    before it, running to the end of the arena."""
+    rng = np.random.default_rng(seed)
+
+    def rand(n, a=2):
+        return bytes(rng.integers(97, 97 + a, size=n, dtype=np.uint8))
+    s = [b"A" + b"x" * 5000] * 32                      # one run of 32
+    for _ in range(3):                                   # identical pairs past 8 KB
+        t = b"B" + rand(20000)
+        s += [t, t]
+    for _ in range(4):                                   # differ in the last byte
+        t = b"C" + rand(3000)
+        s += [t + b"a", t + b"b"]
+    for _ in range(4):                                   # one a prefix of the other
+        t = b"D" + rand(2500)
+        s += [t, t + rand(int(rng.integers(1, 40)))]
+    for k in range(3, 9):                                # runs of 3..8 sharing 700 bytes
+        t = b"E" + bytes([96 + k]) + rand(700)
+        s += [t + rand(int(rng.integers(0, 300))) for _ in range(k)]
+    order = rng.permutation(len(s))
+    s = [s[int(i)] for i in order]
+    last = b"F" + rand(3000)
+    return s + [last, last]
+
+
+@pytest.mark.parametrize("deep", [1, 3, 64, 4096])
+def test_in_warp_refinement_edges(deep):
+    strings = _deep_families(90)
+    body = b"".join(x + b"\0" for x in strings[:-1]) + strings[-1]  # last one unterminated
+    arena = np.frombuffer(body, dtype=np.uint8).copy()
+    offs = np.zeros(len(strings), dtype=np.uint64)
+    offs[1:] = np.cumsum([len(x) + 1 for x in strings])[:-1]
+    rp, rl = pyoracle.oracle_sort(np.concatenate([arena, np.zeros(16, np.uint8)]), offs)
+    assert int(rl.max()) >= 20000
+    with pyssort.Sorter(0) as s:
+        s.set_param(pyssort.SSORT_PARAM_WARP1_DEEP, deep)
+        p, l = s.sort_host(arena, offs)
+        assert s.stats().warp1_deep > 0
+    assert np.array_equal(p, rp)
+    assert np.array_equal(l, rl)
