@@ -180,8 +180,8 @@ KB = 16  # key bytes per round
 # launch handles to give `roofline.traffic` per launch.  Writes that stay in
 # L2 until a later kernel evicts them are not counted here.
 TRAFFIC_PER_STRING = {
-    "count_gather": 219.8,  # random offset + key reads (>= 32-byte sectors each)
-    "gather": 80.4,         # round 0: the arena streamed in order
+    "count_gather": 120.3,  # round 1 from the kept copies, round 2 random offset + key reads
+    "gather": 95.0,         # round 0: the arena streamed in order, bytes 16..31 kept
     "count": 17.9,
     "scatter": 36.3,
     "block": 57.2,
@@ -211,8 +211,14 @@ def kernel_bytes(st, w):
     equality buckets copy idx (8) and/or write lcp (4)."""
     def sort_bytes(fresh, keyed):
         return fresh * (4 + w + KB) + keyed * (KB + 4) + (fresh + keyed) * 8
-    return {
-        "gather": (st.gather_elems - st.gather_fused) * (4 + w + KB + KB),
+    # Round 0's gather may also keep key bytes 16..31 per string (read 16 more,
+    # write 16); round 1's first level then reads those (idx 4 + 16) instead of
+    # the offset and the arena, in whichever kernel gathers that level.
+    saved = getattr(st, "window_saved", 0)
+    used = getattr(st, "window_used", 0)
+    used_by = "count_gather" if st.gather_fused else "gather"
+    out = {
+        "gather": (st.gather_elems - st.gather_fused) * (4 + w + KB + KB) + saved * 2 * KB,
         "count_gather": st.gather_fused * (4 + w + KB + KB),
         "count": (st.partitioned - st.gather_fused) * KB,
         "scatter": st.partitioned * 2 * (KB + 4),
@@ -221,6 +227,8 @@ def kernel_bytes(st, w):
         "block": sort_bytes(st.block_fresh, st.block_keyed),
         "equal": st.equal_moved * 8 + st.equal_final * 4,
     }
+    out[used_by] -= used * w
+    return out
 
 
 def intrinsic_live(lcp, n):

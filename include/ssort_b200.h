@@ -218,6 +218,13 @@ typedef struct {
                               64-bit keys could not order them (a run of more
                               than 64 equal windows) and were re-sorted with
                               the full key comparator */
+    uint64_t window_saved; /* strings whose key bytes 16..31 round 0's gather
+                              kept for round 1 (sorts of at least 2^20 strings
+                              whose arena holds >= 24 bytes per string, unless
+                              the context's previous sort sent fewer than a
+                              quarter of its strings into round 1) */
+    uint64_t window_used;  /* round-1 keys read from those copies instead of
+                              through the offset and the arena */
 } ssort_stats;
 
 int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);

@@ -167,7 +167,7 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     if (n_large && !fused_gather) {
         LAUNCH(this, "seg_tiles",
                launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));
-        LAUNCH(this, "gather", launch_gather(a, lcur, n_large, ws.tile_base, g8, st));
+        LAUNCH(this, "gather", launch_gather(a, lcur, n_large, ws.tile_base, dc, g8, st));
     }
     uint32_t levels_this_round = 0;
     while (n_large) {
@@ -186,7 +186,7 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
                                 st));
         LAUNCH(this, first ? "count_gather" : "count",
                launch_count(a, lcur, n_large, ws.tile_base, ws.spl, ws.nspl, ws.tbl, ws.cm_base,
-                            ws.cm, first, g2, st));
+                            ws.cm, dc, first, g2, st));
         SS_TRY(scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
                     ws.cm_base + n_large));
         LAUNCH(this, "scatter",
@@ -221,6 +221,8 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     stats.warp1_fresh += h_ctr->warp1_fresh;
     stats.warp1_deep += h_ctr->warp1_deep;
     stats.full_sorted += h_ctr->full_sorted;
+    stats.window_saved += h_ctr->window_saved;
+    stats.window_used += h_ctr->window_used;
     stats.warp1_keyed += h_ctr->warp1_keyed;
     stats.warp8_fresh += h_ctr->warp8_fresh;
     stats.warp8_keyed += h_ctr->warp8_keyed;
@@ -237,7 +239,22 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
                    int off_width, uint32_t n, uint32_t *d_perm, uint32_t *d_lcp,
                    const uint32_t *d_inst, uint32_t ninst) {
     SS_TRY(reserve(n));
-    return run_ws(arena_p, arena_bytes, offs_p, off_width, n, d_perm, d_lcp, d_inst, ninst);
+    // Saving key bytes 16..31 in round 0 pays where many strings share their
+    // first 16 bytes and so enter round 1: judged without a device read, by
+    // the arena's bytes per string and by the share of strings that entered
+    // round 1 in this context's previous sort (none yet: length alone).
+    key2 = nullptr;
+    if (n >= KEY2_MIN_N && arena_bytes >= (uint64_t)KEY2_MIN_BYTES_PER_STRING * n &&
+        (round1_live < 0 || round1_live >= KEY2_MIN_ROUND1_LIVE)) {
+        SS_TRY(ensure(key2_buf, (size_t)n * sizeof(ulonglong2)));
+        key2 = (ulonglong2 *)key2_buf.p;
+    }
+    const int rc =
+        run_ws(arena_p, arena_bytes, offs_p, off_width, n, d_perm, d_lcp, d_inst, ninst);
+    key2 = nullptr;
+    if (rc == SSORT_OK && n)
+        round1_live = stats.rounds >= 2 ? (double)stats.live[1] / (double)n : 0.0;
+    return rc;
 }
 
 // The round loop over an already laid-out workspace `ws`.  Every position's
@@ -266,6 +283,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.target_bucket = target_bucket;
     a.warp8_cap = warp8_cap;
     a.warp1_deep = warp1_deep;
+    a.key2 = key2;
 
     Seg *cur = ws.R, *nxt = ws.N;
     Counters *dc = ws.ctr;

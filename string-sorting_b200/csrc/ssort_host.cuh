@@ -64,6 +64,9 @@ struct ssort_ctx {
     size_t ws_n = 0;  // string capacity ws is laid out for
     ssort::DBuf arena, offs, perm, inst;  // staging for the host-buffer entry points
     ssort::DBuf aux, aux2;  // text inputs: tile counts + scan partials, sorted offsets
+    ssort::DBuf key2_buf;   // round-1 keys saved by round 0 (SortArgs::key2)
+    ulonglong2 *key2 = nullptr;  // set by run() for the sort it starts
+    double round1_live = -1.0;   // share of strings entering round 1 in the last sort
     ssort::HBuf h_offs, h_arena, h_perm;
     ssort::Counters *h_ctr = nullptr;
 

@@ -42,6 +42,9 @@ constexpr int WARP1_CAP = 32;
 constexpr int WARP8_CAP = 256;
 constexpr uint32_t WARP1_DEEP = 64;       // default in-warp refinement steps (16 bytes each)
 constexpr uint32_t WARP1_DEEP_MAX = 4096;
+constexpr uint32_t KEY2_MIN_N = 1u << 20;           // sorts that may save round-1 keys
+constexpr uint32_t KEY2_MIN_BYTES_PER_STRING = 24;  // ... when the arena has this many
+constexpr double KEY2_MIN_ROUND1_LIVE = 0.25;       // ... and the last sort's round-1 share
 constexpr int SMALL_CAP = 2048;
 constexpr int SMALL_THREADS = 256;
 constexpr int SMALL_ITEMS = SMALL_CAP / SMALL_THREADS;  // 8
@@ -86,6 +89,7 @@ struct Counters {
     uint32_t n_small2, n_small3;  // CTA-sort segments of the 2nd and 3rd size class
     unsigned long long warp1_deep;  // strings re-sorted by in-warp refinement steps
     unsigned long long full_sorted;  // strings of segments re-sorted by the full comparator
+    unsigned long long window_saved, window_used;  // key2 entries written / read
 };
 
 // The CTA-sort segment lists, one per size class (n_small, n_small2, n_small3).
@@ -109,6 +113,11 @@ struct SortArgs {
     uint32_t target_bucket;  // wanted strings per range bucket of a partition
     uint32_t warp8_cap;      // largest segment for the one-warp sort (64..WARP8_CAP)
     uint32_t warp1_deep;     // in-warp refinement steps of the one-per-lane sort
+    // Per string id, key bytes 16..31 as round 0's gather read them (it reads
+    // those sectors of the arena anyway); round 1's first partition level
+    // takes its keys from here instead of the offset and a random arena read.
+    // Null when not in use.
+    ulonglong2 *key2;
 };
 
 // ---- device workspace ---------------------------------------------------------
@@ -259,7 +268,7 @@ void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint3
                  uint32_t *partials, cudaStream_t st);
 uint32_t scan_partials_needed(uint32_t n);
 void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                   int grid, cudaStream_t st);
+                   Counters *c, int grid, cudaStream_t st);
 // from_arena / gather: first partition level of a round, whose keys the
 // count kernel gathers from the arena (the sample reads its strings there).
 void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl,
@@ -267,7 +276,7 @@ void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl
                    bool from_arena, cudaStream_t st);
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                   const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
-                  const uint32_t *cm_base, uint32_t *cm, bool gather, int grid,
+                  const uint32_t *cm_base, uint32_t *cm, Counters *c, bool gather, int grid,
                   cudaStream_t st);
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                     const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,

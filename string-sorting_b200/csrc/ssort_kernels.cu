@@ -1049,7 +1049,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t *in, 
 // ---- key gather for large segments ----------------------------------------
 __global__ void __launch_bounds__(GATHER_THREADS) k_gather(SortArgs a, const Seg *__restrict__ L,
                                                           uint32_t nL,
-                                                          const uint32_t *__restrict__ tile_base) {
+                                                          const uint32_t *__restrict__ tile_base,
+                                                          Counters *ctr) {
     constexpr int U = GATHER_ITEMS;
     static_assert(GATHER_TILE % (GATHER_THREADS * GATHER_ITEMS) == 0, "tile shape");
     const uint32_t total_tiles = tile_base[nL] * (GATHER_TILE / (GATHER_THREADS * U));
@@ -1061,6 +1062,10 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(SortArgs a, const Seg
         const uint32_t lo = (t - tile_base[si]) * GATHER_TILE + (t2 % SUBT) * GATHER_THREADS * U;
         if (lo >= s.len) continue;
         const uint32_t *I = a.idx[0];
+        // Depth 0 with a.key2: also keep key bytes 16..31 for round 1 (their
+        // sectors are read here anyway); depth 16: read those copies.
+        const bool save = a.key2 && s.depth == 0;
+        const bool saved = a.key2 && s.depth == KEY_BYTES;
         uint32_t id[U];
         uint64_t off[U];
 #pragma unroll
@@ -1070,13 +1075,25 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(SortArgs a, const Seg
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            off[u] = id[u] != IDX_MAX ? string_offset(a.offs, a.off_width, id[u]) : 0;
+            off[u] = id[u] != IDX_MAX && !saved ? string_offset(a.offs, a.off_width, id[u]) : 0;
+        uint32_t kept = 0;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t i = lo + u * GATHER_THREADS + threadIdx.x;
-            if (id[u] != IDX_MAX)
+            if (id[u] != IDX_MAX) {
                 a.key[0][s.start + i] =
-                    from_key(load_key(a.arena, a.arena_bytes, off[u] + s.depth));
+                    saved ? a.key2[id[u]]
+                          : from_key(load_key(a.arena, a.arena_bytes, off[u] + s.depth));
+                if (save)
+                    a.key2[id[u]] =
+                        from_key(load_key(a.arena, a.arena_bytes, off[u] + KEY_BYTES));
+                ++kept;
+            }
+        }
+        if (save || saved) {
+            const unsigned long long k = warp_sum((unsigned long long)kept);
+            if ((threadIdx.x & 31) == 0 && k)
+                atomicAdd(save ? &ctr->window_saved : &ctr->window_used, k);
         }
     }
 }
@@ -1318,7 +1335,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
                                                         const uint32_t *__restrict__ nspl,
                                                         const uint16_t *__restrict__ tbl,
                                                         const uint32_t *__restrict__ cm_base,
-                                                        uint32_t *cm) {
+                                                        uint32_t *cm, Counters *cnt_ctr) {
     extern __shared__ __align__(16) unsigned char part_smem[];
     PartSmem &sm = *reinterpret_cast<PartSmem *>(part_smem);
     auto &hist = sm.cnt;
@@ -1349,20 +1366,39 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
             // round-start segments live in buffer 0
             const uint32_t *I = a.idx[0] + s.start;
             ulonglong2 *KW = a.key[0] + s.start;
-            uint64_t off[PART_ITEMS];
+            if (a.key2 && s.depth == KEY_BYTES) {
+                // round 1: the keys round 0's gather kept, by string id
+                uint32_t got = 0;
 #pragma unroll
-            for (int c = 0; c < PART_ITEMS; ++c) {
-                const uint32_t e = lo + c * 32 + lane;
-                off[c] = e < s.len ? string_offset(a.offs, a.off_width, I[e]) + s.depth : 0;
-            }
+                for (int c = 0; c < PART_ITEMS; ++c) {
+                    const uint32_t e = lo + c * 32 + lane;
+                    if (e < s.len) {
+                        const ulonglong2 k2 = a.key2[I[e]];
+                        kk[c] = to_key(k2);
+                        KW[e] = k2;
+                        ++got;
+                    } else {
+                        kk[c] = key_max();
+                    }
+                }
+                const unsigned long long g = warp_sum((unsigned long long)got);
+                if (lane == 0 && g) atomicAdd(&cnt_ctr->window_used, g);
+            } else {
+                uint64_t off[PART_ITEMS];
 #pragma unroll
-            for (int c = 0; c < PART_ITEMS; ++c) {
-                const uint32_t e = lo + c * 32 + lane;
-                if (e < s.len) {
-                    kk[c] = load_key(a.arena, a.arena_bytes, off[c]);
-                    KW[e] = from_key(kk[c]);
-                } else {
-                    kk[c] = key_max();
+                for (int c = 0; c < PART_ITEMS; ++c) {
+                    const uint32_t e = lo + c * 32 + lane;
+                    off[c] = e < s.len ? string_offset(a.offs, a.off_width, I[e]) + s.depth : 0;
+                }
+#pragma unroll
+                for (int c = 0; c < PART_ITEMS; ++c) {
+                    const uint32_t e = lo + c * 32 + lane;
+                    if (e < s.len) {
+                        kk[c] = load_key(a.arena, a.arena_bytes, off[c]);
+                        KW[e] = from_key(kk[c]);
+                    } else {
+                        kk[c] = key_max();
+                    }
                 }
             }
         } else {
@@ -2441,9 +2477,9 @@ void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint3
 }
 
 void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
-                   int grid, cudaStream_t st) {
+                   Counters *c, int grid, cudaStream_t st) {
     if (!nL) return;
-    k_gather<<<grid, GATHER_THREADS, 0, st>>>(a, L, nL, tile_base);
+    k_gather<<<grid, GATHER_THREADS, 0, st>>>(a, L, nL, tile_base, c);
 }
 
 void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl, uint32_t *nspl,
@@ -2457,15 +2493,16 @@ void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl
 
 void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
                   const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
-                  const uint32_t *cm_base, uint32_t *cm, bool gather, int grid, cudaStream_t st) {
+                  const uint32_t *cm_base, uint32_t *cm, Counters *c, bool gather, int grid,
+                  cudaStream_t st) {
     if (!nL) return;
     set_smem_attrs();
     if (gather)
         k_count<true><<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl,
-                                                                    tbl, cm_base, cm);
+                                                                    tbl, cm_base, cm, c);
     else
         k_count<false><<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl,
-                                                                     nspl, tbl, cm_base, cm);
+                                                                     nspl, tbl, cm_base, cm, c);
 }
 
 void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,

@@ -68,6 +68,8 @@ class Stats(ctypes.Structure):
         ("gather_fused", ctypes.c_uint64),
         ("warp1_deep", ctypes.c_uint64),
         ("full_sorted", ctypes.c_uint64),
+        ("window_saved", ctypes.c_uint64),
+        ("window_used", ctypes.c_uint64),
     ]
 
     def as_dict(self):

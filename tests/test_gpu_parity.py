@@ -159,3 +159,51 @@ def test_tied_packed_windows(sorter, n, lead, alpha, full):
     ref_perm, ref_lcp = pyoracle.oracle_sort(arena, offs)
     assert np.array_equal(perm, ref_perm) and np.array_equal(lcp, ref_lcp)
     assert (sorter.stats().full_sorted > 0) == full
+
+
+def test_saved_round1_keys():
+    """URLs (54 bytes per string): round 0's gather keeps every string's key
+    bytes 16..31 and round 1 reads them instead of the arena; short strings
+    (about 11 bytes each) keep none, and a sort right after a sort that sent
+    few strings into round 1 keeps none either, the one after it does again.
+    Results are the oracle's every time."""
+    ss = pyssort.gen_urls(2_000_000, seed=48)
+    rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+    short = pyssort.gen_uniform(2_000_000, 1, 20, ord("a"), 26, 49)
+    with pyssort.Sorter(0) as s:
+        perm, lcp = s.sort_host(ss.arena, ss.offs)
+        st = s.stats()
+        assert st.window_saved == ss.n and st.window_used > 0
+        assert np.array_equal(perm, rp) and np.array_equal(lcp, rl)
+        s.sort_host(short.arena, short.offs)
+        assert s.stats().window_saved == 0
+        for saved in (0, ss.n):
+            perm, lcp = s.sort_host(ss.arena, ss.offs)
+            assert s.stats().window_saved == saved
+            assert np.array_equal(perm, rp) and np.array_equal(lcp, rl)
+
+
+def test_saved_round1_keys_batched():
+    """A batched call of URL instances, small (sorted on chip in round 0) and
+    large (gathered in round 0, keys kept for round 1): every instance is the
+    oracle's sort of it alone."""
+    sizes = [3000, 1500, 700_000, 2000, 400_000, 10, 2049]
+    sets = [pyssort.gen_urls(m, seed=500 + k) for k, m in enumerate(sizes)]
+    parts, offs, base = [], [], 0
+    for st in sets:
+        parts.append(st.arena[:st.text_bytes])
+        offs.append(st.offs + np.uint64(base))
+        base += st.text_bytes
+    arena = np.concatenate(parts + [np.zeros(16, np.uint8)])
+    offs = np.concatenate(offs)
+    inst = np.zeros(len(sizes) + 1, dtype=np.uint32)
+    inst[1:] = np.cumsum(sizes)
+    with pyssort.Sorter(0) as s:
+        p, l = s.sort_batch_host(arena, offs, inst)
+        st = s.stats()
+    assert st.window_saved == sum(m for m in sizes if m > 2048) and st.window_used > 0
+    for k in range(len(sizes)):
+        lo, hi = int(inst[k]), int(inst[k + 1])
+        rp, rl = pyoracle.oracle_sort(arena, offs[lo:hi])
+        assert np.array_equal(p[lo:hi], rp), k
+        assert np.array_equal(l[lo:hi], rl), k
