@@ -240,7 +240,7 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
                    const uint32_t *d_inst, uint32_t ninst) {
     SS_TRY(reserve(n));
     // Saving key bytes 16..31 in round 0 pays where many strings share their
-    // first 16 bytes and so enter round 1: judged without a device read, by
+    // first 16 bytes and so enter round 1: decided without a device read, by
     // the arena's bytes per string and by the share of strings that entered
     // round 1 in this context's previous sort (none yet: length alone).
     key2 = nullptr;
