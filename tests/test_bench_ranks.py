@@ -84,3 +84,24 @@ def test_text_workload_cpu_sample():
     assert ss.offs.dtype == np.uint64 and list(ss.offs[:3]) == [0, 1, 2]
     t, kind = bench.time_cpu_sort(ss, 5000)
     assert t > 0 and kind in ("reference", "port")
+
+
+def test_kernel_bytes_with_kept_windows():
+    """Algorithmic bytes of the gathering kernels: round 0's gather reads and
+    writes 16 more bytes per kept window; a key read from a kept copy skips
+    the offset (W bytes), in whichever kernel gathers round 1's first level."""
+    from types import SimpleNamespace as NS
+    base = dict(gather_elems=150, gather_fused=50, partitioned=300, warp1_fresh=0,
+                warp1_keyed=0, warp8_fresh=0, warp8_keyed=0, block_fresh=0, block_keyed=0,
+                equal_moved=0, equal_final=0)
+    w = 8
+    plain = bench.kernel_bytes(NS(**base, window_saved=0, window_used=0), w)
+    assert plain["gather"] == 100 * (4 + w + 32)
+    assert plain["count_gather"] == 50 * (4 + w + 32)
+    kept = bench.kernel_bytes(NS(**base, window_saved=100, window_used=40), w)
+    assert kept["gather"] == plain["gather"] + 100 * 32
+    assert kept["count_gather"] == plain["count_gather"] - 40 * w
+    base["gather_fused"] = 0  # separate gather in every round: it reads the copies
+    sep = bench.kernel_bytes(NS(**base, window_saved=100, window_used=40), w)
+    assert sep["gather"] == 150 * (4 + w + 32) + 100 * 32 - 40 * w
+    assert sep["count_gather"] == 0
