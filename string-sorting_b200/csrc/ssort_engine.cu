@@ -243,12 +243,13 @@ int ssort_ctx::run(const uint8_t *arena_p, uint64_t arena_bytes, const void *off
     // first 16 bytes and so enter round 1: decided without a device read, by
     // the arena's bytes per string and by the share of strings that entered
     // round 1 in this context's previous sort (none yet: length alone).
+    // The copies are an optimisation: without device memory for them the sort
+    // goes ahead without (the workspace itself was reserved first).
     key2 = nullptr;
     if (n >= KEY2_MIN_N && arena_bytes >= (uint64_t)KEY2_MIN_BYTES_PER_STRING * n &&
-        (round1_live < 0 || round1_live >= KEY2_MIN_ROUND1_LIVE)) {
-        SS_TRY(ensure(key2_buf, (size_t)n * sizeof(ulonglong2)));
+        (round1_live < 0 || round1_live >= KEY2_MIN_ROUND1_LIVE) &&
+        ensure(key2_buf, (size_t)n * sizeof(ulonglong2)) == SSORT_OK)
         key2 = (ulonglong2 *)key2_buf.p;
-    }
     const int rc =
         run_ws(arena_p, arena_bytes, offs_p, off_width, n, d_perm, d_lcp, d_inst, ninst);
     key2 = nullptr;
