@@ -84,3 +84,31 @@ def test_null_server_is_rejected():
     L.ssort_server_destroy(None)
     out = ctypes.c_void_p()
     assert L.ssort_server_create(0, 1 << 20, 0, ctypes.byref(out)) == -1
+
+
+@pytest.mark.parametrize("cname,pyname", [("ssort_stats", "Stats"),
+                                          ("ssort_server_info", "ServerInfo"),
+                                          ("ssort_tuning", "Tuning")])
+def test_ctypes_structs_match_header_layout(tmp_path, cname, pyname):
+    """The ctypes mirrors of the header's result structs: same size and the
+    same offset for every field, as the C compiler lays them out."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    cls = getattr(pyssort, pyname)
+    fields = [f for f, _ in cls._fields_]
+    src = tmp_path / "layout.c"
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "ssort_b200.h"',
+             "int main(void) {", f'    printf("%zu\\n", sizeof({cname}));']
+    lines += [f'    printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+    lines += ["    return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(cls)
+    assert got[1:] == [getattr(cls, f).offset for f in fields]
