@@ -105,3 +105,16 @@ def test_autotune_then_sort_stays_exact():
         rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
         assert np.array_equal(d_perm.cpu().numpy().view(np.uint32), rp)
         assert np.array_equal(d_lcp.cpu().numpy().view(np.uint32), rl)
+
+
+def test_kept_keys_with_separate_gather():
+    """With the fused gather off, round 1's separate gather reads the key
+    copies round 0 kept (2 M URLs: above the size where copies are kept)."""
+    ss = pyssort.gen_urls(2_000_000, seed=63)
+    rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+    with pyssort.Sorter(0) as s:
+        s.set_param(pyssort.SSORT_PARAM_FUSED_GATHER, 0)
+        p, l = s.sort_host(ss.arena, ss.offs)
+        st = s.stats()
+    assert st.gather_fused == 0 and st.window_saved > 0 and st.window_used > 0
+    assert np.array_equal(p, rp) and np.array_equal(l, rl)
