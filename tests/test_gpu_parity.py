@@ -207,3 +207,13 @@ def test_saved_round1_keys_batched():
         rp, rl = pyoracle.oracle_sort(arena, offs[lo:hi])
         assert np.array_equal(p[lo:hi], rp), k
         assert np.array_equal(l[lo:hi], rl), k
+
+
+def test_saved_round1_keys_u32_offsets():
+    """Kept round-1 keys with 4-byte offsets (the width whole-text sorts use)."""
+    ss = pyssort.gen_urls(1_500_000, seed=51)
+    rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+    with pyssort.Sorter(0) as s:
+        p, l = s.sort_host(ss.arena, ss.offs.astype(np.uint32))
+        assert s.stats().window_saved == ss.n
+    assert np.array_equal(p, rp) and np.array_equal(l, rl)
