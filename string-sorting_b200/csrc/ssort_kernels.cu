@@ -1722,15 +1722,17 @@ __device__ __forceinline__ void warp1_pairs(const uint8_t *__restrict__ arena,
 }
 
 // In-warp refinement of the runs a one-per-lane sort left (lanes with `run`,
-// h = the run's first lane, keys equal up to `depth`, id = the lane's record):
-// the members load their next 16 bytes, each run is re-sorted inside its own
-// lanes, the LCPs decided at this depth are written, and the runs of equal
-// keys that remain become the next step's runs; at most `steps` steps, then
-// what is left goes to the next round.  This is the next round's one-warp sort
-// of those runs done without a round trip: the same order and LCPs.  The keys
-// of the segment's first and last position, which the round's boundary pass
-// reads, stay as the first sort wrote them.  Returns the strings this lane
-// re-sorted.  Warp-collective.
+// h = the run's first lane, keys equal up to `depth`, id = the lane's record).
+// Each step first resolves the runs of two with the whole warp (warp1_pairs);
+// then the members of the other runs load their next 16 bytes, each run is
+// re-sorted inside its own lanes, the LCPs decided at this depth are written,
+// and the runs of equal keys that remain become the next step's runs.  At
+// most `steps` steps, then what is left goes to the next round.  This is the
+// next round's one-warp sort of those runs done without a round trip: the
+// same order and LCPs.  The keys of the segment's first and last position,
+// which the round's boundary pass reads, stay as the first sort wrote them.
+// Returns this lane's count of string steps (for the statistics).
+// Warp-collective.
 template <int W>
 __device__ __forceinline__ uint32_t warp1_deepen(const uint8_t *__restrict__ arena,
                                               uint64_t arena_bytes, const void *__restrict__ offs,
