@@ -34,6 +34,12 @@ import numpy as np  # noqa: E402
 import pyssort  # noqa: E402
 
 METRIC = "sort throughput (strings/s)"
+# Wall-clock bound of the reference arm's timed steps (seconds): a full-size
+# CPU sort of the 50 M URLs takes about 14 s on one core.
+REF_BUDGET_S = 300.0
+# Most distinct requests one serving sweep generates up front (about 17 MB of
+# keys each on average, held in pinned host memory and in HBM).
+SERVE_FRESH_CAP = 1200
 UNIT = "strings/s"
 DEFAULT_WORKLOAD = "urls_50m"
 CPU_SAMPLE = {"urls_50m": 4_000_000, "zipf_words_100m": 8_000_000, "uniform_1m": 1_000_000,
@@ -74,6 +80,8 @@ def parse():
     ap.add_argument("--autotune", action="store_true",
                     help="run ssort_autotune on the input before timing (reported in `tuning`)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations measured beside the default one")
     ap.add_argument("--warp1-deep", type=int, default=None,
                     help="in-warp refinement steps of the one-per-lane sort (library default "
                          "when absent)")
@@ -83,7 +91,9 @@ def parse():
                     help="requests per arrival rate of the serve_c5 sweep")
     ap.add_argument("--serve-rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--serve-pool", type=int, default=64,
-                    help="distinct requests the serve_c5 stream draws from")
+                    help="distinct requests the serve_c5 stream draws from (without --serve-fresh)")
+    ap.add_argument("--serve-fresh", action="store_true",
+                    help="every request of the sweep is a distinct, newly generated one")
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--serve-max-strings", type=int, default=1 << 27)
     ap.add_argument("--scale", type=float, default=1.0,
@@ -179,6 +189,7 @@ KB = 16  # key bytes per round
 # and divided by the strings the kernel handled); scaled by the strings a
 # launch handles to give `roofline.traffic` per launch.  Writes that stay in
 # L2 until a later kernel evicts them are not counted here.
+TRAFFIC_WORKLOAD = "urls_50m"
 TRAFFIC_PER_STRING = {
     "count_gather": 120.3,  # round 1 from the kept copies, round 2 random offset + key reads
     "gather": 95.0,         # round 0: the arena streamed in order, bytes 16..31 kept
@@ -361,6 +372,10 @@ def run_ours(args, rank, world, local_rank, dist):
                "with_lcp": {"value": job_rate(n, args.steps, world, e2e_lcp_s),
                             "d2h_bytes_per_step": int(n * 8),
                             "ms_per_step": 1000 * e2e_lcp_s / args.steps}}
+        del h_arena, h_offs, h_perm, h_lcp
+        dropin = time_dropin(ss, n, max(1, min(args.steps, 5))) if world == 1 else None
+        if dropin is not None:
+            e2e["dropin"] = dropin
     clocks.stop()
 
     if rank != 0:
@@ -386,7 +401,8 @@ def run_ours(args, rank, world, local_rank, dist):
         per_launch_s = d["ms_total"] / 1e3 / d["launches"]
         ach = per_launch_bytes / per_launch_s / 1e9
         traffic = None
-        if dom in TRAFFIC_PER_STRING:
+        # measured DRAM bytes exist only for the URL workload's kernels
+        if dom in TRAFFIC_PER_STRING and args.workload == TRAFFIC_WORKLOAD:
             strings_per_launch = kernel_strings(st)[dom] * args.steps / d["launches"]
             traffic = int(TRAFFIC_PER_STRING[dom] * strings_per_launch)
         roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
@@ -648,6 +664,13 @@ def run_batch(args):
     time.sleep(0.3)
     ms_b = timed(batched, args.steps)
     st = sorter.stats()
+    # launches of one batched call (the scan is three kernels per launch)
+    sorter.set_profiling(True)
+    batched()
+    torch.cuda.synchronize()
+    kt = sorter.kernel_times()
+    sorter.set_profiling(False)
+    launches_per_call = int(sum(v[1] * (3 if k == "scan" else 1) for k, v in kt.items()))
     plain()
     ms_p = timed(plain, max(1, min(args.steps, 3)))
     clocks.stop()
@@ -662,7 +685,7 @@ def run_batch(args):
         "key_gbs": round(ss.text_bytes / (ms_b / 1e3) / 1e9, 2),
         "plain": {"value": n / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p,
                   "calls_per_step": k},
-        "batched_vs_plain": round(ms_p / ms_b, 2),
+        "batched_vs_plain": round(ms_p / ms_b, 2), "launches_per_call": launches_per_call,
         "clocks": clocks.summary(), "stats": st.as_dict(),
     }
 
@@ -817,14 +840,20 @@ def run_serve(args):
     import torch
     torch.cuda.set_device(0)
     rates = [float(r) for r in args.serve_rates.split(",") if r]
-    pool = RequestPool(args.serve_pool)
+    # Fresh requests: every request of every rate's stream is a distinct,
+    # newly generated one (up to SERVE_FRESH_CAP in all, a host- and
+    # device-memory bound); otherwise the streams draw from a pool.
+    fresh = getattr(args, "serve_fresh", False)
+    need = args.serve_requests * len(rates)
+    pool = RequestPool(min(need, SERVE_FRESH_CAP) if fresh else args.serve_pool)
+    fresh = fresh and len(pool.reqs) >= need
     pool.to_device()
     budget = int(args.serve_budget_gb * 1e9)
     srv = pyssort.Server(budget, args.serve_max_strings)
     sorter = pyssort.Sorter(0)
-    # warm-up: every pool request once through each path, largest first so
-    # that the plain context's buffers reach their final size
-    order = np.array(sorted(range(len(pool.reqs)), key=lambda k: -pool.reqs[k]["m"]))
+    # warm-up: the largest pool requests once through each path, largest
+    # first so that the plain context's buffers reach their final size
+    order = np.array(sorted(range(len(pool.reqs)), key=lambda k: -pool.reqs[k]["m"])[:64])
     w_arr = np.zeros(len(order))
     for _ in range(max(1, args.warmup)):
         for resident in (False, True):
@@ -838,6 +867,8 @@ def run_serve(args):
         rows = []
         for i, rate in enumerate(rates):
             arr, picks = _arrivals(args.serve_requests, rate, len(pool.reqs), 100 + i)
+            if fresh:  # distinct requests, none replayed
+                picks = np.arange(i * args.serve_requests, (i + 1) * args.serve_requests)
             served = serve_stream(srv, pool, arr, picks, resident)
             plain = plain_stream(sorter, pool, arr, picks, resident)
             rows.append({"rate_req_s": rate, "served": served, "plain": plain,
@@ -858,6 +889,7 @@ def run_serve(args):
         "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
         "config": {"workload": "serve_c5", "description": DESCRIPTIONS["serve_c5"],
                    "requests_per_rate": args.serve_requests, "pool_requests": len(pool.reqs),
+                   "fresh_requests": bool(fresh),
                    "pool_strings": pool.n, "pool_key_bytes": pool.key_bytes,
                    "arena_budget_bytes": budget, "max_strings": args.serve_max_strings,
                    "parallelism": "single",
@@ -887,6 +919,31 @@ def _port_lib():
     return L
 
 
+def time_dropin(ss, n, steps):
+    """The drop-in as the reference's own driver calls it: msd_gpu(strings, n)
+    through r->f of the reference's routine registry (sortstring's run(),
+    src/sortstring.c:424-451), on a pointer array into the workload's arena
+    in ordinary (pageable) host memory.  The pointer array is built outside
+    the timed call, as sortstring builds it while reading its input.  One
+    untimed call first (the routine's context and staging buffers)."""
+    p = os.path.join(ROOT, "oracle", "_ref", "libref_dropin.so")
+    if not os.path.exists(p):
+        return None
+    L = ctypes.CDLL(p)
+    L.ref_time_sort.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_size_t]
+    L.ref_time_sort.restype = ctypes.c_double
+    if L.ref_time_sort(b"msd_gpu", ss.arena.ctypes.data, ss.offs.ctypes.data, n) < 0:
+        return None
+    ts = [L.ref_time_sort(b"msd_gpu", ss.arena.ctypes.data, ss.offs.ctypes.data, n)
+          for _ in range(steps)]
+    t = statistics.median(ts)
+    return {"value": n / t, "unit": UNIT, "ms_per_step": round(1000 * t, 3), "steps": steps,
+            "api": "msd_gpu(unsigned char **, size_t) through the reference registry's r->f",
+            "h2d_bytes_per_step": int(ss.text_bytes + n * (4 if ss.text_bytes < 2**32 else 8)),
+            "d2h_bytes_per_step": int(n * 4)}
+
+
 def time_cpu_sort(ss, m):
     """Seconds for one sort of the first m strings: the reference's msd_CE6
     timed around its routine call, or the oracle port when the reference
@@ -904,9 +961,9 @@ def time_cpu_sort(ss, m):
     return time.perf_counter() - t0, "port"
 
 
-def instance_sample(workload, budget):
-    """The first instances of the batched or served workload's list, up to
-    about `budget` strings (the reference arm's bounded sample)."""
+def instance_params(workload, budget):
+    """(params, seed) of the first instances of the batched or served
+    workload's list, up to about `budget` strings (a bounded sample)."""
     if workload == "batch_c4":
         params = pyssort.batch_instance_params(20000, 5, key_byte_limit=1.5e9)
         seed = 4
@@ -919,6 +976,11 @@ def instance_sample(workload, budget):
             break
         take.append(p)
         total += p[0]
+    return take, seed
+
+
+def instance_sample(workload, budget):
+    take, seed = instance_params(workload, budget)
     return pyssort.gen_instances(take, seed=seed)
 
 
@@ -946,7 +1008,109 @@ def time_cpu_instances(ss):
     return total, kind
 
 
-def cpu_baseline(workload, ss, reps=3):
+# ---- all host cores on independent instances (separate processes) -----------------
+_worker_ss = None
+
+
+def _instances_worker_init(params, seed):
+    """Each worker process generates the same instance list (seeded) once."""
+    global _worker_ss
+    sys.path.insert(0, os.path.join(ROOT, "string-sorting_b200"))
+    import pyssort as _p
+    _worker_ss = _p.gen_instances(params, seed=seed)
+
+
+def _instances_worker_sort(ids):
+    """Wall seconds for sorting instances `ids` of the worker's list with
+    msd_CE6 one after another (the pointer arrays are built outside)."""
+    L = _ref_lib()
+    ss = _worker_ss
+    total = 0.0
+    for i in ids:
+        lo, hi = int(ss.inst_start[i]), int(ss.inst_start[i + 1])
+        if hi - lo >= 2:
+            t = L.ref_time_sort(b"msd_CE6", ss.arena.ctypes.data, ss.offs.ctypes.data + 8 * lo,
+                                hi - lo)
+            if t < 0:
+                raise RuntimeError("reference sort failed")
+            total += t
+    return total
+
+
+class AllCoreInstances:
+    """msd_CE6 on independent instances across every host core, one process
+    per core (msd_CE3..CE8 keep function-static bucket arrays, so they are not
+    reentrant and cannot share a process, src/msd_ce.cpp:392).  The instances
+    are dealt to the workers largest first; a step's time is the slowest
+    worker's.  Spawned processes: safe after the parent has used the GPU."""
+
+    def __init__(self, params, seed, procs=None):
+        import multiprocessing as mp
+        self.procs = procs or os.cpu_count() or 1
+        self.counts = [p[0] for p in params]
+        order = sorted(range(len(params)), key=lambda i: -params[i][0])
+        load = [0] * self.procs
+        self.assign = [[] for _ in range(self.procs)]
+        for i in order:
+            k = min(range(self.procs), key=lambda j: load[j])
+            self.assign[k].append(i)
+            load[k] += params[i][0]
+        self.pool = mp.get_context("spawn").Pool(self.procs, _instances_worker_init,
+                                                 (params, seed))
+
+    def step(self):
+        return max(self.pool.map(_instances_worker_sort, self.assign, chunksize=1))
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+# The reference's CPU routines timed beside the GPU sort (name, cores used,
+# note).  msd_CE6 is the oracle; msd_CE7/CE8 share a sortedness shortcut that
+# mis-sorts segments of >= 65,536 strings whose 2-byte keys are non-increasing
+# but not all equal (src/msd_ce.cpp:452,529), so CE8 is timed but flagged.
+CPU_ROUTINES = (
+    ("msd_CE6", "stable MSD radix sort, 16-bit digits for >= 65,536 strings "
+                "(src/msd_ce.cpp:367-419); the oracle"),
+    ("msd_CE2", "stable MSD radix sort, 8-bit digits, reentrant (src/msd_ce.cpp:143-178)"),
+    ("multikey_cache8", "multikey quicksort with an 8-byte cache (src/multikey_cache.cpp:231-238)"),
+    ("multikey_cache4", "multikey quicksort with a 4-byte cache (src/multikey_cache.cpp:231-238)"),
+    ("burstsort_vector", "burstsort with vector buckets (src/burstsort.cpp:290-299)"),
+    ("msd_CE8", "FLAGGED: mis-sorts non-increasing 2-byte keys in segments >= 65,536 "
+                "(src/msd_ce.cpp:529); timed only"),
+    ("parallel_msd_radix_sort", "multicore MSD radix sort (external/"
+                                "parallel_string_radix_sort.cpp), OpenMP over all host threads"),
+)
+
+
+def cpu_routines(ss, m, reps=5):
+    """Every routine of CPU_ROUTINES on the first m strings of ss, median of
+    `reps` runs each (fresh pointer array per run), through the reference's
+    own routine registry.  None when the reference library is absent."""
+    L = _ref_lib()
+    if L is None:
+        return None
+    out = {}
+    for name, note in CPU_ROUTINES:
+        ts = []
+        for _ in range(reps):
+            t = L.ref_time_sort(name.encode(), ss.arena.ctypes.data, ss.offs.ctypes.data, m)
+            if t < 0:
+                ts = None
+                break
+            ts.append(t)
+        if not ts:
+            out[name] = {"unavailable": "not registered in the reference library"}
+            continue
+        t = statistics.median(ts)
+        cores = os.cpu_count() if name == "parallel_msd_radix_sort" else 1
+        out[name] = {"value": m / t, "unit": UNIT, "seconds_median": round(t, 4),
+                     "runs": reps, "cores": cores, "note": note}
+    return out
+
+
+def cpu_baseline(workload, ss, reps=5):
     m = min(ss.n, CPU_SAMPLE.get(workload, 2_000_000))
     if isinstance(ss, TextSample):
         ss.first(m)
@@ -956,23 +1120,131 @@ def cpu_baseline(workload, ss, reps=3):
         t, kind = time_cpu_sort(ss, m)
         ts.append(t)
     t = statistics.median(ts)
-    return {"value": m / t, "unit": UNIT, "cores": 1, "kind": kind,
-            "routine": "msd_CE6" if kind == "reference" else "oracle port of msd_CE6",
-            "sample": f"first {m:,} strings of {workload}, median of {reps} runs "
-                      f"({t:.3f} s each), single thread",
-            "host": {"cpu": cpu_model(), "nproc": os.cpu_count()}}
+    out = {"value": m / t, "unit": UNIT, "cores": 1, "kind": kind,
+           "routine": "msd_CE6" if kind == "reference" else "oracle port of msd_CE6",
+           "sample": f"first {m:,} strings of {workload}, median of {reps} runs "
+                     f"({t:.3f} s each), single thread",
+           "host": {"cpu": cpu_model(), "nproc": os.cpu_count()}}
+    if kind == "reference":
+        out["routines"] = cpu_routines(ss, m, reps)
+    return out
+
+
+
+# ---- the other configurations, measured in the same run ---------------------------
+def plain_config_summary(workload, steps, warmup, no_cpu):
+    """One more plain configuration measured beside the headline: strings/s
+    from device-resident inputs (CUDA events on the sort's stream), the
+    whole-sort roofline, the dominant kernel's roofline from a profiled pass,
+    and msd_CE6 on a bounded sample of the same strings."""
+    import torch
+    ss = pyssort.WORKLOADS[workload]()
+    n, w, ab = ss.n, ss.offs.dtype.itemsize, ss.arena.nbytes
+    d_arena = torch.from_numpy(ss.arena).cuda()
+    d_offs = torch.from_numpy(ss.offs.view(np.int64)).cuda()
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_lcp = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    with pyssort.Sorter(0) as sorter:
+        def step():
+            sorter.sort_device(d_arena, ab, d_offs, w, n, d_perm, d_lcp,
+                               stream=stream.cuda_stream)
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        sorter.set_profiling(True)
+        for _ in range(steps):
+            step()
+        torch.cuda.synchronize()
+        ktimes = sorter.kernel_times()
+        sorter.set_profiling(False)
+        st = sorter.stats()
+    peak, peak_kind = peaks()
+    kb = kernel_bytes(st, w)
+    dom = max((k for k in ktimes if k in kb), key=lambda k: ktimes[k][0], default=None)
+    roof = None
+    if dom:
+        kms, launches = ktimes[dom]
+        ach = kb[dom] * steps / (kms / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
+                "launch_ms": round(kms / launches, 4)}
+    live8 = intrinsic_live(d_lcp.cpu().numpy().view(np.uint32), n)
+    sb = sort_algorithmic_bytes(live8, n, w)
+    out = {"workload": workload, "description": DESCRIPTIONS[workload], "n_strings": n,
+           "value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": round(ms, 4), "steps": steps,
+           "warmup": warmup, "key_gbs": round(ss.text_bytes / (ms / 1e3) / 1e9, 2),
+           "sort_roofline": {"algorithmic_bytes_per_sort": int(sb),
+                             "achieved": round(sb / (ms / 1e3) / 1e9, 1), "peak": peak,
+                             "frac": round(sb / (ms / 1e3) / 1e9 / peak, 4),
+                             "frac_of_8tbs": round(sb / (ms / 1e3) / 1e9 / 8000, 4),
+                             "live_per_8byte_round": live8[:8]},
+           "roofline": roof,
+           "kernels_ms_per_step": {k: round(v[0] / steps, 4) for k, v in sorted(
+               ktimes.items(), key=lambda kv: -kv[1][0])[:8]},
+           "stats": {k: st.as_dict()[k] for k in ("rounds", "partition_levels", "partitioned")}}
+    if not no_cpu:
+        out["cpu_baseline"] = cpu_baseline(workload, ss, reps=3)
+    del d_arena, d_offs, d_perm, d_lcp
+    torch.cuda.empty_cache()
+    return out
+
+
+def extra_configs(args):
+    """The other configurations of the benchmark, each measured briefly in the
+    default run so that one invocation reports all of them: the uniform 1 M
+    and Zipf-words 100 M plain sorts, the batched-vs-plain ratio on the
+    batched workload, and a two-rate serving sweep with latency percentiles."""
+    import argparse as _ap
+    import torch
+    out = {}
+    for wl in ("zipf_words_100m", "uniform_1m"):
+        out[wl] = plain_config_summary(wl, 5, 3, args.no_cpu)
+    b = run_batch(_ap.Namespace(scale=1.0, warmup=2, steps=3))
+    out["batch_c4"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "plain",
+                                         "batched_vs_plain", "config", "launches_per_call")
+                       if k in b}
+    torch.cuda.empty_cache()
+    sv = run_serve(_ap.Namespace(serve_rates="1000,20000", serve_pool=args.serve_pool,
+                                 serve_requests=300, serve_budget_gb=args.serve_budget_gb,
+                                 serve_max_strings=args.serve_max_strings, warmup=1,
+                                 serve_fresh=True))
+    out["serve_c5"] = {k: sv[k] for k in ("value", "unit", "config", "sweep_resident",
+                                          "sweep_host") if k in sv}
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_reference(args, rank):
     if rank != 0:
         return None
+    warm = None
+    cores = 1
+    pool = None
+    same = False
     if args.workload in ("batch_c4", "serve_c5"):
-        # independent instances, sorted one after another on one core
-        ss = instance_sample(args.workload, 2_000_000)
+        # independent instances, each sorted alone by msd_CE6, spread over
+        # every host core (one process per core)
+        params, seed = instance_params(args.workload, 16_000_000)
+        ss = pyssort.gen_instances(params, seed=seed)
         m = ss.n
-        sample = (f"the first {len(ss.inst_start) - 1} instances ({m:,} strings) of the "
-                  f"{args.workload} list per step, each sorted alone")
-        timer = lambda: time_cpu_instances(ss)  # noqa: E731
+        kind0 = "reference" if _ref_lib() is not None else "port"
+        if kind0 == "reference":
+            pool = AllCoreInstances(params, seed)
+            cores = pool.procs
+            timer = lambda: (pool.step(), "reference")  # noqa: E731
+        else:
+            timer = lambda: time_cpu_instances(ss)  # noqa: E731
+        sample = (f"the first {len(params)} instances ({m:,} strings) of the {args.workload} "
+                  f"list per step, each sorted alone, on {cores} host cores (one process each)")
     elif args.workload in TEXT_WORKLOADS:
         text, _, _, _, _, n, starts_of = text_workload(args.workload, args.scale)
         m = min(n, CPU_SAMPLE[args.workload])
@@ -980,26 +1252,45 @@ def run_reference(args, rank):
         sample = f"first {m:,} strings of {args.workload} per step (pointers into the whole text)"
         timer = lambda: time_cpu_sort(ss, m)  # noqa: E731
     else:
+        # The plain workloads: every timed step sorts the whole configuration
+        # (the same strings the GPU arm sorts); warm-up steps sort the bounded
+        # sample, which touches the same code and pages.
         ss = pyssort.WORKLOADS[args.workload](args.scale)
-        m = min(ss.n, CPU_SAMPLE.get(args.workload, 2_000_000))
-        sample = f"first {m:,} strings of {args.workload} per step"
+        m = ss.n
+        ms_ = min(ss.n, CPU_SAMPLE.get(args.workload, 2_000_000))
+        sample = (f"all {m:,} strings of {args.workload} per timed step (the full "
+                  f"configuration); warm-up steps sort the first {ms_:,}")
         timer = lambda: time_cpu_sort(ss, m)  # noqa: E731
+        warm = lambda: time_cpu_sort(ss, ms_)  # noqa: E731
+        same = True
+    if warm is None:
+        warm = timer
     for _ in range(args.warmup):
-        timer()
+        warm()
     total = 0.0
     kind = None
+    timed = 0
+    t_start = time.perf_counter()
     for _ in range(args.steps):
         t, kind = timer()
         total += t
-    v = m * args.steps / total
+        timed += 1
+        # Bounded run: once the timed steps have taken REF_BUDGET_S, the
+        # remaining steps are skipped (reported in steps_timed).
+        if time.perf_counter() - t_start > REF_BUDGET_S:
+            break
+    if pool is not None:
+        pool.close()
+    v = m * timed / total
     return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "steps": args.steps, "steps_timed": timed, "warmup": args.warmup,
+        "ms_per_step": 1000 * total / timed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
         "config": {"workload": args.workload, "description": DESCRIPTIONS.get(args.workload),
-                   "n_strings": ss.n, "sample_strings": m},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+                   "n_strings": ss.n, "sample_strings": m, "same_config": same},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
                          "routine": "msd_CE6 (single-threaded by design: function-static "
                                     "bucket arrays, src/msd_ce.cpp:392)",
                          "sample": sample,
@@ -1039,6 +1330,11 @@ def main():
     finally:
         if dist is not None:
             dist.destroy_process_group()
+    if (out is not None and world == 1 and args.workload == DEFAULT_WORKLOAD and
+            args.scale == 1.0 and not args.no_extras):
+        import gc
+        gc.collect()
+        out["configs"] = extra_configs(args)
     if out is not None:
         print(json.dumps(out), flush=True)
 

@@ -85,7 +85,8 @@ int ssort_sort_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byt
  * loads the library holds until the process exits; larger n is rejected with
  * SSORT_EINVAL.  The caller still passes the inputs and the perm (and
  * optional lcp) outputs, and a cudaStream_t (NULL = the legacy default
- * stream); the call returns when the results are complete.  The first call
+ * stream); the call waits for that stream (cudaStreamSynchronize) before it
+ * returns, on failure too, so the results are complete.  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress), so
  * it should come before any stream capture.  Every call uses the same array
  * and leaves its contents behind (what must start at zero is cleared by each

@@ -20,7 +20,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 ORACLE = os.path.join(ROOT, "oracle")
-REF_DIR = os.environ.get("SSORT_REF_DIR", "/root/reference")
+# The reference checkout: $SSORT_REF_DIR, else a sibling directory of this
+# repository named `reference`.  Without it the reference-built checkers are
+# skipped (the GPU box only uses the files built beforehand).
+REF_DIR = os.environ.get("SSORT_REF_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
 
 LIB = os.path.join(PKG, "libssort_b200.so")
 WLIB = os.path.join(PKG, "libssort_workloads.so")

@@ -1120,7 +1120,11 @@ extern "C" int ssort_sort_device_noalloc(const uint8_t *d_arena, uint64_t arena_
     c.ws = ws_bind(ws_layout(NOALLOC_MAX_N), d.scratch);
     c.ws_n = NOALLOC_MAX_N;
     const int rc = c.run_ws(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, d_perm, d_lcp);
-    if (rc == SSORT_OK) SS_CUDA(cudaStreamSynchronize(c.st));
+    // Drain the stream on every exit, failed ones included: kernels queued
+    // before an error still use the shared scratch, and the next call (which
+    // may start as soon as the lock is released) must not race with them.
+    const cudaError_t se = cudaStreamSynchronize(c.st);
     c.h_ctr = nullptr;
+    if (rc == SSORT_OK && se != cudaSuccess) return cuda_fail(se, "cudaStreamSynchronize");
     return rc;
 }

@@ -1,7 +1,8 @@
 """GPU test of ssort_sort_device_noalloc, the entry point for callers that
 cannot let the library allocate device memory (its scratch is a fixed array
 inside the library).  It must return exactly what ssort_sort_device returns for
-the same input, call after call, although every call reuses the same scratch.
+the same input, and what the oracle returns, call after call, although every
+call reuses the same scratch.
 
 Kept in its own file named to be collected last, so a failure here cannot hide
 the rest of the suite; it also passes when run alone in a fresh process.
@@ -11,6 +12,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import pyoracle
 import pyssort
 
 pytestmark = pytest.mark.gpu
@@ -26,14 +28,17 @@ def _device_set(ss, off_dtype):
     return arena, offs, offs_np.dtype.itemsize
 
 
-def _sort_noalloc(arena, nbytes, offs, width, n):
+def _sort_noalloc(arena, nbytes, offs, width, n, with_lcp=True, stream=None):
     torch = pytest.importorskip("torch")
-    perm = torch.empty(n, dtype=torch.int32, device="cuda")
-    lcp = torch.empty(n, dtype=torch.int32, device="cuda")
+    perm = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    lcp = torch.empty(max(n, 1), dtype=torch.int32, device="cuda") if with_lcp else None
+    st = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
     rc = pyssort.lib().ssort_sort_device_noalloc(arena.data_ptr(), nbytes, offs.data_ptr(), width,
-                                                 n, perm.data_ptr(), lcp.data_ptr(), None)
+                                                 n, perm.data_ptr(),
+                                                 lcp.data_ptr() if with_lcp else None, st)
     assert rc == 0, pyssort.lib().ssort_last_error().decode()
-    return perm.cpu().numpy().view(np.uint32), lcp.cpu().numpy().view(np.uint32)
+    p = perm.cpu().numpy().view(np.uint32)[:n]
+    return p, (lcp.cpu().numpy().view(np.uint32)[:n] if with_lcp else None)
 
 
 def _sort_regular(sorter, arena, nbytes, offs, width, n):
@@ -59,6 +64,32 @@ def test_noalloc_matches_regular_entry_point_twice():
                 perm, lcp = _sort_noalloc(arena, ss.arena.nbytes, offs, width, ss.n)
                 assert np.array_equal(perm, ref_perm)
                 assert np.array_equal(lcp, ref_lcp)
+
+
+def test_noalloc_matches_oracle_on_caller_stream_and_without_lcp():
+    torch = pytest.importorskip("torch")
+    ss = pyssort.gen_urls(100_000, seed=64)
+    ref_perm, ref_lcp = pyoracle.oracle_sort(ss.arena, ss.offs)
+    arena, offs, width = _device_set(ss, np.uint64)
+    side = torch.cuda.Stream()
+    for _ in range(2):
+        perm, lcp = _sort_noalloc(arena, ss.arena.nbytes, offs, width, ss.n, stream=side)
+        assert np.array_equal(perm, ref_perm)
+        assert np.array_equal(lcp, ref_lcp)
+        perm, none = _sort_noalloc(arena, ss.arena.nbytes, offs, width, ss.n, with_lcp=False)
+        assert none is None
+        assert np.array_equal(perm, ref_perm)
+
+
+@pytest.mark.parametrize("n", [1, 2])
+def test_noalloc_tiny_inputs(n):
+    ss = pyssort.gen_uniform(n, 0, 5, ord("a"), 3, seed=65 + n)
+    ref_perm, ref_lcp = pyoracle.oracle_sort(ss.arena, ss.offs)
+    arena, offs, width = _device_set(ss, np.uint32)
+    for _ in range(2):
+        perm, lcp = _sort_noalloc(arena, ss.arena.nbytes, offs, width, n)
+        assert np.array_equal(perm, ref_perm)
+        assert np.array_equal(lcp, ref_lcp)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
