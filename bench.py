@@ -34,6 +34,29 @@ import numpy as np  # noqa: E402
 import pyssort  # noqa: E402
 
 METRIC = "sort throughput (strings/s)"
+PARAMS = {"target_bucket": pyssort.SSORT_PARAM_TARGET_BUCKET,
+          "warp8_cap": pyssort.SSORT_PARAM_WARP8_CAP,
+          "overlap": pyssort.SSORT_PARAM_OVERLAP,
+          "fused_gather": pyssort.SSORT_PARAM_FUSED_GATHER,
+          "warp1_deep": pyssort.SSORT_PARAM_WARP1_DEEP,
+          "block_prefetch": pyssort.SSORT_PARAM_BLOCK_PREFETCH,
+          "graph": pyssort.SSORT_PARAM_GRAPH}
+
+
+def apply_params(sorter, args):
+    """--param NAME=VALUE settings (and the older dedicated flags)."""
+    out = {}
+    for kv in getattr(args, "param", []) or []:
+        k, v = kv.split("=", 1)
+        sorter.set_param(PARAMS[k], int(v))
+        out[k] = int(v)
+    if getattr(args, "target_bucket", 0):
+        sorter.set_param(pyssort.SSORT_PARAM_TARGET_BUCKET, args.target_bucket)
+        out["target_bucket"] = args.target_bucket
+    if getattr(args, "warp1_deep", None) is not None:
+        sorter.set_param(pyssort.SSORT_PARAM_WARP1_DEEP, args.warp1_deep)
+        out["warp1_deep"] = args.warp1_deep
+    return out
 # Wall-clock bound of the reference arm's timed steps (seconds): a full-size
 # CPU sort of the 50 M URLs takes about 14 s on one core.
 REF_BUDGET_S = 300.0
@@ -74,7 +97,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
-                    choices=sorted(pyssort.WORKLOADS) + ["batch_c4", "serve_c5",
+                    choices=sorted(pyssort.WORKLOADS) + ["batch_c4", "batch_c4_full", "serve_c5",
                                                          "text_urls_50m", "suffixes_160m"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--autotune", action="store_true",
@@ -87,6 +110,9 @@ def parse():
                          "when absent)")
     ap.add_argument("--target-bucket", type=int, default=0,
                     help="override the partition's wanted strings per range bucket")
+    ap.add_argument("--param", action="append", default=[], metavar="NAME=VALUE",
+                    help="set a tuning parameter of the sort context (names: " +
+                         ", ".join(sorted(PARAMS)) + "); repeatable")
     ap.add_argument("--serve-requests", type=int, default=2000,
                     help="requests per arrival rate of the serve_c5 sweep")
     ap.add_argument("--serve-rates", default="1000,2000,5000,10000,20000,50000")
@@ -294,10 +320,7 @@ def run_ours(args, rank, world, local_rank, dist):
     d_perm = torch.empty(n, dtype=torch.int32, device=f"cuda:{local_rank}")
     d_lcp = torch.empty(n, dtype=torch.int32, device=f"cuda:{local_rank}")
     sorter = pyssort.Sorter(local_rank)
-    if args.target_bucket:
-        sorter.set_param(pyssort.SSORT_PARAM_TARGET_BUCKET, args.target_bucket)
-    if args.warp1_deep is not None:
-        sorter.set_param(pyssort.SSORT_PARAM_WARP1_DEEP, args.warp1_deep)
+    params = apply_params(sorter, args)
     stream = torch.cuda.Stream(device=local_rank)
     ab = ss.arena.nbytes
 
@@ -438,6 +461,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "key_gbs": round(ss.text_bytes * args.steps * world / (ms / 1e3) / 1e9, 2),
         "roofline": roofline, "sort_roofline": sort_roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clocks.summary(), "tuning": tuning,
+        "params": params,
         "stats": {k: v for k, v in st.as_dict().items()}, "kernels": per_kernel,
     }
     return out
@@ -483,8 +507,7 @@ def run_text(args, rank, world, local_rank, dist):
     d_perm = torch.empty(n, dtype=torch.int32, device=dev)
     d_lcp = torch.empty(n, dtype=torch.int32, device=dev)
     sorter = pyssort.Sorter(local_rank)
-    if args.warp1_deep is not None:
-        sorter.set_param(pyssort.SSORT_PARAM_WARP1_DEEP, args.warp1_deep)
+    apply_params(sorter, args)
     stream = torch.cuda.Stream(device=local_rank)
 
     def step():
@@ -615,6 +638,117 @@ class TextSample:
         return self
 
 
+BATCH_WAVE_STRINGS = 200_000_000  # strings per wave of the full batched list
+
+
+def run_batch_full(args):
+    """The whole batched instance list, not the 1.5e9-byte subset: 20,000
+    instances (about 4.0e9 strings, 1.2e11 key bytes; far more than one
+    sort's 32-bit positions and the device memory), streamed through one GPU
+    in waves of consecutive instances of up to BATCH_WAVE_STRINGS strings.
+    Each wave is one batched call; a host thread generates the next wave
+    while the GPU sorts the current one.  `value` counts device time (CUDA
+    events around each batched call); wall time (generation, copies,
+    checks) is reported beside it.  Two instances of every wave are checked
+    against the oracle."""
+    import queue
+    import threading as th
+
+    import torch
+    import pyoracle
+    torch.cuda.set_device(0)
+    params = pyssort.batch_instance_params(20000, 5)
+    if args.scale < 1.0:
+        params = params[:max(1, int(len(params) * args.scale))]
+    waves, cur, m = [], [], 0
+    for p in params:
+        if cur and m + p[0] > BATCH_WAVE_STRINGS:
+            waves.append(cur)
+            cur, m = [], 0
+        cur.append(p)
+        m += p[0]
+    if cur:
+        waves.append(cur)
+    q = queue.Queue(maxsize=1)
+
+    def producer():
+        for k, wp in enumerate(waves):
+            q.put((k, wp, pyssort.gen_instances(wp, seed=1000 + k)))
+        q.put(None)
+
+    prod = th.Thread(target=producer, daemon=True)
+    sorter = pyssort.Sorter(0)
+    apply_params(sorter, args)
+    stream = torch.cuda.Stream()
+    rng = np.random.default_rng(9)
+    clocks = Clocks(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    prod.start()
+    dev_ms = 0.0
+    tot_n = tot_bytes = tot_inst = checked = 0
+    launches = []
+    while True:
+        item = q.get()
+        if item is None:
+            break
+        k, wp, ss = item
+        n, ninst = ss.n, len(wp)
+        d_arena = torch.from_numpy(ss.arena).cuda()
+        d_offs = torch.from_numpy(ss.offs.view(np.int64)).cuda()
+        d_inst = torch.from_numpy(ss.inst_start.view(np.int32)).cuda()
+        d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+        d_lcp = torch.empty(n, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sorter.sort_batch_device(d_arena, ss.arena.nbytes, d_offs, 8, n, d_inst, ninst, d_perm,
+                                 d_lcp, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dev_ms += e0.elapsed_time(e1)
+        # two instances of the wave (of at most 500,000 strings) against the oracle
+        st = ss.inst_start
+        small = [i for i in range(ninst) if 2 <= int(st[i + 1]) - int(st[i]) <= 500_000]
+        for i in rng.choice(small, size=min(2, len(small)), replace=False) if small else []:
+            lo, hi = int(st[i]), int(st[i + 1])
+            rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs[lo:hi])
+            gp = d_perm[lo:hi].cpu().numpy().view(np.uint32)
+            gl = d_lcp[lo:hi].cpu().numpy().view(np.uint32)
+            if not (np.array_equal(gp, rp) and np.array_equal(gl, rl)):
+                raise RuntimeError(f"wave {k} instance {i}: GPU result differs from the oracle")
+            checked += 1
+        tot_n += n
+        tot_bytes += ss.text_bytes
+        tot_inst += ninst
+        launches.append(n)
+        del d_arena, d_offs, d_inst, d_perm, d_lcp, ss
+    wall = time.perf_counter() - t0
+    prod.join()
+    clocks.stop()
+    sorter.close()
+    return {
+        "metric": METRIC, "value": tot_n / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1,
+        "steps": len(waves), "warmup": 0, "ms_per_step": dev_ms / len(waves),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator, stand-in for the reference's text corpora)",
+        "config": {"workload": "batch_c4_full",
+                   "description": "the full list: " + DESCRIPTIONS["batch_c4"].split(";")[0] +
+                                  f"; {len(params)} instances in {len(waves)} waves of at most "
+                                  f"{BATCH_WAVE_STRINGS:,} strings, one batched call per wave; "
+                                  "seeds 5 (list), 1000 + wave (strings)",
+                   "n_instances": tot_inst, "n_strings": tot_n, "key_bytes": tot_bytes,
+                   "parallelism": "single", "l2": "inputs larger than L2 (GBs per wave)"},
+        "key_gbs": round(tot_bytes / (dev_ms / 1e3) / 1e9, 2),
+        "device_s": round(dev_ms / 1e3, 3), "wall_s": round(wall, 2),
+        "wall_strings_per_s": tot_n / wall,
+        "wall_note": "wall time includes host generation of every wave (overlapped with the "
+                     "sorts), the pageable host-to-device copies and the oracle checks",
+        "instances_checked_against_oracle": checked, "clocks": clocks.summary(),
+    }
+
+
 def run_batch(args):
     """Batched form vs plain form on the same GPU: one ssort_sort_batch_device
     call over all instances vs one ssort_sort_device call per instance."""
@@ -629,6 +763,7 @@ def run_batch(args):
     d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
     d_lcp = torch.empty(n, dtype=torch.int32, device="cuda")
     sorter = pyssort.Sorter(0)
+    apply_params(sorter, args)
     stream = torch.cuda.Stream()
     ab = ss.arena.nbytes
 
@@ -1230,10 +1365,11 @@ def run_reference(args, rank):
     cores = 1
     pool = None
     same = False
-    if args.workload in ("batch_c4", "serve_c5"):
+    if args.workload in ("batch_c4", "batch_c4_full", "serve_c5"):
         # independent instances, each sorted alone by msd_CE6, spread over
         # every host core (one process per core)
-        params, seed = instance_params(args.workload, 16_000_000)
+        params, seed = instance_params("serve_c5" if args.workload == "serve_c5" else "batch_c4",
+                                       16_000_000)
         ss = pyssort.gen_instances(params, seed=seed)
         m = ss.n
         kind0 = "reference" if _ref_lib() is not None else "port"
@@ -1309,9 +1445,10 @@ def main():
         if out is not None:
             print(json.dumps(out), flush=True)
         return
-    if args.workload in ("batch_c4", "serve_c5"):
+    if args.workload in ("batch_c4", "batch_c4_full", "serve_c5"):
         if rank == 0:
-            fn = run_batch if args.workload == "batch_c4" else run_serve
+            fn = {"batch_c4": run_batch, "batch_c4_full": run_batch_full,
+                  "serve_c5": run_serve}[args.workload]
             print(json.dumps(fn(args)), flush=True)
         return
     dist = None

@@ -244,6 +244,18 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                        sorts a segment of <= 32 strings takes on its own
                                        runs of equal keys before handing what is left to
                                        the next round; 0: every run waits for the next round */
+#define SSORT_PARAM_BLOCK_PREFETCH 6 /* 1 (default): the CTA sort of segments of 257..2048
+                                        strings copies the next segment's records into
+                                        shared memory while it sorts the current one;
+                                        0: one record buffer, loaded through registers */
+#define SSORT_PARAM_GRAPH 7          /* 1: device-driven round loop: the sort runs as a CUDA
+                                        graph whose rounds and partition levels are
+                                        conditional loops (no host round trip between
+                                        kernels; one host read per up to 64 rounds);
+                                        0 (default): the host drives the rounds */
+#define SSORT_PARAM_GRAPH_MAX_LEVELS 8 /* 1..4096 (default 4096): partition levels one round
+                                          of the device-driven loop may take; a round that
+                                          needs more fails with SSORT_EINTERNAL */
 int ssort_set_param(ssort_ctx *ctx, int param, int64_t value);
 
 /*

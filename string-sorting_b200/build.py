@@ -64,7 +64,8 @@ def _run(cmd, cwd=None):
 
 def build_cuda(force=False, extra_flags=()):
     srcs = [os.path.join(CSRC, f) for f in ("ssort_kernels.cu", "ssort_engine.cu",
-                                             "ssort_server.cu", "ssort_merge.cpp")]
+                                             "ssort_graph.cu", "ssort_server.cu",
+                                             "ssort_merge.cpp")]
     deps = srcs + [os.path.join(CSRC, h) for h in ("ssort_internal.cuh", "ssort_host.cuh")]
     deps.append(os.path.join(INCLUDE, "ssort_b200.h"))
     if not force and not _newer(LIB, deps):

@@ -66,8 +66,8 @@ int ssort_ctx::sample_entropy(const uint8_t *arena_p, uint64_t arena_bytes, cons
     return SSORT_OK;
 }
 
-int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev) {
-    LAUNCH(this, "scan", launch_scan(in, out, n_host, n_dev, ws.partials, st));
+int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t cap, Count n) {
+    LAUNCH(this, "scan", launch_scan(in, out, cap, n, ws.partials, st));
     return SSORT_OK;
 }
 
@@ -94,10 +94,11 @@ int ssort_ctx::launch_small(const SortArgs &a, Seg *nxt, SmallDone &d) {
     auto grid = [&](uint32_t n, uint32_t per_cta) { return (int)((n + per_cta - 1) / per_cta); };
     uint32_t n = h_ctr->n_w1 - d.w1;
     LAUNCH(this, "warp1",
-           launch_warp1(a, ws.W1 + d.w1, n, nxt, dc, std::min(grid(n, 32), grid_for(8)), s2));
+           launch_warp1(a, ws.W1, hspan(d.w1, d.w1 + n), nxt, dc,
+                        std::min(grid(n, 32), grid_for(8)), s2));
     d.w1 += n;
     n = h_ctr->n_w8 - d.w8;
-    LAUNCH(this, "warp8", launch_warp8(a, ws.W8 + d.w8, n, nxt, dc, grid(n, 8), s2));
+    LAUNCH(this, "warp8", launch_warp8(a, ws.W8, hspan(d.w8, d.w8 + n), nxt, dc, grid(n, 8), s2));
     d.w8 += n;
     // CTA-sort size classes: groups of 64, 128, 256 threads per segment.
     Seg *lists[3] = {ws.S, ws.S2, ws.S3};
@@ -106,11 +107,12 @@ int ssort_ctx::launch_small(const SortArgs &a, Seg *nxt, SmallDone &d) {
         n = counts[k] - d.s[k];
         const uint32_t per_cta = (uint32_t)SMALL_THREADS / (64u << k);
         LAUNCH(this, "block",
-               launch_block(a, lists[k] + d.s[k], n, k, nxt, dc, grid(n, per_cta), s2));
+               launch_block(a, lists[k], hspan(d.s[k], d.s[k] + n), k, nxt, dc,
+                            grid(n, per_cta * (block_prefetch ? 4u : 1u)), s2, block_prefetch));
         d.s[k] += n;
     }
     n = h_ctr->n_equal - d.e;
-    LAUNCH(this, "equal", launch_equal(a, ws.E + d.e, n, nxt, dc, grid(n, 1), s2));
+    LAUNCH(this, "equal", launch_equal(a, ws.E, hspan(d.e, d.e + n), nxt, dc, grid(n, 1), s2));
     d.e += n;
     return SSORT_OK;
 }
@@ -148,8 +150,8 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     const int g8 = grid_for(8), g4 = grid_for(4), g2 = grid_for(2);
     SS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
     LAUNCH(this, "classify",
-           launch_classify(cur, n_cur, a.warp8_cap, ws.W1, ws.W8,
-                           SmallLists{{ws.S, ws.S2, ws.S3}}, ws.L, dc, st));
+           launch_classify(cur, hcount(n_cur), a.warp8_cap, ws.W1, ws.W8,
+                           SmallLists{{ws.S, ws.S2, ws.S3}}, ws.L, dc, 0, st));
     SS_TRY(sync_counters());
     if (round_no < SSORT_MAX_ROUNDS) stats.live[round_no] = h_ctr->live_next;
     // The on-chip sorts of the segments known after each host read of the
@@ -166,8 +168,8 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     const bool fused_gather = !fresh_round && this->fused_gather;
     if (n_large && !fused_gather) {
         LAUNCH(this, "seg_tiles",
-               launch_seg_tiles(lcur, n_large, GATHER_TILE, ws.tile_base, st));
-        LAUNCH(this, "gather", launch_gather(a, lcur, n_large, ws.tile_base, dc, g8, st));
+               launch_seg_tiles(lcur, hcount(n_large), GATHER_TILE, ws.tile_base, st));
+        LAUNCH(this, "gather", launch_gather(a, lcur, hcount(n_large), ws.tile_base, dc, g8, st));
     }
     uint32_t levels_this_round = 0;
     while (n_large) {
@@ -178,27 +180,22 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
             return fail(SSORT_EINTERNAL, "partition levels exceeded 4096");
         stats.partition_levels++;
         const bool first = fused_gather && levels_this_round == 1;
+        const Count nl = hcount(n_large);
         LAUNCH(this, "sample",
-               launch_sample(a, lcur, n_large, ws.spl, ws.nspl, ws.tbl, ws.ntiles, ws.cm_size,
-                             first, st));
+               launch_sample(a, lcur, nl, ws.spl, ws.nspl, ws.tbl, ws.ntiles, ws.cm_size,
+                             first, 0, st));
         LAUNCH(this, "scan_pair",
-               launch_scan_pair(ws.ntiles, ws.tile_base, ws.cm_size, ws.cm_base, n_large,
-                                st));
+               launch_scan_pair(ws.ntiles, ws.tile_base, ws.cm_size, ws.cm_base, nl, st));
         LAUNCH(this, first ? "count_gather" : "count",
-               launch_count(a, lcur, n_large, ws.tile_base, ws.spl, ws.nspl, ws.tbl, ws.cm_base,
+               launch_count(a, lcur, nl, ws.tile_base, ws.spl, ws.nspl, ws.tbl, ws.cm_base,
                             ws.cm, dc, first, g2, st));
-        SS_TRY(scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
-                    ws.cm_base + n_large));
+        SS_TRY(scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1), dcount(ws.cm_base + n_large)));
         LAUNCH(this, "scatter",
-               launch_scatter(a, lcur, n_large, ws.tile_base,
-                              ws.spl, ws.nspl,
-                              ws.tbl, ws.cm_base,
+               launch_scatter(a, lcur, nl, ws.tile_base, ws.spl, ws.nspl, ws.tbl, ws.cm_base,
                               ws.cm, g2, st));
         LAUNCH(this, "emit",
-               launch_emit(a, lcur, n_large, ws.tile_base,
-                           ws.nspl, ws.cm_base,
-                           ws.cm, ws.W1, ws.W8, SmallLists{{ws.S, ws.S2, ws.S3}}, lnext,
-                           ws.E, ws.B, nxt, dc, st));
+               launch_emit(a, lcur, nl, ws.tile_base, ws.nspl, ws.cm_base, ws.cm, ws.W1, ws.W8,
+                           SmallLists{{ws.S, ws.S2, ws.S3}}, lnext, ws.E, ws.B, nxt, dc, 0, st));
         SS_TRY(launch_small(a, nxt, done));  // segments known before this level
         SS_TRY(sync_counters());
         SS_TRY(fork_small());
@@ -285,6 +282,10 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.warp8_cap = warp8_cap;
     a.warp1_deep = warp1_deep;
     a.key2 = key2;
+
+    // The device-driven loop: not while profiling (per-kernel events need
+    // host launches) and not for the server's per-round calls.
+    if (graph_mode && !prof) return run_graph(a, n, d_inst, ninst);
 
     Seg *cur = ws.R, *nxt = ws.N;
     Counters *dc = ws.ctr;
@@ -468,6 +469,10 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
     if (!ctx) return;
     with_device(ctx, [&]() -> int {
         if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+        ctx->graph_release();
+        for (cudaStream_t c : ctx->cap)
+            if (c) cudaStreamDestroy(c);
+        if (ctx->h_gs) cudaFreeHost(ctx->h_gs);
         for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst, &ctx->aux,
                      &ctx->aux2})
             if (b->p) cudaFree(b->p);
@@ -714,6 +719,19 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "fused_gather must be 0 or 1");
             ctx->fused_gather = value != 0;
             return SSORT_OK;
+        case SSORT_PARAM_GRAPH:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "graph must be 0 or 1");
+            ctx->graph_mode = value != 0;
+            return SSORT_OK;
+        case SSORT_PARAM_GRAPH_MAX_LEVELS:
+            if (value < 1 || value > (int64_t)GRAPH_MAX_LEVELS)
+                return fail(SSORT_EINVAL, "graph_max_levels out of range (1..4096)");
+            ctx->graph_max_levels = (uint32_t)value;
+            return SSORT_OK;
+        case SSORT_PARAM_BLOCK_PREFETCH:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "block_prefetch must be 0 or 1");
+            ctx->block_prefetch = value != 0;
+            return SSORT_OK;
         case SSORT_PARAM_WARP1_DEEP:
             if (value < 0 || value > WARP1_DEEP_MAX)
                 return fail(SSORT_EINVAL, "warp1_deep out of range (0..4096)");
@@ -802,7 +820,7 @@ int text_write(ssort_ctx *ctx, uint8_t *d_text, uint64_t len, uint8_t delim, uin
     uint32_t *d_tiles = (uint32_t *)((unsigned char *)ctx->aux.p + 256);
     uint32_t *d_parts =
         (uint32_t *)((unsigned char *)ctx->aux.p + 256 + (((size_t)nt + 1) * 4 + 255) / 256 * 256);
-    LAUNCH(ctx, "scan", launch_scan(d_tiles, d_tiles, nt, nullptr, d_parts, ctx->st));
+    LAUNCH(ctx, "scan", launch_scan(d_tiles, d_tiles, nt, hcount(nt), d_parts, ctx->st));
     LAUNCH(ctx, "text_starts",
            launch_text_starts(d_text, len, delim, d_tiles, n, d_offs, off_width, ctx->st));
     return SSORT_OK;

@@ -80,6 +80,17 @@ struct ssort_ctx {
     uint32_t warp1_deep = ssort::WARP1_DEEP;        // in-warp refinement steps
     bool overlap = true;       // round-0 on-chip sorts on the side stream
     bool fused_gather = true;  // rounds >= 1 gather inside the first count
+    bool block_prefetch = true;  // double-buffered CTA sort (k_block2)
+    // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
+    // key it was built for, three streams to capture nested conditional
+    // bodies on, and a pinned copy of the loop state.
+    bool graph_mode = false;
+    uint32_t graph_max_levels = ssort::GRAPH_MAX_LEVELS;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<unsigned char> gkey;
+    cudaStream_t cap[3] = {nullptr, nullptr, nullptr};
+    ssort::GraphState *h_gs = nullptr;
     // Autotuned values per (size class * 4 + entropy class), applied to later
     // sorts of the same classes; not while the tuner itself runs.
     struct Tuned {
@@ -179,7 +190,7 @@ struct ssort_ctx {
     int grid_for(int per_sm) const { return num_sms * per_sm; }
 
     int reserve(uint32_t n);
-    int scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev);
+    int scan(const uint32_t *in, uint32_t *out, uint32_t cap, ssort::Count n);
     int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
             uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
             uint32_t ninst = 0);
@@ -197,6 +208,11 @@ struct ssort_ctx {
     int run_ws(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
                uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
                uint32_t ninst = 0);
+    // device-driven round loop (ssort_graph.cu)
+    int run_graph(const ssort::SortArgs &a, uint32_t n, const uint32_t *d_inst, uint32_t ninst);
+    int graph_build(const ssort::SortArgs &a);
+    int graph_small(const ssort::SortArgs &a, cudaStream_t s);
+    void graph_release();
 };
 
 #define LAUNCH(ctx, name, call)                 \

@@ -92,6 +92,29 @@ struct Counters {
     unsigned long long window_saved, window_used;  // key2 entries written / read
 };
 
+// A count the host knows (dev == nullptr: `host`) or only the device knows:
+// *dev, or dev[*at] when `at` is set (a count stored at an index that is
+// itself a device value).  The host-driven round loop passes host counts;
+// the device-driven loop (a CUDA graph whose kernels find their work in
+// device memory) passes device ones.
+struct Count {
+    uint32_t host;
+    const uint32_t *dev;
+    const uint32_t *at;
+};
+inline Count hcount(uint32_t n) { return Count{n, nullptr, nullptr}; }
+inline Count dcount(const uint32_t *d, const uint32_t *at = nullptr) { return Count{0, d, at}; }
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t count_of(const Count &c) {
+    return c.dev ? (c.at ? c.dev[*c.at] : *c.dev) : c.host;
+}
+#endif
+// Entries [lo, hi) of a segment list.
+struct Span {
+    Count lo, hi;
+};
+inline Span hspan(uint32_t lo, uint32_t hi) { return Span{hcount(lo), hcount(hi)}; }
+
 // The CTA-sort segment lists, one per size class (n_small, n_small2, n_small3).
 struct SmallLists {
     Seg *s[3];
@@ -120,6 +143,33 @@ struct SortArgs {
     ulonglong2 *key2;
 };
 
+// ---- device-driven round loop ----------------------------------------------
+// The counters the host round loop keeps on the host, kept on the device for
+// a sort driven by a CUDA graph with conditional nodes (the graph's control
+// kernels advance them and set the loops' conditions).  One per workspace.
+constexpr uint32_t GRAPH_MAX_LEVELS = 4096;  // partition levels per round
+constexpr uint32_t GRAPH_ROUNDS_PER_LAUNCH = 64;
+
+struct GraphState {
+    uint32_t n_cur;    // segments of the current round (list R)
+    uint32_t n_large;  // large segments of the current partition level (list L)
+    uint32_t round;    // rounds finished in this sort
+    uint32_t round_in_launch;
+    uint32_t levels;   // partition levels of the current round
+    uint32_t first;    // 1 while the level gathers its keys in the count kernel
+    uint32_t done;     // 1 once no segment is left
+    uint32_t error;    // 1: more than GRAPH_MAX_LEVELS levels in a round
+    uint32_t cur_w1, cur_w8, cur_s[3], cur_e;  // on-chip sort list entries launched
+    uint32_t ticket;   // CTAs finished in the current control kernel
+    uint32_t fused;    // rounds >= 1 gather inside their first count (tuning)
+    uint32_t max_levels;
+    uint32_t partition_levels;
+    unsigned long long small_segments, partitioned, gather_elems, gather_fused, warp1_fresh,
+        warp1_keyed, warp8_fresh, warp8_keyed, block_fresh, block_keyed, equal_moved,
+        equal_final, boundaries, warp1_deep, full_sorted, window_saved, window_used;
+    unsigned long long live[64];
+};
+
 // ---- device workspace ---------------------------------------------------------
 // Every scratch buffer of one sort of up to n strings, carved from one block
 // of device memory by ws_layout (offsets, 256-byte aligned).
@@ -131,7 +181,7 @@ constexpr uint32_t scan_partials_for(uint64_t n) {
 
 struct WsLayout {
     size_t idx1, key0, key1, lcp, bkt, R, N, W1, W8, S, S2, S3, E, B, L, L2, spl, nspl, tbl, ntiles,
-        cm_size, cm_base, tile_base, tmp, cm, partials, ctr;
+        cm_size, cm_base, tile_base, tmp, cm, partials, ctr, gs;
     size_t cm_cap, total;
 };
 
@@ -176,6 +226,7 @@ constexpr WsLayout ws_layout(uint64_t n) {
     o.cm = take(o.cm_cap * 4);
     o.partials = take((size_t)scan_partials_for(o.cm_cap) * 4);
     o.ctr = take(sizeof(Counters));
+    o.gs = take(sizeof(GraphState));
     o.total = off;
     return o;
 }
@@ -188,6 +239,7 @@ struct Workspace {
     uint16_t *tbl;
     uint32_t *bkt;
     Counters *ctr;
+    GraphState *gs;
     size_t cm_cap;
 };
 
@@ -220,6 +272,7 @@ inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
     w.cm = (uint32_t *)(base + o.cm);
     w.partials = (uint32_t *)(base + o.partials);
     w.ctr = (Counters *)(base + o.ctr);
+    w.gs = (GraphState *)(base + o.gs);
     w.cm_cap = o.cm_cap;
     return w;
 }
@@ -229,8 +282,10 @@ void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st);
 // 256-bin histogram of the first 8 key bytes of `samples` strings (tuning).
 void launch_byte_hist(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
                       uint32_t n, uint32_t samples, uint32_t *hist, cudaStream_t st);
-void launch_classify(const Seg *R, uint32_t nR, uint32_t warp8_cap, Seg *W1, Seg *W8,
-                     SmallLists S, Seg *L, Counters *c, cudaStream_t st);
+// Launchers with a Count take `grid` CTAs (or size the grid from a host count
+// when grid <= 0); their kernels loop over the work they find.
+void launch_classify(const Seg *R, Count nR, uint32_t warp8_cap, Seg *W1, Seg *W8,
+                     SmallLists S, Seg *L, Counters *c, int grid, cudaStream_t st);
 // Batches: one round-0 segment per instance; instance-local result indices.
 void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
                        Counters *c, cudaStream_t st);
@@ -260,44 +315,70 @@ void launch_localize(uint32_t *perm, uint32_t n, const uint32_t *inst_start, uin
                      cudaStream_t st);
 // Single-CTA scans of short per-segment arrays (out*[n] = totals).
 void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,
-                      uint32_t n, cudaStream_t st);
-void launch_seg_tiles(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out, cudaStream_t st);
+                      Count n, cudaStream_t st);
+void launch_seg_tiles(const Seg *segs, Count n, uint32_t tile, uint32_t *out, cudaStream_t st);
 // exclusive scan of in[0..n) into out[0..n); out[n] = total (out has n+1 slots).
-// n is read from *n_dev when n_dev is not null (n_host is then an upper bound).
-void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
-                 uint32_t *partials, cudaStream_t st);
+// cap (host) bounds n and sizes the grid; n itself is count_of(n).
+void launch_scan(const uint32_t *in, uint32_t *out, uint32_t cap, Count n, uint32_t *partials,
+                 cudaStream_t st);
 uint32_t scan_partials_needed(uint32_t n);
-void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+void launch_gather(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                    Counters *c, int grid, cudaStream_t st);
 // from_arena / gather: first partition level of a round, whose keys the
 // count kernel gathers from the arena (the sample reads its strings there).
-void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl,
+void launch_sample(const SortArgs &a, const Seg *L, Count nL, ulonglong2 *spl,
                    uint32_t *nspl, uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size,
-                   bool from_arena, cudaStream_t st);
-void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+                   bool from_arena, int grid, cudaStream_t st);
+void launch_count(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                   const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
                   const uint32_t *cm_base, uint32_t *cm, Counters *c, bool gather, int grid,
                   cudaStream_t st);
-void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+void launch_scatter(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                     const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
                     const uint32_t *cm_base, const uint32_t *cm_scan, int grid,
                     cudaStream_t st);
-void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+void launch_emit(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                  const uint32_t *nspl, const uint32_t *cm_base, const uint32_t *cm_scan,
                  Seg *W1, Seg *W8, SmallLists S, Seg *L2, Seg *E, uint2 *B, Seg *N,
-                 Counters *c, cudaStream_t st);
+                 Counters *c, int grid, cudaStream_t st);
 // On-chip segment sorts; list lengths are read from the counters on the device.
 // The on-chip sorts take n list entries from the given list pointer (a range
 // of the list), so that they can run while the list is still being appended.
-void launch_warp1(const SortArgs &a, const Seg *W1, uint32_t n, Seg *N, Counters *c, int grid,
+void launch_warp1(const SortArgs &a, const Seg *W1, Span sp, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
-void launch_warp8(const SortArgs &a, const Seg *W8, uint32_t n, Seg *N, Counters *c, int grid,
+void launch_warp8(const SortArgs &a, const Seg *W8, Span sp, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
 // cls: size class 0, 1, 2 (segment list S holds that class)
-void launch_block(const SortArgs &a, const Seg *S, uint32_t n, int cls, Seg *N, Counters *c,
-                  int grid, cudaStream_t st);
-void launch_equal(const SortArgs &a, const Seg *E, uint32_t n, Seg *N, Counters *c, int grid,
+// prefetch: the double-buffered variant (records of the next segment copied
+// asynchronously while the current one sorts; two CTAs per SM instead of three).
+void launch_block(const SortArgs &a, const Seg *S, Span sp, int cls, Seg *N, Counters *c,
+                  int grid, cudaStream_t st, bool prefetch);
+void launch_equal(const SortArgs &a, const Seg *E, Span sp, Seg *N, Counters *c, int grid,
                   cudaStream_t st);
 void launch_boundary(const SortArgs &a, const uint2 *B, Counters *c, int grid, cudaStream_t st);
+
+// Control kernels of the device-driven round loop.  Conditions are
+// cudaGraphConditionalHandle values (unsigned long long).
+// Round start: clear the round's counters and the sort-list cursors (and the
+// round condition, which only the round's last kernel sets again).
+void launch_g_round_begin(GraphState *g, Counters *c, unsigned long long h_round,
+                          cudaStream_t st);
+// After classification: the level loop's condition (large segments left) and
+// whether this round gathers its keys with a separate pass (round 0, or the
+// fused gather switched off).
+void launch_g_after_classify(GraphState *g, Counters *c, unsigned long long h_level,
+                             unsigned long long h_gather, cudaStream_t st);
+// Before a level: whether its count kernel gathers the keys itself (and the
+// level condition cleared, set again only by the level's last kernel).
+void launch_g_level_begin(GraphState *g, unsigned long long h_level, unsigned long long h_first,
+                          cudaStream_t st);
+// After a level: the next level's large segments move from L2 to L, the
+// cursors advance past the on-chip sorts launched, the level condition is set.
+void launch_g_level_end(GraphState *g, Counters *c, Seg *L, const Seg *L2,
+                        unsigned long long h_level, int grid, cudaStream_t st);
+// After a round: its statistics are added up, the next round's segments move
+// from N to R, and the round condition is set.
+void launch_g_round_end(GraphState *g, Counters *c, Seg *R, const Seg *N,
+                        unsigned long long h_round, int grid, cudaStream_t st);
 
 }  // namespace ssort

@@ -236,6 +236,16 @@ __device__ __forceinline__ uint32_t classify_tbl(const ulonglong2 *s, const uint
 // (stride 8) and the striped (stride 1) access patterns free of bank conflicts.
 __device__ __forceinline__ uint32_t pad(uint32_t e) { return e + (e >> 3); }
 
+// Slot of record e in a record array: padded (PK, arrays filled by the
+// threads themselves) or contiguous (arrays filled by asynchronous copies).
+template <bool PK>
+__device__ __forceinline__ uint32_t kslot(uint32_t e) {
+    if constexpr (PK)
+        return pad(e);
+    else
+        return e;
+}
+
 // ---- bitonic sort of (key, index) pairs held in registers -------------------
 // Element e = tid * ITEMS + i of a group of THREADS threads (blocked layout).
 // Strides below ITEMS run inside a thread, below 32 * ITEMS across lanes with
@@ -308,7 +318,7 @@ __device__ __forceinline__ void warp_bitonic(Key (&k)[ITEMS], uint32_t (&x)[ITEM
 
 // One warp sorts the 32 * ITEMS pairs at padded shared-memory positions
 // base .. base + 32 * ITEMS - 1 in place.
-template <int ITEMS>
+template <int ITEMS, bool PK = true>
 __device__ __noinline__ void warp_sort_run(ulonglong2 *sk, uint32_t *sx, uint32_t base,
                                               uint32_t lane) {
     Key k[ITEMS];
@@ -316,15 +326,15 @@ __device__ __noinline__ void warp_sort_run(ulonglong2 *sk, uint32_t *sx, uint32_
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         const uint32_t e = base + lane * ITEMS + i;
-        k[i] = to_key(sk[pad(e)]);
-        x[i] = sx[pad(e)];
+        k[i] = to_key(sk[kslot<PK>(e)]);
+        x[i] = sx[kslot<PK>(e)];
     }
     warp_bitonic<ITEMS>(k, x, lane);
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         const uint32_t e = base + lane * ITEMS + i;
-        sk[pad(e)] = from_key(k[i]);
-        sx[pad(e)] = x[i];
+        sk[kslot<PK>(e)] = from_key(k[i]);
+        sx[kslot<PK>(e)] = x[i];
     }
 }
 
@@ -422,13 +432,14 @@ __device__ __forceinline__ uint32_t merge_split64(const uint64_t *s, uint32_t a0
 
 // Merge-path split: number of elements of run A (length la, at a0) among the
 // first d outputs of merging A with run B (length lb, at b0); ties go to A.
+template <bool PK = true>
 __device__ __forceinline__ uint32_t merge_split(const ulonglong2 *sk, const uint32_t *sx,
                                                 uint32_t a0, uint32_t la, uint32_t b0,
                                                 uint32_t lb, uint32_t d) {
     uint32_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
-        const uint32_t pa = pad(a0 + mid), pb = pad(b0 + d - 1 - mid);
+        const uint32_t pa = kslot<PK>(a0 + mid), pb = kslot<PK>(b0 + d - 1 - mid);
         // A[mid] <= B[d-1-mid]: A[mid] is among the first d outputs.
         if (!pair_lt(to_key(sk[pb]), sx[pb], to_key(sk[pa]), sx[pa]))
             lo = mid + 1;
@@ -444,15 +455,15 @@ __device__ __forceinline__ uint32_t merge_split(const ulonglong2 *sk, const uint
 // numbered t = 0..threads-1.
 // Sorted position e -> shared-memory slot of its record: the slot itself
 // (records already in order) or the position field of the e-th packed key.
-template <bool IND>
+template <bool IND, bool PK = true>
 __device__ __forceinline__ uint32_t rec_slot(const uint64_t *sv, uint32_t e) {
     if constexpr (IND)
-        return pad((uint32_t)(sv[pad(e)] & POS_MASK));
+        return kslot<PK>((uint32_t)(sv[pad(e)] & POS_MASK));
     else
-        return pad(e);
+        return kslot<PK>(e);
 }
 
-template <bool IND>
+template <bool IND, bool PK = true>
 __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
                                                const ulonglong2 *sk, const uint32_t *sx,
                                                const uint64_t *sv, uint32_t t, uint32_t threads,
@@ -464,13 +475,13 @@ __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
         uint32_t run_lo = 0;
         if (e < s.len) {
             const uint32_t p = s.start + e;
-            const uint32_t q = rec_slot<IND>(sv, e);
+            const uint32_t q = rec_slot<IND, PK>(sv, e);
             const Key k = to_key(sk[q]);
             a.idx[0][p] = sx[q];
             if (e == 0 || e == s.len - 1) a.key[0][p] = from_key(k);
             bool same_prev = false;
             if (e > 0) {
-                const Key kp = to_key(sk[rec_slot<IND>(sv, e - 1)]);
+                const Key kp = to_key(sk[rec_slot<IND, PK>(sv, e - 1)]);
                 same_prev = key_eq(kp, k);
                 if (!same_prev)
                     a.lcp[p] = s.depth + key_lcp(kp, k);
@@ -478,11 +489,11 @@ __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
                     a.lcp[p] = s.depth + key_len(k);
             }
             if (same_prev && !key_is_end(k) &&
-                (e == s.len - 1 || !key_eq(to_key(sk[rec_slot<IND>(sv, e + 1)]), k))) {
+                (e == s.len - 1 || !key_eq(to_key(sk[rec_slot<IND, PK>(sv, e + 1)]), k))) {
                 uint32_t lo = 0, hi = e;  // first position of this run
                 while (lo < hi) {
                     const uint32_t mid = (lo + hi) >> 1;
-                    if (key_lt(to_key(sk[rec_slot<IND>(sv, mid)]), k))
+                    if (key_lt(to_key(sk[rec_slot<IND, PK>(sv, mid)]), k))
                         lo = mid + 1;
                     else
                         hi = mid;
@@ -495,17 +506,84 @@ __device__ __forceinline__ void finish_segment(const SortArgs &a, const Seg &s,
     }
 }
 
+// finish_segment for a packed sort whose order lives in sv (records in place):
+// neighbours whose windows differ get their LCP from the windows alone (all
+// keys share their first f bits, so the first differing bit is f + the
+// leading zeros of the windows' xor, and no NUL can precede it in either
+// key); only neighbours with equal windows read their full keys.  Same
+// writes and next-round runs as finish_segment<true>.
+template <bool PK>
+__device__ __forceinline__ void finish_packed(const SortArgs &a, const Seg &s,
+                                              const ulonglong2 *sk, const uint32_t *sx,
+                                              const uint64_t *sv, uint32_t f, uint32_t t,
+                                              uint32_t threads, Seg *N, Counters *c) {
+    // Uniform trip count so that every warp reaches the collective append.
+    for (uint32_t e0 = 0; e0 < s.len; e0 += threads) {
+        const uint32_t e = e0 + t;
+        bool want = false;
+        uint32_t run_lo = 0;
+        if (e < s.len) {
+            const uint32_t p = s.start + e;
+            const uint64_t v = sv[pad(e)];
+            const uint32_t q = kslot<PK>((uint32_t)(v & POS_MASK));
+            a.idx[0][p] = sx[q];
+            if (e == 0 || e == s.len - 1) a.key[0][p] = sk[q];
+            bool same_prev = false;
+            Key k = key_max();
+            if (e > 0) {
+                const uint64_t vp = sv[pad(e - 1)];
+                const uint64_t x = (v ^ vp) & ~POS_MASK;
+                if (x) {
+                    a.lcp[p] = s.depth + ((f + (uint32_t)__clzll((long long)x)) >> 3);
+                } else {
+                    k = to_key(sk[q]);
+                    const Key kp = to_key(sk[kslot<PK>((uint32_t)(vp & POS_MASK))]);
+                    same_prev = key_eq(kp, k);
+                    if (!same_prev)
+                        a.lcp[p] = s.depth + key_lcp(kp, k);
+                    else if (key_is_end(k))
+                        a.lcp[p] = s.depth + key_len(k);
+                }
+            }
+            if (same_prev && !key_is_end(k)) {
+                // a run of equal keys that do not end: is this its last record?
+                bool last = e == s.len - 1;
+                if (!last) {
+                    const uint64_t vn = sv[pad(e + 1)];
+                    last = ((v ^ vn) & ~POS_MASK) != 0 ||
+                           !key_eq(to_key(sk[kslot<PK>((uint32_t)(vn & POS_MASK))]), k);
+                }
+                if (last) {
+                    uint32_t lo = 0, hi = e;  // first position of this run
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        const uint32_t qm = kslot<PK>((uint32_t)(sv[pad(mid)] & POS_MASK));
+                        if (key_lt(to_key(sk[qm]), k))
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    want = true;
+                    run_lo = lo;
+                }
+            }
+        }
+        emit_next_warp(N, c, want, s.start + run_lo, e - run_lo + 1, s.depth + KEY_BYTES);
+    }
+}
+
 // True when the sorted order (through the packed keys) agrees with full
 // (key, index) order wherever the packed keys could not tell records apart
 // (equal windows).  Called by `threads` threads numbered t; per-thread verdict.
+template <bool PK = true>
 __device__ __forceinline__ bool window_pairs_ok_ind(const ulonglong2 *sk, const uint64_t *sv,
                                                     uint32_t len, uint32_t t, uint32_t threads) {
     bool ok = true;
     for (uint32_t e = t + 1; e < len; e += threads) {
         const uint64_t va = sv[pad(e - 1)], vb = sv[pad(e)];
         if ((va >> POS_BITS) == (vb >> POS_BITS)) {
-            const Key kp = to_key(sk[pad((uint32_t)(va & POS_MASK))]);
-            const Key k = to_key(sk[pad((uint32_t)(vb & POS_MASK))]);
+            const Key kp = to_key(sk[kslot<PK>((uint32_t)(va & POS_MASK))]);
+            const Key k = to_key(sk[kslot<PK>((uint32_t)(vb & POS_MASK))]);
             if (key_lt(k, kp)) ok = false;
         }
     }
@@ -540,6 +618,7 @@ __device__ __forceinline__ bool window_runs_short(const uint64_t *sv, uint32_t l
     return true;
 }
 
+template <bool PK = true>
 __device__ __forceinline__ void sort_window_runs(const ulonglong2 *sk, uint64_t *sv, uint32_t len,
                                                  uint32_t t, uint32_t threads) {
     for (uint32_t e = t; e + 1 < len; e += threads) {
@@ -549,11 +628,11 @@ __device__ __forceinline__ void sort_window_runs(const ulonglong2 *sk, uint64_t 
         while (r < len && (sv[pad(r)] >> POS_BITS) == w) ++r;
         for (uint32_t i = e + 1; i < r; ++i) {
             const uint64_t v = sv[pad(i)];
-            const Key kv = to_key(sk[pad((uint32_t)(v & POS_MASK))]);
+            const Key kv = to_key(sk[kslot<PK>((uint32_t)(v & POS_MASK))]);
             uint32_t j = i;
             while (j > e) {
                 const uint64_t u = sv[pad(j - 1)];
-                if (!key_lt(kv, to_key(sk[pad((uint32_t)(u & POS_MASK))]))) break;
+                if (!key_lt(kv, to_key(sk[kslot<PK>((uint32_t)(u & POS_MASK))]))) break;
                 sv[pad(j)] = u;
                 --j;
             }
@@ -599,9 +678,12 @@ __device__ __forceinline__ void append_small(const SmallLists &S, Counters *c, b
     if (c2) S.s[2][slot] = o;
 }
 
-__global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, uint32_t warp8_cap, Seg *W1,
+__global__ void k_classify(const Seg *__restrict__ R, Count cnt, uint32_t warp8_cap, Seg *W1,
                            Seg *W8, SmallLists S, Seg *L, Counters *c) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nR = count_of(cnt);
+    // Block-uniform trip count: every warp reaches the collective appends.
+    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < nR; b0 += gridDim.x * blockDim.x) {
+    const uint32_t i = b0 + threadIdx.x;
     const bool v = i < nR;
     const Seg s = v ? R[i] : Seg{0, 0, 0, 0};
     const bool w1 = v && s.len <= (uint32_t)WARP1_CAP;
@@ -620,6 +702,7 @@ __global__ void k_classify(const Seg *__restrict__ R, uint32_t nR, uint32_t warp
     if ((threadIdx.x & 31) == 0) {
         if (live) atomicAdd(&c->live_next, live);
         if (big) atomicAdd(&c->gather_elems, big);
+    }
     }
 }
 
@@ -909,8 +992,9 @@ __device__ __forceinline__ uint32_t cta_inclusive_scan(uint32_t v, uint32_t &tot
 __global__ void __launch_bounds__(SMALL_SCAN_THREADS) k_scan_pair(const uint32_t *__restrict__ in0,
                                                                    uint32_t *out0,
                                                                    const uint32_t *__restrict__ in1,
-                                                                   uint32_t *out1, uint32_t n) {
+                                                                   uint32_t *out1, Count cnt) {
     __shared__ uint32_t warp_sums[SMALL_SCAN_THREADS / 32];
+    const uint32_t n = count_of(cnt);
     uint32_t c0 = 0, c1 = 0;
     for (uint32_t b = 0; b < n; b += SMALL_SCAN_THREADS) {
         const uint32_t i = b + threadIdx.x;
@@ -933,9 +1017,10 @@ __global__ void __launch_bounds__(SMALL_SCAN_THREADS) k_scan_pair(const uint32_t
 
 // out = exclusive scan of ceil(len / tile) over the segments; out[n] = total.
 __global__ void __launch_bounds__(SMALL_SCAN_THREADS) k_seg_tiles(const Seg *__restrict__ segs,
-                                                                   uint32_t n, uint32_t tile,
+                                                                   Count cnt, uint32_t tile,
                                                                    uint32_t *out) {
     __shared__ uint32_t warp_sums[SMALL_SCAN_THREADS / 32];
+    const uint32_t n = count_of(cnt);
     uint32_t c = 0;
     for (uint32_t b = 0; b < n; b += SMALL_SCAN_THREADS) {
         const uint32_t i = b + threadIdx.x;
@@ -976,15 +1061,9 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &e
     return total;
 }
 
-__device__ __forceinline__ uint32_t scan_n(uint32_t n_host, const uint32_t *n_dev) {
-    return n_dev ? *n_dev : n_host;
-}
-
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t *__restrict__ in,
-                                                              uint32_t n_host,
-                                                              const uint32_t *n_dev,
-                                                              uint32_t *partials) {
-    const uint32_t n = scan_n(n_host, n_dev);
+                                                              Count cnt, uint32_t *partials) {
+    const uint32_t n = count_of(cnt);
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_CHUNK;
     uint32_t s = 0;
     if (base < n) {
@@ -1013,11 +1092,11 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_partials(uint32_t *partia
 }
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t *in, uint32_t *out,
-                                                            uint32_t n_host, const uint32_t *n_dev,
+                                                            Count cnt,
                                                             const uint32_t *__restrict__ partials,
                                                             uint32_t nparts) {
     __shared__ uint32_t buf[SCAN_CHUNK];
-    const uint32_t n = scan_n(n_host, n_dev);
+    const uint32_t n = count_of(cnt);
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_CHUNK;
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = partials[nparts];
     if (base >= n) return;
@@ -1048,9 +1127,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t *in, 
 
 // ---- key gather for large segments ----------------------------------------
 __global__ void __launch_bounds__(GATHER_THREADS) k_gather(SortArgs a, const Seg *__restrict__ L,
-                                                          uint32_t nL,
+                                                          Count cnt,
                                                           const uint32_t *__restrict__ tile_base,
                                                           Counters *ctr) {
+    const uint32_t nL = count_of(cnt);
     constexpr int U = GATHER_ITEMS;
     static_assert(GATHER_TILE % (GATHER_THREADS * GATHER_ITEMS) == 0, "tile shape");
     const uint32_t total_tiles = tile_base[nL] * (GATHER_TILE / (GATHER_THREADS * U));
@@ -1110,10 +1190,28 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
     return x;
 }
 
+__device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__restrict__ L,
+                                               uint32_t si, ulonglong2 *spl, uint32_t *nspl,
+                                               uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size,
+                                               bool from_arena);
+
+// One CTA per large segment at a time (segments si = blockIdx.x, + gridDim.x, ...).
 __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg *__restrict__ L,
-                                                           ulonglong2 *spl, uint32_t *nspl,
-                                                           uint16_t *tbl, uint32_t *ntiles,
-                                                           uint32_t *cm_size, bool from_arena) {
+                                                           Count cnt, ulonglong2 *spl,
+                                                           uint32_t *nspl, uint16_t *tbl,
+                                                           uint32_t *ntiles, uint32_t *cm_size,
+                                                           bool from_arena) {
+    const uint32_t nL = count_of(cnt);
+    for (uint32_t si = blockIdx.x; si < nL; si += gridDim.x) {
+        sample_segment(a, L, si, spl, nspl, tbl, ntiles, cm_size, from_arena);
+        __syncthreads();  // shared memory is reused by the next segment
+    }
+}
+
+__device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__restrict__ L,
+                                               uint32_t si, ulonglong2 *spl, uint32_t *nspl,
+                                               uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size,
+                                               bool from_arena) {
     // smp: SAMPLES_MAX keys; sv: their packed sort keys (padded layout)
     extern __shared__ __align__(16) unsigned char sample_smem[];
     ulonglong2 *smp = reinterpret_cast<ulonglong2 *>(sample_smem);
@@ -1121,7 +1219,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
     __shared__ ulonglong2 cands[SAMPLE_THREADS];
     __shared__ uint32_t warp_cnt[SAMPLE_THREADS / 32 + 1];
     __shared__ uint64_t red[2][SAMPLE_THREADS / 32];
-    const Seg s = L[blockIdx.x];
+    const Seg s = L[si];
     const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t k = (s.len + a.target_bucket - 1) / a.target_bucket;
@@ -1265,7 +1363,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
     }
     __syncthreads();
     const uint32_t u = warp_cnt[SAMPLE_THREADS / 32];
-    ulonglong2 *out = spl + (uint64_t)blockIdx.x * SPL_STRIDE;
+    ulonglong2 *out = spl + (uint64_t)si * SPL_STRIDE;
     if (keep) {
         const uint32_t pos = warp_cnt[w] + __popc(bal & lanemask_lt());
         out[pos] = from_key(cand);
@@ -1279,7 +1377,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
     const Key s0 = to_key(smp[0]), sl = to_key(smp[u - 1]);
     const uint32_t f = u >= 2 ? clz128(s0.hi ^ sl.hi, s0.lo ^ sl.lo) : 128u;
     if (f < 128) {
-        uint16_t *T = tbl + (uint64_t)blockIdx.x * TBL_STRIDE;
+        uint16_t *T = tbl + (uint64_t)si * TBL_STRIDE;
         for (uint32_t wv = threadIdx.x; wv <= (uint32_t)TBL_N; wv += SAMPLE_THREADS) {
             uint32_t lo = 0, hi = u;
             while (lo < hi) {
@@ -1293,10 +1391,10 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg
         }
     }
     if (threadIdx.x == 0) {
-        nspl[blockIdx.x] = u | (f << 16);
+        nspl[si] = u | (f << 16);
         const uint32_t nt = (s.len + PART_TILE - 1) / PART_TILE;
-        ntiles[blockIdx.x] = nt;
-        cm_size[blockIdx.x] = (2 * u + 1) * nt;
+        ntiles[si] = nt;
+        cm_size[si] = (2 * u + 1) * nt;
     }
 }
 
@@ -1329,7 +1427,7 @@ __device__ __forceinline__ void load_splitters(PartSmem &sm, const ulonglong2 *_
 // key gather's random arena reads overlap the classification work.
 template <bool GATHER>
 __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg *__restrict__ L,
-                                                        uint32_t nL,
+                                                        Count cnt,
                                                         const uint32_t *__restrict__ tile_base,
                                                         const ulonglong2 *__restrict__ spl,
                                                         const uint32_t *__restrict__ nspl,
@@ -1341,6 +1439,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
     auto &hist = sm.cnt;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr int SUB = PART_TILE / PART_WARPS;
+    const uint32_t nL = count_of(cnt);
     const uint32_t total_tiles = tile_base[nL];
     const uint32_t lt = lanemask_lt();
     uint32_t loaded = ~0u;
@@ -1471,7 +1570,7 @@ struct ScatterSmem {
 };
 
 __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const Seg *__restrict__ L,
-                                                             uint32_t nL,
+                                                             Count cnt,
                                                              const uint32_t *__restrict__ tile_base,
                                                              const uint32_t *__restrict__ nspl,
                                                              const uint32_t *__restrict__ cm_base,
@@ -1480,6 +1579,7 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
     ScatterSmem &sm = *reinterpret_cast<ScatterSmem *>(scatter_smem);
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr uint32_t QPT = (NB_MAX + 1) / SCATTER_THREADS;  // buckets per thread (4)
+    const uint32_t nL = count_of(cnt);
     const uint32_t total_tiles = tile_base[nL];
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
@@ -1565,11 +1665,13 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
 }
 
 // ---- bucket emission: one CTA per partitioned segment ----------------------
-__global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__restrict__ tile_base,
+__global__ void k_emit(SortArgs a, const Seg *__restrict__ L, Count cnt,
+                       const uint32_t *__restrict__ tile_base,
                        const uint32_t *__restrict__ nspl, const uint32_t *__restrict__ cm_base,
                        const uint32_t *__restrict__ cm_scan, Seg *W1, Seg *W8, SmallLists S,
                        Seg *L2, Seg *E, uint2 *B, Seg *N, Counters *c) {
-    const uint32_t si = blockIdx.x;
+    const uint32_t nL = count_of(cnt);
+    for (uint32_t si = blockIdx.x; si < nL; si += gridDim.x) {
     const Seg s = L[si];
     const uint32_t u = nspl[si] & 0xFFFF, nb = 2 * u + 1;
     const uint32_t nt = tile_base[si + 1] - tile_base[si];
@@ -1635,6 +1737,7 @@ __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, const uint32_t *__
         if (lg) L2[slot] = o;
     }
     if (threadIdx.x == 0) atomicAdd(&c->partitioned, (unsigned long long)s.len);
+    }
 }
 
 // ---- segments of <= 32 strings: one warp, one string per lane -------------
@@ -1928,8 +2031,11 @@ __device__ __forceinline__ uint32_t warp1_group(const SortArgs &a, const Seg &s,
 // remaining segment.
 constexpr uint32_t W1_PACK = 4;
 
-__global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *__restrict__ T,
-                                                        uint32_t nT, Seg *N, Counters *c) {
+__global__ void __launch_bounds__(WARP_THREADS) k_warp1(SortArgs a, const Seg *__restrict__ T0,
+                                                        Span sp, Seg *N, Counters *c) {
+    const uint32_t lo = count_of(sp.lo);
+    const Seg *__restrict__ T = T0 + lo;
+    const uint32_t nT = count_of(sp.hi) - lo;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1983,8 +2089,11 @@ constexpr int W8_WARPS = WARP_THREADS / 32;
 constexpr size_t W8_SMEM = (size_t)W8_WARPS * W8_PAD * (sizeof(ulonglong2) + sizeof(uint64_t) +
                                                          sizeof(uint32_t));
 
-__global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg *__restrict__ T,
-                                                           uint32_t nT, Seg *N, Counters *c) {
+__global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg *__restrict__ T0,
+                                                           Span sp, Seg *N, Counters *c) {
+    const uint32_t lo = count_of(sp.lo);
+    const Seg *__restrict__ T = T0 + lo;
+    const uint32_t nT = count_of(sp.hi) - lo;
     extern __shared__ __align__(16) unsigned char w8_smem[];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     ulonglong2 *sk = reinterpret_cast<ulonglong2 *>(w8_smem) + w * W8_PAD;
@@ -2093,12 +2202,12 @@ __device__ __forceinline__ void group_sync(uint32_t gi) {
 // Full-comparator sort of the span (multiple of BLOCK_RUN) records at padded
 // positions 0..span-1 by the GT threads of a group (thread t): warp runs, then
 // pairwise merge-path merges.
-template <int GT>
+template <int GT, bool PK = true>
 __device__ __noinline__ void group_sort_full(ulonglong2 *sk, uint32_t *sx, uint32_t span,
                                              uint32_t t, uint32_t gi) {
     const uint32_t nruns = span / BLOCK_RUN;
     const uint32_t lane = t & 31, gw = t >> 5;
-    if (gw < nruns) warp_sort_run<SMALL_ITEMS>(sk, sx, gw * BLOCK_RUN, lane);
+    if (gw < nruns) warp_sort_run<SMALL_ITEMS, PK>(sk, sx, gw * BLOCK_RUN, lane);
     group_sync<GT>(gi);
     for (uint32_t run = BLOCK_RUN; run < span; run <<= 1) {
         const uint32_t o = t * SMALL_ITEMS;
@@ -2111,7 +2220,7 @@ __device__ __noinline__ void group_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
             const uint32_t la = min(run, span - a0);
             const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
             const uint32_t d = o - a0;
-            uint32_t ia = merge_split(sk, sx, a0, la, b0, lb, d);
+            uint32_t ia = merge_split<PK>(sk, sx, a0, la, b0, lb, d);
             uint32_t ib = d - ia;
 #pragma unroll
             for (int i = 0; i < SMALL_ITEMS; ++i) {
@@ -2119,12 +2228,12 @@ __device__ __noinline__ void group_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
                 Key ka, kb;
                 uint32_t xa = 0, xb = 0;
                 if (ia < la) {
-                    ka = to_key(sk[pad(a0 + ia)]);
-                    xa = sx[pad(a0 + ia)];
+                    ka = to_key(sk[kslot<PK>(a0 + ia)]);
+                    xa = sx[kslot<PK>(a0 + ia)];
                 }
                 if (ib < lb) {
-                    kb = to_key(sk[pad(b0 + ib)]);
-                    xb = sx[pad(b0 + ib)];
+                    kb = to_key(sk[kslot<PK>(b0 + ib)]);
+                    xb = sx[kslot<PK>(b0 + ib)];
                     if (ia < la) take_a = !pair_lt(kb, xb, ka, xa);
                 }
                 if (take_a) {
@@ -2142,8 +2251,8 @@ __device__ __noinline__ void group_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
         if (active) {
 #pragma unroll
             for (int i = 0; i < SMALL_ITEMS; ++i) {
-                sk[pad(o + i)] = from_key(ok[i]);
-                sx[pad(o + i)] = ox[i];
+                sk[kslot<PK>(o + i)] = from_key(ok[i]);
+                sx[kslot<PK>(o + i)] = ox[i];
             }
         }
         group_sync<GT>(gi);
@@ -2304,12 +2413,212 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
 // three bodies and spills more; measured slower).
 template <int GT>
 __global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
-                                                            uint32_t nS, Seg *N, Counters *c) {
-    block_class<GT>(a, S, nS, 0, gridDim.x, N, c);
+                                                            Span sp, Seg *N, Counters *c) {
+    const uint32_t lo = count_of(sp.lo);
+    block_class<GT>(a, S + lo, count_of(sp.hi) - lo, 0, gridDim.x, N, c);
+}
+
+// ---- segments of 257..SMALL_CAP strings, with the next segment prefetched ---
+// The same thread groups and sort as k_block, but a group's records (16-byte
+// key, index) of a keyed segment reach shared memory through cp.async (global
+// -> shared copies that bypass the registers), issued for the group's NEXT
+// segment before it sorts the current one, so that the copy runs under the
+// sort.  Two record buffers per group (contiguous slots: the copies cannot
+// write the padded layout); the packed keys are built from the records
+// loaded once into registers.  Segments without keys at their depth (fresh)
+// are gathered by the group's threads as in k_block.
+constexpr size_t BLOCK2_SMEM =
+    2 * (size_t)SMALL_CAP * (sizeof(ulonglong2) + sizeof(uint32_t)) + SMALL_PAD * sizeof(uint64_t);
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// Waits until at most N of this thread's committed copy groups are pending.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int GT>
+__device__ __forceinline__ void block2_class(const SortArgs &a, const Seg *__restrict__ S,
+                                             uint32_t nS, Seg *N, Counters *c) {
+    constexpr uint32_t G = SMALL_THREADS / GT;  // groups per CTA
+    constexpr uint32_t CAP = GT * SMALL_ITEMS;  // strings per group
+    constexpr uint32_t PADC = CAP + CAP / 8;    // padded packed-key slots per group
+    static_assert(G * PADC == SMALL_PAD, "group slots");
+    extern __shared__ __align__(16) unsigned char block_smem[];
+    __shared__ uint64_t red[2][SMALL_THREADS / 32];
+    __shared__ int ok_flag[G], fix_flag[G];
+    const uint32_t gi = threadIdx.x / GT, t = threadIdx.x % GT;
+    const uint32_t lane = threadIdx.x & 31, gw = t >> 5, w = threadIdx.x >> 5;
+    ulonglong2 *rk_all = reinterpret_cast<ulonglong2 *>(block_smem);  // [2][SMALL_CAP]
+    uint32_t *rx_all = reinterpret_cast<uint32_t *>(rk_all + 2 * SMALL_CAP);
+    uint64_t *sv = reinterpret_cast<uint64_t *>(rx_all + 2 * SMALL_CAP) + gi * PADC;
+    unsigned long long fresh = 0, keyed = 0, full = 0;
+    const uint32_t stride = gridDim.x * G;
+    // Copies of a keyed segment's records into record buffer `buf`; every
+    // thread commits one copy group per call (empty when there is nothing).
+    auto prefetch = [&](const Seg &q, uint32_t buf) {
+        if (q.len && (q.flags & SEG_KEYS)) {
+            const int b = q.flags & SEG_BUF1;
+            const ulonglong2 *K = a.keyb(b) + q.start;
+            const uint32_t *I = a.idxb(b) + q.start;
+            ulonglong2 *dk = rk_all + buf * SMALL_CAP + gi * CAP;
+            uint32_t *dx = rx_all + buf * SMALL_CAP + gi * CAP;
+#pragma unroll
+            for (int cc = 0; cc < SMALL_ITEMS; ++cc) {
+                const uint32_t e = t + cc * GT;
+                if (e < q.len) {
+                    cp_async16(dk + e, K + e);
+                    cp_async4(dx + e, I + e);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    const Seg none{0, 0, 0, 0};
+    uint32_t g = blockIdx.x * G + gi;
+    Seg s_cur = g < nS ? S[g] : none;
+    Seg s_nxt = g + stride < nS ? S[g + stride] : none;
+    prefetch(s_cur, 0);
+    uint32_t cb = 0;
+    for (; g < nS; g += stride, cb ^= 1) {
+        const Seg s = s_cur;
+        prefetch(s_nxt, cb ^ 1);
+        s_cur = s_nxt;
+        s_nxt = g + 2 * stride < nS ? S[g + 2 * stride] : none;
+        ulonglong2 *sk = rk_all + cb * SMALL_CAP + gi * CAP;
+        uint32_t *sx = rx_all + cb * SMALL_CAP + gi * CAP;
+        if (s.flags & SEG_KEYS) {
+            keyed += s.len;
+        } else {
+            fresh += s.len;
+            // Gather at this depth: all of a thread's loads first.
+            Key kk[SMALL_ITEMS];
+            uint32_t ii[SMALL_ITEMS];
+#pragma unroll
+            for (int cc = 0; cc < SMALL_ITEMS; ++cc) {
+                const uint32_t e = t + cc * GT;
+                if (e < s.len) load_elem(a, s, e, kk[cc], ii[cc]);
+            }
+#pragma unroll
+            for (int cc = 0; cc < SMALL_ITEMS; ++cc) {
+                const uint32_t e = t + cc * GT;
+                if (e < s.len) {
+                    sk[e] = from_key(kk[cc]);
+                    sx[e] = ii[cc];
+                }
+            }
+        }
+        cp_async_wait<1>();  // this segment's copies (the next one's may run on)
+        if (t == 0) ok_flag[gi] = fix_flag[gi] = 1;
+        group_sync<GT>(gi);
+        // f: first bit in which the keys differ (thread t's records are
+        // t, t + GT, ...; contiguous across threads, so no bank conflicts).
+        {
+            const Key k0 = to_key(sk[0]);
+            uint64_t dh = 0, dl = 0;
+#pragma unroll
+            for (int cc = 0; cc < SMALL_ITEMS; ++cc) {
+                const uint32_t e = t + cc * GT;
+                if (e < s.len) {
+                    const Key k = to_key(sk[e]);
+                    dh |= k.hi ^ k0.hi;
+                    dl |= k.lo ^ k0.lo;
+                }
+            }
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                dh |= __shfl_xor_sync(0xffffffffu, dh, d);
+                dl |= __shfl_xor_sync(0xffffffffu, dl, d);
+            }
+            if (lane == 0) {
+                red[0][w] = dh;
+                red[1][w] = dl;
+            }
+        }
+        group_sync<GT>(gi);
+        uint64_t dh = 0, dl = 0;
+#pragma unroll
+        for (uint32_t q = 0; q < GT / 32; ++q) {
+            dh |= red[0][gi * (GT / 32) + q];
+            dl |= red[1][gi * (GT / 32) + q];
+        }
+        bool packed = false;
+        const uint32_t f = (dh | dl) ? clz128(dh, dl) : 128u;
+        if (f < 128) {
+            // Every warp of the group sorts the packed keys of its own
+            // records (t, t + GT, ...; any split of the records works: the
+            // position in the low bits identifies each one); positions past
+            // the end pad as distinct values above every real one.
+            uint64_t v[SMALL_ITEMS];
+#pragma unroll
+            for (int cc = 0; cc < SMALL_ITEMS; ++cc) {
+                const uint32_t e = t + cc * GT;
+                v[cc] = e < s.len ? sort_key(to_key(sk[e]), f, e) : ((~0ull << POS_BITS) | e);
+            }
+            warp_bitonic64<SMALL_ITEMS>(v, lane);
+#pragma unroll
+            for (int i = 0; i < SMALL_ITEMS; ++i) sv[pad(gw * BLOCK_RUN + lane * SMALL_ITEMS + i)] = v[i];
+            group_sync<GT>(gi);
+            group_merge_passes64<GT>(sv, CAP, t, gi);
+            if (!window_pairs_ok_ind<false>(sk, sv, s.len, t, GT)) ok_flag[gi] = 0;
+            group_sync<GT>(gi);
+            packed = ok_flag[gi] != 0;
+            if (!packed) {
+                if (!window_runs_short(sv, s.len, t, GT)) fix_flag[gi] = 0;
+                group_sync<GT>(gi);
+                packed = fix_flag[gi] != 0;
+                if (packed) {
+                    sort_window_runs<false>(sk, sv, s.len, t, GT);
+                } else {
+                    // Full comparator over the whole group span (rare): the
+                    // slots past the end sort last.
+                    for (uint32_t e = s.len + t; e < CAP; e += GT) {
+                        sk[e] = from_key(key_max());
+                        sx[e] = IDX_MAX;
+                    }
+                    group_sync<GT>(gi);
+                    if (t == 0) full += s.len;
+                    group_sort_full<GT, false>(sk, sx, CAP, t, gi);
+                }
+            }
+        }
+        group_sync<GT>(gi);
+        if (packed)
+            finish_packed<false>(a, s, sk, sx, sv, f, t, GT, N, c);
+        else
+            finish_segment<false, false>(a, s, sk, sx, sv, t, GT, N, c);
+        group_sync<GT>(gi);
+    }
+    cp_async_wait<0>();
+    if (t == 0 && (fresh | keyed)) {
+        atomicAdd(&c->block_fresh, fresh);
+        atomicAdd(&c->block_keyed, keyed);
+        if (full) atomicAdd(&c->full_sorted, full);
+    }
+}
+
+template <int GT>
+__global__ void __launch_bounds__(SMALL_THREADS, 2) k_block2(SortArgs a, const Seg *__restrict__ S,
+                                                             Span sp, Seg *N, Counters *c) {
+    const uint32_t lo = count_of(sp.lo);
+    block2_class<GT>(a, S + lo, count_of(sp.hi) - lo, N, c);
 }
 
 // ---- equality buckets: work items of up to EQ_TILE strings ------------------
-__global__ void k_equal(SortArgs a, const Seg *__restrict__ E, uint32_t nE, Seg *N, Counters *c) {
+__global__ void k_equal(SortArgs a, const Seg *__restrict__ E0, Span sp, Seg *N, Counters *c) {
+    const uint32_t lo = count_of(sp.lo);
+    const Seg *__restrict__ E = E0 + lo;
+    const uint32_t nE = count_of(sp.hi) - lo;
     unsigned long long moved = 0, fin = 0;
     for (uint32_t g = blockIdx.x; g < nE; g += gridDim.x) {
         const Seg s = E[g];
@@ -2349,6 +2658,122 @@ __global__ void k_boundary(SortArgs a, const uint2 *__restrict__ B, Counters *c)
     }
 }
 
+// ---- control kernels of the device-driven round loop --------------------------
+// The graph's loops (rounds, partition levels) and branches (separate gather,
+// gathering count) are CUDA graph conditional nodes; these kernels read the
+// device counters and set their conditions, so no host round trip is needed
+// between launches.  None of them waits on another block: the multi-CTA ones
+// copy a list and let the last CTA to finish (atomic ticket) do the update.
+
+// Each loop body first clears its own condition, and only the kernel that
+// ends the body sets it again when another iteration is due: a body whose
+// last kernel did not run cannot repeat.
+__global__ void k_g_round_begin(GraphState *g, Counters *c, cudaGraphConditionalHandle h_round) {
+    uint32_t *w = reinterpret_cast<uint32_t *>(c);
+    for (uint32_t i = threadIdx.x; i < sizeof(Counters) / 4; i += blockDim.x) w[i] = 0;
+    if (threadIdx.x == 0) {
+        cudaGraphSetConditional(h_round, 0u);
+        g->cur_w1 = g->cur_w8 = g->cur_e = 0;
+        g->cur_s[0] = g->cur_s[1] = g->cur_s[2] = 0;
+        g->levels = 0;
+    }
+}
+
+__global__ void k_g_after_classify(GraphState *g, const Counters *c,
+                                   cudaGraphConditionalHandle h_level,
+                                   cudaGraphConditionalHandle h_gather) {
+    if (threadIdx.x != 0) return;
+    const uint32_t nl = c->n_large;
+    g->n_large = nl;
+    g->levels = 0;
+    if (g->round < 64) g->live[g->round] = c->live_next;
+    const bool fresh = g->round == 0;
+    // Round 0 streams the arena in index order with a separate gather; later
+    // rounds gather inside the first level's count unless that is switched off.
+    g->first = (!fresh && g->fused) ? 1u : 0u;
+    cudaGraphSetConditional(h_gather, (nl > 0 && (fresh || !g->fused)) ? 1u : 0u);
+    cudaGraphSetConditional(h_level, nl > 0 ? 1u : 0u);
+}
+
+__global__ void k_g_level_begin(const GraphState *g, cudaGraphConditionalHandle h_level,
+                                cudaGraphConditionalHandle h_first) {
+    if (threadIdx.x != 0) return;
+    cudaGraphSetConditional(h_level, 0u);
+    cudaGraphSetConditional(h_first, g->first ? 1u : 0u);
+}
+
+// True in thread 0 of the last CTA of the grid to get here (after its own
+// writes are visible); that CTA resets the ticket for the next launch.
+__device__ __forceinline__ bool last_cta(uint32_t *ticket) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return false;
+    __threadfence();
+    *ticket = 0;
+    return true;
+}
+
+__global__ void k_g_level_end(GraphState *g, Counters *c, Seg *L, const Seg *__restrict__ L2,
+                              cudaGraphConditionalHandle h_level) {
+    const uint32_t n = c->n_large_next;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        L[i] = L2[i];
+    if (!last_cta(&g->ticket)) return;
+    g->n_large = n;
+    c->n_large_next = 0;
+    g->first = 0;
+    g->levels += 1;
+    g->partition_levels += 1;
+    g->cur_w1 = c->n_w1;
+    g->cur_w8 = c->n_w8;
+    g->cur_s[0] = c->n_small;
+    g->cur_s[1] = c->n_small2;
+    g->cur_s[2] = c->n_small3;
+    g->cur_e = c->n_equal;
+    bool more = n > 0;
+    if (more && g->levels >= g->max_levels) {
+        g->error = 1;  // reported by the host as an internal error, not a hang
+        more = false;
+    }
+    cudaGraphSetConditional(h_level, more ? 1u : 0u);
+}
+
+__global__ void k_g_round_end(GraphState *g, const Counters *c, Seg *R, const Seg *__restrict__ N,
+                              cudaGraphConditionalHandle h_round) {
+    const uint32_t n = c->n_next;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        R[i] = N[i];
+    if (!last_cta(&g->ticket)) return;
+    const bool fused = g->round > 0 && g->fused;
+    g->small_segments += (unsigned long long)c->n_w1 + c->n_w8 + c->n_small + c->n_small2 +
+                         c->n_small3;
+    g->partitioned += c->partitioned;
+    g->gather_elems += c->gather_elems;
+    if (fused) g->gather_fused += c->gather_elems;
+    g->warp1_fresh += c->warp1_fresh;
+    g->warp1_keyed += c->warp1_keyed;
+    g->warp8_fresh += c->warp8_fresh;
+    g->warp8_keyed += c->warp8_keyed;
+    g->block_fresh += c->block_fresh;
+    g->block_keyed += c->block_keyed;
+    g->equal_moved += c->equal_moved;
+    g->equal_final += c->equal_final;
+    g->boundaries += c->n_bound;
+    g->warp1_deep += c->warp1_deep;
+    g->full_sorted += c->full_sorted;
+    g->window_saved += c->window_saved;
+    g->window_used += c->window_used;
+    g->n_cur = n;
+    g->round += 1;
+    g->round_in_launch += 1;
+    g->done = n == 0 ? 1u : 0u;
+    const bool more = n > 0 && !g->error && g->round_in_launch < GRAPH_ROUNDS_PER_LAUNCH;
+    cudaGraphSetConditional(h_round, more ? 1u : 0u);
+}
+
 }  // namespace
 
 // ---- launchers --------------------------------------------------------------
@@ -2380,6 +2805,12 @@ static void set_smem_attrs() {
                          (int)BLOCK_SMEM);
     cudaFuncSetAttribute(k_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block2<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK2_SMEM);
+    cudaFuncSetAttribute(k_block2<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK2_SMEM);
+    cudaFuncSetAttribute(k_block2<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK2_SMEM);
     done.fetch_or(bit, std::memory_order_release);
 }
 
@@ -2388,10 +2819,20 @@ void launch_iota(uint32_t *idx, uint32_t n, cudaStream_t st) {
     k_iota<<<g ? g : 1, 256, 0, st>>>(idx, n);
 }
 
-void launch_classify(const Seg *R, uint32_t nR, uint32_t warp8_cap, Seg *W1, Seg *W8,
-                     SmallLists S, Seg *L, Counters *c, cudaStream_t st) {
-    if (!nR) return;
-    k_classify<<<cdiv(nR, 256), 256, 0, st>>>(R, nR, warp8_cap, W1, W8, S, L, c);
+// Grid for a launcher given `grid` (> 0: as given) or a host count of work
+// units of `per` each (capped at cap CTAs; 0 when there is no work).
+static int grid_of(int grid, const Count &n, uint32_t per, uint32_t cap) {
+    if (grid > 0) return grid;
+    if (n.dev) return (int)cap;
+    const uint32_t g = cdiv(n.host, per);
+    return (int)(g < cap ? g : cap);
+}
+
+void launch_classify(const Seg *R, Count nR, uint32_t warp8_cap, Seg *W1, Seg *W8,
+                     SmallLists S, Seg *L, Counters *c, int grid, cudaStream_t st) {
+    const int g = grid_of(grid, nR, 256, 1u << 30);
+    if (!g) return;
+    k_classify<<<g, 256, 0, st>>>(R, nR, warp8_cap, W1, W8, S, L, c);
 }
 
 void launch_init_batch(const uint32_t *inst_start, uint32_t ninst, Seg *R, uint32_t *lcp,
@@ -2460,44 +2901,45 @@ void launch_byte_hist(const uint8_t *arena, uint64_t arena_bytes, const void *of
 }
 
 void launch_scan_pair(const uint32_t *in0, uint32_t *out0, const uint32_t *in1, uint32_t *out1,
-                      uint32_t n, cudaStream_t st) {
+                      Count n, cudaStream_t st) {
     k_scan_pair<<<1, SMALL_SCAN_THREADS, 0, st>>>(in0, out0, in1, out1, n);
 }
 
-void launch_seg_tiles(const Seg *segs, uint32_t n, uint32_t tile, uint32_t *out, cudaStream_t st) {
+void launch_seg_tiles(const Seg *segs, Count n, uint32_t tile, uint32_t *out, cudaStream_t st) {
     k_seg_tiles<<<1, SMALL_SCAN_THREADS, 0, st>>>(segs, n, tile, out);
 }
 
 uint32_t scan_partials_needed(uint32_t n) { return cdiv(n ? n : 1, SCAN_CHUNK) + 1; }
 
-void launch_scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
-                 uint32_t *partials, cudaStream_t st) {
-    const uint32_t nb = cdiv(n_host ? n_host : 1, SCAN_CHUNK);
-    k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(in, n_host, n_dev, partials);
+void launch_scan(const uint32_t *in, uint32_t *out, uint32_t cap, Count n, uint32_t *partials,
+                 cudaStream_t st) {
+    const uint32_t nb = cdiv(cap ? cap : 1, SCAN_CHUNK);
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(in, n, partials);
     k_scan_partials<<<1, SCAN_THREADS, 0, st>>>(partials, nb);
-    k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(in, out, n_host, n_dev, partials, nb);
+    k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(in, out, n, partials, nb);
 }
 
-void launch_gather(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+void launch_gather(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                    Counters *c, int grid, cudaStream_t st) {
-    if (!nL) return;
+    if (!nL.dev && !nL.host) return;
     k_gather<<<grid, GATHER_THREADS, 0, st>>>(a, L, nL, tile_base, c);
 }
 
-void launch_sample(const SortArgs &a, const Seg *L, uint32_t nL, ulonglong2 *spl, uint32_t *nspl,
-                   uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size, bool from_arena,
+void launch_sample(const SortArgs &a, const Seg *L, Count nL, ulonglong2 *spl, uint32_t *nspl,
+                   uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size, bool from_arena, int grid,
                    cudaStream_t st) {
-    if (!nL) return;
+    const int g = grid_of(grid, nL, 1, 1u << 30);
+    if (!g) return;
     set_smem_attrs();
-    k_sample<<<nL, SAMPLE_THREADS, SAMPLE_SMEM, st>>>(a, L, spl, nspl, tbl, ntiles, cm_size,
-                                                      from_arena);
+    k_sample<<<g, SAMPLE_THREADS, SAMPLE_SMEM, st>>>(a, L, nL, spl, nspl, tbl, ntiles, cm_size,
+                                                     from_arena);
 }
 
-void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+void launch_count(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                   const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
                   const uint32_t *cm_base, uint32_t *cm, Counters *c, bool gather, int grid,
                   cudaStream_t st) {
-    if (!nL) return;
+    if (!nL.dev && !nL.host) return;
     set_smem_attrs();
     if (gather)
         k_count<true><<<grid, PART_THREADS, sizeof(PartSmem), st>>>(a, L, nL, tile_base, spl, nspl,
@@ -2507,57 +2949,99 @@ void launch_count(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *
                                                                      nspl, tbl, cm_base, cm, c);
 }
 
-void launch_scatter(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+void launch_scatter(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                     const ulonglong2 *spl, const uint32_t *nspl, const uint16_t *tbl,
                     const uint32_t *cm_base, const uint32_t *cm_scan, int grid, cudaStream_t st) {
-    if (!nL) return;
+    if (!nL.dev && !nL.host) return;
     set_smem_attrs();
     k_scatter<<<grid, SCATTER_THREADS, sizeof(ScatterSmem), st>>>(a, L, nL, tile_base, nspl,
                                                                   cm_base, cm_scan);
 }
 
-void launch_emit(const SortArgs &a, const Seg *L, uint32_t nL, const uint32_t *tile_base,
+void launch_emit(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                  const uint32_t *nspl, const uint32_t *cm_base, const uint32_t *cm_scan,
                  Seg *W1, Seg *W8, SmallLists S, Seg *L2, Seg *E, uint2 *B, Seg *N,
-                 Counters *c, cudaStream_t st) {
-    if (!nL) return;
-    k_emit<<<nL, 256, 0, st>>>(a, L, tile_base, nspl, cm_base, cm_scan, W1, W8, S, L2, E, B, N,
-                               c);
+                 Counters *c, int grid, cudaStream_t st) {
+    const int g = grid_of(grid, nL, 1, 1u << 30);
+    if (!g) return;
+    k_emit<<<g, 256, 0, st>>>(a, L, nL, tile_base, nspl, cm_base, cm_scan, W1, W8, S, L2, E, B,
+                              N, c);
 }
 
-void launch_warp1(const SortArgs &a, const Seg *W1, uint32_t n, Seg *N, Counters *c, int grid,
+// A span with host bounds and nothing in it launches nothing.
+static bool span_empty(const Span &sp) {
+    return !sp.lo.dev && !sp.hi.dev && sp.hi.host <= sp.lo.host;
+}
+
+void launch_warp1(const SortArgs &a, const Seg *W1, Span sp, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
-    if (!n) return;
-    k_warp1<<<grid, WARP_THREADS, 0, st>>>(a, W1, n, N, c);
+    if (span_empty(sp) || grid <= 0) return;
+    k_warp1<<<grid, WARP_THREADS, 0, st>>>(a, W1, sp, N, c);
 }
 
-void launch_warp8(const SortArgs &a, const Seg *W8, uint32_t n, Seg *N, Counters *c, int grid,
+void launch_warp8(const SortArgs &a, const Seg *W8, Span sp, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
-    if (!n) return;
+    if (span_empty(sp) || grid <= 0) return;
     set_smem_attrs();
-    k_warp8<<<grid, WARP_THREADS, W8_SMEM, st>>>(a, W8, n, N, c);
+    k_warp8<<<grid, WARP_THREADS, W8_SMEM, st>>>(a, W8, sp, N, c);
 }
 
-void launch_block(const SortArgs &a, const Seg *S, uint32_t n, int cls, Seg *N, Counters *c,
-                  int grid, cudaStream_t st) {
-    if (!n) return;
+void launch_block(const SortArgs &a, const Seg *S, Span sp, int cls, Seg *N, Counters *c,
+                  int grid, cudaStream_t st, bool prefetch) {
+    if (span_empty(sp) || grid <= 0) return;
     set_smem_attrs();
+    if (prefetch) {
+        if (cls == 0)
+            k_block2<64><<<grid, SMALL_THREADS, BLOCK2_SMEM, st>>>(a, S, sp, N, c);
+        else if (cls == 1)
+            k_block2<128><<<grid, SMALL_THREADS, BLOCK2_SMEM, st>>>(a, S, sp, N, c);
+        else
+            k_block2<256><<<grid, SMALL_THREADS, BLOCK2_SMEM, st>>>(a, S, sp, N, c);
+        return;
+    }
     if (cls == 0)
-        k_block<64><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, n, N, c);
+        k_block<64><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
     else if (cls == 1)
-        k_block<128><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, n, N, c);
+        k_block<128><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
     else
-        k_block<256><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, n, N, c);
+        k_block<256><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
 }
 
-void launch_equal(const SortArgs &a, const Seg *E, uint32_t n, Seg *N, Counters *c, int grid,
+void launch_equal(const SortArgs &a, const Seg *E, Span sp, Seg *N, Counters *c, int grid,
                   cudaStream_t st) {
-    if (!n) return;
-    k_equal<<<grid, 256, 0, st>>>(a, E, n, N, c);
+    if (span_empty(sp) || grid <= 0) return;
+    k_equal<<<grid, 256, 0, st>>>(a, E, sp, N, c);
 }
 
 void launch_boundary(const SortArgs &a, const uint2 *B, Counters *c, int grid, cudaStream_t st) {
     k_boundary<<<grid, 256, 0, st>>>(a, B, c);
+}
+
+void launch_g_round_begin(GraphState *g, Counters *c, unsigned long long h_round,
+                          cudaStream_t st) {
+    k_g_round_begin<<<1, 128, 0, st>>>(g, c, (cudaGraphConditionalHandle)h_round);
+}
+
+void launch_g_after_classify(GraphState *g, Counters *c, unsigned long long h_level,
+                             unsigned long long h_gather, cudaStream_t st) {
+    k_g_after_classify<<<1, 32, 0, st>>>(g, c, (cudaGraphConditionalHandle)h_level,
+                                         (cudaGraphConditionalHandle)h_gather);
+}
+
+void launch_g_level_begin(GraphState *g, unsigned long long h_level, unsigned long long h_first,
+                          cudaStream_t st) {
+    k_g_level_begin<<<1, 32, 0, st>>>(g, (cudaGraphConditionalHandle)h_level,
+                                      (cudaGraphConditionalHandle)h_first);
+}
+
+void launch_g_level_end(GraphState *g, Counters *c, Seg *L, const Seg *L2,
+                        unsigned long long h_level, int grid, cudaStream_t st) {
+    k_g_level_end<<<grid, 256, 0, st>>>(g, c, L, L2, (cudaGraphConditionalHandle)h_level);
+}
+
+void launch_g_round_end(GraphState *g, Counters *c, Seg *R, const Seg *N,
+                        unsigned long long h_round, int grid, cudaStream_t st) {
+    k_g_round_end<<<grid, 256, 0, st>>>(g, c, R, N, (cudaGraphConditionalHandle)h_round);
 }
 
 }  // namespace ssort

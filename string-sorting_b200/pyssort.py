@@ -37,6 +37,9 @@ SSORT_PARAM_WARP8_CAP = 2
 SSORT_PARAM_OVERLAP = 3
 SSORT_PARAM_FUSED_GATHER = 4
 SSORT_PARAM_WARP1_DEEP = 5
+SSORT_PARAM_BLOCK_PREFETCH = 6
+SSORT_PARAM_GRAPH = 7
+SSORT_PARAM_GRAPH_MAX_LEVELS = 8
 
 
 class SsortError(RuntimeError):

@@ -23,6 +23,8 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_WARP1_DEEP, 0),
     (pyssort.SSORT_PARAM_WARP1_DEEP, 1),
     (pyssort.SSORT_PARAM_WARP1_DEEP, 4096),
+    (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 0),
+    (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 1),
 ]
 
 
@@ -76,6 +78,7 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_TARGET_BUCKET, 4096),
                              (pyssort.SSORT_PARAM_WARP1_DEEP, -1),
                              (pyssort.SSORT_PARAM_WARP1_DEEP, 4097),
+                             (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 2),
                              (99, 1)]:
             with pytest.raises(pyssort.SsortError) as e:
                 s.set_param(param, value)
