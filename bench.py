@@ -40,7 +40,9 @@ PARAMS = {"target_bucket": pyssort.SSORT_PARAM_TARGET_BUCKET,
           "fused_gather": pyssort.SSORT_PARAM_FUSED_GATHER,
           "warp1_deep": pyssort.SSORT_PARAM_WARP1_DEEP,
           "block_prefetch": pyssort.SSORT_PARAM_BLOCK_PREFETCH,
-          "graph": pyssort.SSORT_PARAM_GRAPH}
+          "graph": pyssort.SSORT_PARAM_GRAPH,
+          "l2_prefetch": pyssort.SSORT_PARAM_L2_PREFETCH,
+          "digit_bits": pyssort.SSORT_PARAM_DIGIT_BITS}
 
 
 def apply_params(sorter, args):
@@ -84,9 +86,9 @@ DESCRIPTIONS = {
                      "2,000 copies of earlier passages of log-uniform length in [32, 4096] "
                      "bytes; uint32 offsets",
     "serve_c5": "Poisson request stream swept over 1k-50k req/s; request string counts "
-                "log-uniform in [1,000, 5,000,000], strings as batch_c4; requests drawn from a "
-                "pool of distinct requests in pinned host memory; uint32 offsets; 120 GB arena "
-                "budget",
+                "log-uniform in [1,000, 5,000,000], strings as batch_c4; every request a "
+                "distinct, freshly generated one (generated before the sweep, in pinned host "
+                "memory); uint32 offsets; 120 GB arena budget",
 }
 
 
@@ -113,13 +115,14 @@ def parse():
     ap.add_argument("--param", action="append", default=[], metavar="NAME=VALUE",
                     help="set a tuning parameter of the sort context (names: " +
                          ", ".join(sorted(PARAMS)) + "); repeatable")
-    ap.add_argument("--serve-requests", type=int, default=2000,
+    ap.add_argument("--serve-requests", type=int, default=300,
                     help="requests per arrival rate of the serve_c5 sweep")
-    ap.add_argument("--serve-rates", default="1000,2000,5000,10000,20000,50000")
+    ap.add_argument("--serve-rates", default="1000,5000,20000,50000")
     ap.add_argument("--serve-pool", type=int, default=64,
                     help="distinct requests the serve_c5 stream draws from (without --serve-fresh)")
-    ap.add_argument("--serve-fresh", action="store_true",
-                    help="every request of the sweep is a distinct, newly generated one")
+    ap.add_argument("--serve-pooled", dest="serve_fresh", action="store_false",
+                    help="draw the sweep's requests from a pool of --serve-pool distinct "
+                         "requests instead of generating every request afresh")
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--serve-max-strings", type=int, default=1 << 27)
     ap.add_argument("--scale", type=float, default=1.0,

@@ -248,6 +248,13 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         strings copies the next segment's records into
                                         shared memory while it sorts the current one;
                                         0: one record buffer, loaded through registers */
+#define SSORT_PARAM_L2_PREFETCH 9    /* 1 (default): the partition's count and scatter
+                                        kernels ask for their next tile to be streamed into
+                                        L2 (bulk prefetch) while they work on the current one */
+#define SSORT_PARAM_DIGIT_BITS 10    /* 8, 9 or 10 (default 10): digit width of one
+                                        partition pass, i.e. a pass splits a segment into
+                                        at most 2^bits buckets (2^(bits-1) - 1 sampled
+                                        splitters and the buckets between and at them) */
 #define SSORT_PARAM_GRAPH 7          /* 1: device-driven round loop: the sort runs as a CUDA
                                         graph whose rounds and partition levels are
                                         conditional loops (no host round trip between
@@ -279,6 +286,7 @@ typedef struct {
     double default_ms;      /* device time of one sort with the values before tuning */
     double tuned_ms;        /* with the chosen values */
     uint32_t trials;        /* sorts timed */
+    int64_t digit_bits, block_prefetch, l2_prefetch, graph; /* chosen values */
 } ssort_tuning;
 int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                    const void *d_offs, int off_width, uint64_t n, ssort_tuning *out);

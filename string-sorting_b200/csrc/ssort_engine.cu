@@ -281,6 +281,8 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.target_bucket = target_bucket;
     a.warp8_cap = warp8_cap;
     a.warp1_deep = warp1_deep;
+    a.l2_prefetch = l2_prefetch ? 1u : 0u;
+    a.max_splitters = (1u << (digit_bits - 1)) - 1;
     a.key2 = key2;
 
     // The device-driven loop: not while profiling (per-kernel events need
@@ -354,6 +356,10 @@ int apply_tuning(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
     ctx->warp8_cap = it->second.warp8_cap;
     ctx->overlap = it->second.overlap;
     ctx->fused_gather = it->second.fused_gather;
+    ctx->digit_bits = it->second.digit_bits;
+    ctx->block_prefetch = it->second.block_prefetch;
+    ctx->l2_prefetch = it->second.l2_prefetch;
+    ctx->graph_mode = it->second.graph;
     return SSORT_OK;
 }
 
@@ -719,6 +725,14 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "fused_gather must be 0 or 1");
             ctx->fused_gather = value != 0;
             return SSORT_OK;
+        case SSORT_PARAM_DIGIT_BITS:
+            if (value < 8 || value > 10) return fail(SSORT_EINVAL, "digit_bits out of range (8..10)");
+            ctx->digit_bits = (uint32_t)value;
+            return SSORT_OK;
+        case SSORT_PARAM_L2_PREFETCH:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "l2_prefetch must be 0 or 1");
+            ctx->l2_prefetch = value != 0;
+            return SSORT_OK;
         case SSORT_PARAM_GRAPH:
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "graph must be 0 or 1");
             ctx->graph_mode = value != 0;
@@ -966,15 +980,27 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                 int param;
                 std::vector<int64_t> values;
             };
+            // Coordinate descent over: range-bucket size, digit width of a
+            // partition pass (splitters per pass), the small-segment cutoff,
+            // the gather and overlap choices, the CTA sort's record prefetch,
+            // the partition's L2 prefetch and the device-driven loop.
             const Knob knobs[] = {{SSORT_PARAM_TARGET_BUCKET, {256, 512, 1024}},
+                                  {SSORT_PARAM_DIGIT_BITS, {10, 9, 8}},
                                   {SSORT_PARAM_WARP8_CAP, {64, 128, 256}},
                                   {SSORT_PARAM_FUSED_GATHER, {1, 0}},
-                                  {SSORT_PARAM_OVERLAP, {1, 0}}};
+                                  {SSORT_PARAM_OVERLAP, {1, 0}},
+                                  {SSORT_PARAM_BLOCK_PREFETCH, {1, 0}},
+                                  {SSORT_PARAM_L2_PREFETCH, {1, 0}},
+                                  {SSORT_PARAM_GRAPH, {0, 1}}};
             auto get = [&](int p) -> int64_t {
                 switch (p) {
                     case SSORT_PARAM_TARGET_BUCKET: return ctx->target_bucket;
+                    case SSORT_PARAM_DIGIT_BITS: return ctx->digit_bits;
                     case SSORT_PARAM_WARP8_CAP: return ctx->warp8_cap;
                     case SSORT_PARAM_FUSED_GATHER: return ctx->fused_gather ? 1 : 0;
+                    case SSORT_PARAM_BLOCK_PREFETCH: return ctx->block_prefetch ? 1 : 0;
+                    case SSORT_PARAM_L2_PREFETCH: return ctx->l2_prefetch ? 1 : 0;
+                    case SSORT_PARAM_GRAPH: return ctx->graph_mode ? 1 : 0;
                     default: return ctx->overlap ? 1 : 0;
                 }
             };
@@ -994,8 +1020,9 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                 SS_TRY(ssort_set_param(ctx, k.param, keep));
             }
             const uint32_t sc = size_class(n), ec = entropy_class(bits);
-            ctx->tuned[sc * 4 + ec] = ssort_ctx::Tuned{ctx->target_bucket, ctx->warp8_cap,
-                                                       ctx->overlap, ctx->fused_gather};
+            ctx->tuned[sc * 4 + ec] = ssort_ctx::Tuned{
+                ctx->target_bucket, ctx->warp8_cap, ctx->digit_bits,  ctx->overlap,
+                ctx->fused_gather,  ctx->block_prefetch, ctx->l2_prefetch, ctx->graph_mode};
             out->size_class = sc;
             out->entropy_class = ec;
             out->entropy_bits = bits;
@@ -1003,6 +1030,10 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
             out->warp8_cap = ctx->warp8_cap;
             out->overlap = ctx->overlap ? 1 : 0;
             out->fused_gather = ctx->fused_gather ? 1 : 0;
+            out->digit_bits = ctx->digit_bits;
+            out->block_prefetch = ctx->block_prefetch ? 1 : 0;
+            out->l2_prefetch = ctx->l2_prefetch ? 1 : 0;
+            out->graph = ctx->graph_mode ? 1 : 0;
             out->default_ms = base;
             out->tuned_ms = best;
             out->trials = trials;

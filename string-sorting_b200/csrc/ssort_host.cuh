@@ -81,6 +81,8 @@ struct ssort_ctx {
     bool overlap = true;       // round-0 on-chip sorts on the side stream
     bool fused_gather = true;  // rounds >= 1 gather inside the first count
     bool block_prefetch = true;  // double-buffered CTA sort (k_block2)
+    bool l2_prefetch = true;     // partition kernels prefetch their next tile into L2
+    uint32_t digit_bits = 10;    // a partition pass makes at most 2^digit_bits buckets
     // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
     // key it was built for, three streams to capture nested conditional
     // bodies on, and a pinned copy of the loop state.
@@ -94,8 +96,8 @@ struct ssort_ctx {
     // Autotuned values per (size class * 4 + entropy class), applied to later
     // sorts of the same classes; not while the tuner itself runs.
     struct Tuned {
-        uint32_t target_bucket, warp8_cap;
-        bool overlap, fused_gather;
+        uint32_t target_bucket, warp8_cap, digit_bits;
+        bool overlap, fused_gather, block_prefetch, l2_prefetch, graph;
     };
     std::map<uint32_t, Tuned> tuned;
     bool tuning = false;

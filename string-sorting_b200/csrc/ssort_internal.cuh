@@ -136,6 +136,8 @@ struct SortArgs {
     uint32_t target_bucket;  // wanted strings per range bucket of a partition
     uint32_t warp8_cap;      // largest segment for the one-warp sort (64..WARP8_CAP)
     uint32_t warp1_deep;     // in-warp refinement steps of the one-per-lane sort
+    uint32_t l2_prefetch;    // partition kernels stream their next tile into L2 ahead
+    uint32_t max_splitters;  // splitters per partition pass, 2^(digit bits - 1) - 1 <= KMAX
     // Per string id, key bytes 16..31 as round 0's gather read them (it reads
     // those sectors of the arena anyway); round 1's first partition level
     // takes its keys from here instead of the offset and a random arena read.

@@ -232,6 +232,20 @@ __device__ __forceinline__ uint32_t classify_tbl(const ulonglong2 *s, const uint
     return (lo < u && key_eq(to_key(s[lo]), key)) ? 2 * lo + 1 : 2 * lo;
 }
 
+// Asks the memory system to stream the bytes of [p, p + bytes) into L2 (a
+// TMA bulk prefetch: no registers, nothing to wait for).  The start is
+// rounded up and the end down to 16-byte boundaries, so nothing outside the
+// range is touched; ranges are issued in pieces of at most 1 MB.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint64_t bytes) {
+    uint64_t a = ((uint64_t)(uintptr_t)p + 15) & ~15ull;
+    const uint64_t e = ((uint64_t)(uintptr_t)p + bytes) & ~15ull;
+    while (a < e) {
+        const uint32_t sz = (uint32_t)min(e - a, (uint64_t)(1u << 20));
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(sz) : "memory");
+        a += sz;
+    }
+}
+
 // Padded shared-memory index: one spare slot per 8 keeps both the blocked
 // (stride 8) and the striped (stride 1) access patterns free of bank conflicts.
 __device__ __forceinline__ uint32_t pad(uint32_t e) { return e + (e >> 3); }
@@ -1223,7 +1237,7 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t k = (s.len + a.target_bucket - 1) / a.target_bucket;
-    if (k > (uint32_t)KMAX) k = KMAX;
+    if (k > a.max_splitters) k = a.max_splitters;
     if (k < 1) k = 1;
     uint32_t S = next_pow2(8 * (k + 1));
     if (S < 256) S = 256;
@@ -1447,6 +1461,18 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
         const uint32_t u = nspl[si] & 0xFFFF, f = nspl[si] >> 16, nb = 2 * u + 1;
+        if (a.l2_prefetch && threadIdx.x == 0 && t + gridDim.x < total_tiles) {
+            // the keys (or, when gathering, the indices) of this CTA's next tile
+            const uint32_t t2 = t + gridDim.x;
+            const uint32_t s2i = find_seg(tile_base, nL, t2);
+            const Seg s2 = L[s2i];
+            const uint32_t lo2 = (t2 - tile_base[s2i]) * PART_TILE;
+            const uint32_t len2 = min((uint32_t)PART_TILE, s2.len - lo2);
+            if (GATHER)
+                prefetch_l2(a.idx[0] + s2.start + lo2, (uint64_t)len2 * 4);
+            else
+                prefetch_l2(a.keyb(s2.flags & SEG_BUF1) + s2.start + lo2, (uint64_t)len2 * 16);
+        }
         if (si != loaded) {
             load_splitters(sm, spl, tbl, si, u, f);
             loaded = si;
@@ -1585,6 +1611,18 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
         const uint32_t u = nspl[si] & 0xFFFF, nb = 2 * u + 1;
+        if (a.l2_prefetch && threadIdx.x == 0 && t + gridDim.x < total_tiles) {
+            // keys, indices and destinations of this CTA's next tile
+            const uint32_t t2 = t + gridDim.x;
+            const uint32_t s2i = find_seg(tile_base, nL, t2);
+            const Seg s2 = L[s2i];
+            const uint32_t lo2 = (t2 - tile_base[s2i]) * PART_TILE;
+            const uint32_t len2 = min((uint32_t)PART_TILE, s2.len - lo2);
+            const int b2 = s2.flags & SEG_BUF1;
+            prefetch_l2(a.keyb(b2) + s2.start + lo2, (uint64_t)len2 * 16);
+            prefetch_l2(a.idxb(b2) + s2.start + lo2, (uint64_t)len2 * 4);
+            prefetch_l2(a.bkt + s2.start + lo2, (uint64_t)len2 * 4);
+        }
         const uint32_t tl = t - tile_base[si];
         const uint32_t nt = tile_base[si + 1] - tile_base[si];
         const uint32_t cmb = cm_base[si];

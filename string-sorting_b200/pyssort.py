@@ -40,6 +40,8 @@ SSORT_PARAM_WARP1_DEEP = 5
 SSORT_PARAM_BLOCK_PREFETCH = 6
 SSORT_PARAM_GRAPH = 7
 SSORT_PARAM_GRAPH_MAX_LEVELS = 8
+SSORT_PARAM_L2_PREFETCH = 9
+SSORT_PARAM_DIGIT_BITS = 10
 
 
 class SsortError(RuntimeError):
@@ -114,6 +116,10 @@ class Tuning(ctypes.Structure):
         ("default_ms", ctypes.c_double),
         ("tuned_ms", ctypes.c_double),
         ("trials", ctypes.c_uint32),
+        ("digit_bits", ctypes.c_int64),
+        ("block_prefetch", ctypes.c_int64),
+        ("l2_prefetch", ctypes.c_int64),
+        ("graph", ctypes.c_int64),
     ]
 
     def as_dict(self):

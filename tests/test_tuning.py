@@ -25,6 +25,10 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_WARP1_DEEP, 4096),
     (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 0),
     (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 1),
+    (pyssort.SSORT_PARAM_L2_PREFETCH, 0),
+    (pyssort.SSORT_PARAM_GRAPH, 1),
+    (pyssort.SSORT_PARAM_DIGIT_BITS, 8),
+    (pyssort.SSORT_PARAM_DIGIT_BITS, 9),
 ]
 
 
@@ -79,6 +83,11 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_WARP1_DEEP, -1),
                              (pyssort.SSORT_PARAM_WARP1_DEEP, 4097),
                              (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 2),
+                             (pyssort.SSORT_PARAM_L2_PREFETCH, 2),
+                             (pyssort.SSORT_PARAM_GRAPH, 2),
+                             (pyssort.SSORT_PARAM_GRAPH_MAX_LEVELS, 0),
+                             (pyssort.SSORT_PARAM_DIGIT_BITS, 7),
+                             (pyssort.SSORT_PARAM_DIGIT_BITS, 11),
                              (99, 1)]:
             with pytest.raises(pyssort.SsortError) as e:
                 s.set_param(param, value)
@@ -99,7 +108,11 @@ def test_autotune_then_sort_stays_exact():
         assert t["warp8_cap"] in (64, 128, 256)
         assert t["overlap"] in (0, 1) and t["fused_gather"] in (0, 1)
         assert t["tuned_ms"] <= t["default_ms"]
-        assert t["trials"] == 2 + 2 * (2 + 2 + 1 + 1)  # base, then every other candidate
+        assert t["digit_bits"] in (8, 9, 10)
+        assert t["block_prefetch"] in (0, 1) and t["l2_prefetch"] in (0, 1)
+        assert t["graph"] in (0, 1)
+        # base, then every other candidate of every knob
+        assert t["trials"] == 2 + 2 * (2 + 2 + 2 + 1 + 1 + 1 + 1 + 1)
         # a later sort of the same class uses the recorded values
         d_perm = torch.empty(ss.n, dtype=torch.int32, device="cuda")
         d_lcp = torch.empty(ss.n, dtype=torch.int32, device="cuda")
