@@ -42,7 +42,9 @@ PARAMS = {"target_bucket": pyssort.SSORT_PARAM_TARGET_BUCKET,
           "block_prefetch": pyssort.SSORT_PARAM_BLOCK_PREFETCH,
           "graph": pyssort.SSORT_PARAM_GRAPH,
           "l2_prefetch": pyssort.SSORT_PARAM_L2_PREFETCH,
-          "digit_bits": pyssort.SSORT_PARAM_DIGIT_BITS}
+          "digit_bits": pyssort.SSORT_PARAM_DIGIT_BITS,
+          "scatter": pyssort.SSORT_PARAM_SCATTER,
+          "block_lean": pyssort.SSORT_PARAM_BLOCK_LEAN}
 
 
 def apply_params(sorter, args):

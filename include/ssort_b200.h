@@ -226,6 +226,8 @@ typedef struct {
                               quarter of its strings into round 1) */
     uint64_t window_used;  /* round-1 keys read from those copies instead of
                               through the offset and the arena */
+    uint64_t graph_launches; /* launches of the device-driven loop's graph
+                                (0: the host drove the rounds) */
 } ssort_stats;
 
 int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
@@ -244,10 +246,15 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                        sorts a segment of <= 32 strings takes on its own
                                        runs of equal keys before handing what is left to
                                        the next round; 0: every run waits for the next round */
-#define SSORT_PARAM_BLOCK_PREFETCH 6 /* 1 (default): the CTA sort of segments of 257..2048
-                                        strings copies the next segment's records into
-                                        shared memory while it sorts the current one;
-                                        0: one record buffer, loaded through registers */
+#define SSORT_PARAM_BLOCK_PREFETCH 6 /* 0 (default): the CTA sort of segments of 257..2048
+                                        strings loads one segment's records through
+                                        registers at three CTAs per SM; 1: it copies the
+                                        next segment's records into shared memory while it
+                                        sorts the current one (two CTAs per SM) */
+#define SSORT_PARAM_BLOCK_LEAN 12    /* 1: the CTA sort takes the LCPs of neighbours whose
+                                        packed windows differ from the windows alone and
+                                        reads full keys only for equal windows; 0 (default):
+                                        it reads both neighbours' keys for every string */
 #define SSORT_PARAM_L2_PREFETCH 9    /* 1 (default): the partition's count and scatter
                                         kernels ask for their next tile to be streamed into
                                         L2 (bulk prefetch) while they work on the current one */
@@ -255,11 +262,18 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         partition pass, i.e. a pass splits a segment into
                                         at most 2^bits buckets (2^(bits-1) - 1 sampled
                                         splitters and the buckets between and at them) */
+#define SSORT_PARAM_SCATTER 11       /* 0 (default): the partition scatter lays each tile out
+                                        in shared memory in output order; 1: it stages only
+                                        indices and destinations and reads each key from the
+                                        tile (in L2) in output order, at more CTAs per SM */
 #define SSORT_PARAM_GRAPH 7          /* 1: device-driven round loop: the sort runs as a CUDA
                                         graph whose rounds and partition levels are
                                         conditional loops (no host round trip between
                                         kernels; one host read per up to 64 rounds);
-                                        0 (default): the host drives the rounds */
+                                        0: the host drives the rounds; 2 (default): the
+                                        graph from the second of two sorts in a row with
+                                        the same buffers and size on (building a graph
+                                        costs more than a host-driven sort) */
 #define SSORT_PARAM_GRAPH_MAX_LEVELS 8 /* 1..4096 (default 4096): partition levels one round
                                           of the device-driven loop may take; a round that
                                           needs more fails with SSORT_EINTERNAL */

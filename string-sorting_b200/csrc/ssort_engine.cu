@@ -282,12 +282,15 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.warp8_cap = warp8_cap;
     a.warp1_deep = warp1_deep;
     a.l2_prefetch = l2_prefetch ? 1u : 0u;
+    a.scatter_staged_idx = scatter_variant;
+    a.block_lean = block_lean ? 1u : 0u;
     a.max_splitters = (1u << (digit_bits - 1)) - 1;
+    std::copy(std::begin(class_targets), std::end(class_targets), std::begin(a.target_by_class));
     a.key2 = key2;
 
     // The device-driven loop: not while profiling (per-kernel events need
     // host launches) and not for the server's per-round calls.
-    if (graph_mode && !prof) return run_graph(a, n, d_inst, ninst);
+    if (graph_mode && !prof && graph_wanted(a)) return run_graph(a, n, d_inst, ninst);
 
     Seg *cur = ws.R, *nxt = ws.N;
     Counters *dc = ws.ctr;
@@ -332,9 +335,23 @@ uint32_t size_class(uint64_t n) { return n ? 63u - (uint32_t)__builtin_clzll(n) 
 uint32_t entropy_class(double bits) { return bits < 2.0 ? 0u : (bits < 4.0 ? 1u : 2u); }
 
 // Applies autotuned values recorded for this input's size and entropy class.
+// A batched sort (many instances of many sizes) also gets, per segment size
+// class, the range-bucket size tuned for that class and the batch's entropy
+// class, so that each instance is partitioned as a plain sort of its size
+// would be.
 int apply_tuning(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
-                 const void *d_offs, int off_width, uint64_t n) {
+                 const void *d_offs, int off_width, uint64_t n, bool batched) {
+    std::fill(std::begin(ctx->class_targets), std::end(ctx->class_targets), uint16_t(0));
     if (ctx->tuned.empty() || ctx->tuning || n < 2) return SSORT_OK;
+    if (batched) {
+        double bits = 0;
+        SS_TRY(ctx->sample_entropy(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, bits));
+        const uint32_t ec = entropy_class(bits);
+        for (uint32_t c = 0; c < 32; ++c) {
+            auto t = ctx->tuned.find(c * 4 + ec);
+            if (t != ctx->tuned.end()) ctx->class_targets[c] = (uint16_t)t->second.target_bucket;
+        }
+    }
     const uint32_t sc = size_class(n);
     uint32_t classes = 0, only = 0;
     for (uint32_t e = 0; e < 3; ++e)
@@ -360,13 +377,14 @@ int apply_tuning(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
     ctx->block_prefetch = it->second.block_prefetch;
     ctx->l2_prefetch = it->second.l2_prefetch;
     ctx->graph_mode = it->second.graph;
+    ctx->block_lean = it->second.block_lean;
     return SSORT_OK;
 }
 
 int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                      const void *d_offs, int off_width, uint64_t n, uint32_t *d_perm,
                      uint32_t *d_lcp, const uint32_t *d_inst = nullptr, uint32_t ninst = 0) {
-    SS_TRY(apply_tuning(ctx, d_arena, arena_bytes, d_offs, off_width, n));
+    SS_TRY(apply_tuning(ctx, d_arena, arena_bytes, d_offs, off_width, n, d_inst != nullptr));
     ctx->stats = ssort_stats{};
     ctx->stats.n = n;
     SS_CUDA(cudaEventRecord(ctx->ev_start, ctx->st));
@@ -729,13 +747,21 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
             if (value < 8 || value > 10) return fail(SSORT_EINVAL, "digit_bits out of range (8..10)");
             ctx->digit_bits = (uint32_t)value;
             return SSORT_OK;
+        case SSORT_PARAM_BLOCK_LEAN:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "block_lean must be 0 or 1");
+            ctx->block_lean = value != 0;
+            return SSORT_OK;
+        case SSORT_PARAM_SCATTER:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "scatter must be 0 or 1");
+            ctx->scatter_variant = (uint32_t)value;
+            return SSORT_OK;
         case SSORT_PARAM_L2_PREFETCH:
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "l2_prefetch must be 0 or 1");
             ctx->l2_prefetch = value != 0;
             return SSORT_OK;
         case SSORT_PARAM_GRAPH:
-            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "graph must be 0 or 1");
-            ctx->graph_mode = value != 0;
+            if (value < 0 || value > 2) return fail(SSORT_EINVAL, "graph must be 0, 1 or 2");
+            ctx->graph_mode = (uint32_t)value;
             return SSORT_OK;
         case SSORT_PARAM_GRAPH_MAX_LEVELS:
             if (value < 1 || value > (int64_t)GRAPH_MAX_LEVELS)
@@ -991,7 +1017,8 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                                   {SSORT_PARAM_OVERLAP, {1, 0}},
                                   {SSORT_PARAM_BLOCK_PREFETCH, {1, 0}},
                                   {SSORT_PARAM_L2_PREFETCH, {1, 0}},
-                                  {SSORT_PARAM_GRAPH, {0, 1}}};
+                                  {SSORT_PARAM_BLOCK_LEAN, {0, 1}},
+                                  {SSORT_PARAM_GRAPH, {2, 0}}};
             auto get = [&](int p) -> int64_t {
                 switch (p) {
                     case SSORT_PARAM_TARGET_BUCKET: return ctx->target_bucket;
@@ -1000,7 +1027,8 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                     case SSORT_PARAM_FUSED_GATHER: return ctx->fused_gather ? 1 : 0;
                     case SSORT_PARAM_BLOCK_PREFETCH: return ctx->block_prefetch ? 1 : 0;
                     case SSORT_PARAM_L2_PREFETCH: return ctx->l2_prefetch ? 1 : 0;
-                    case SSORT_PARAM_GRAPH: return ctx->graph_mode ? 1 : 0;
+                    case SSORT_PARAM_BLOCK_LEAN: return ctx->block_lean ? 1 : 0;
+                    case SSORT_PARAM_GRAPH: return ctx->graph_mode;
                     default: return ctx->overlap ? 1 : 0;
                 }
             };
@@ -1021,8 +1049,9 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
             }
             const uint32_t sc = size_class(n), ec = entropy_class(bits);
             ctx->tuned[sc * 4 + ec] = ssort_ctx::Tuned{
-                ctx->target_bucket, ctx->warp8_cap, ctx->digit_bits,  ctx->overlap,
-                ctx->fused_gather,  ctx->block_prefetch, ctx->l2_prefetch, ctx->graph_mode};
+                ctx->target_bucket, ctx->warp8_cap,     ctx->digit_bits,  ctx->graph_mode,
+                ctx->overlap,       ctx->fused_gather,  ctx->block_prefetch, ctx->l2_prefetch,
+                ctx->block_lean};
             out->size_class = sc;
             out->entropy_class = ec;
             out->entropy_bits = bits;
@@ -1033,7 +1062,7 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
             out->digit_bits = ctx->digit_bits;
             out->block_prefetch = ctx->block_prefetch ? 1 : 0;
             out->l2_prefetch = ctx->l2_prefetch ? 1 : 0;
-            out->graph = ctx->graph_mode ? 1 : 0;
+            out->graph = ctx->graph_mode;
             out->default_ms = base;
             out->tuned_ms = best;
             out->trials = trials;
@@ -1166,6 +1195,7 @@ extern "C" int ssort_sort_device_noalloc(const uint8_t *d_arena, uint64_t arena_
     c.num_sms = d.num_sms;
     c.st = (cudaStream_t)stream;
     c.h_ctr = &d.host_ctr;
+    c.graph_mode = 0;  // the host-driven loop: building a graph would allocate
     c.ws = ws_bind(ws_layout(NOALLOC_MAX_N), d.scratch);
     c.ws_n = NOALLOC_MAX_N;
     const int rc = c.run_ws(d_arena, arena_bytes, d_offs, off_width, (uint32_t)n, d_perm, d_lcp);

@@ -199,6 +199,17 @@ int ssort_ctx::graph_build(const SortArgs &a) {
     return SSORT_OK;
 }
 
+// Whether this sort runs through the graph: always in mode 1; in mode 2 when
+// a graph for these arguments exists or the previous sort had them too.
+bool ssort_ctx::graph_wanted(const SortArgs &a) {
+    if (graph_mode == 1) return true;
+    std::vector<unsigned char> k = graph_key(a, *this);
+    if (!gkey.empty() && k == gkey) return true;
+    const bool repeat = k == last_key;
+    last_key = std::move(k);
+    return repeat;
+}
+
 // One sort through the graph: the prologue (identity permutation, the first
 // round's segments, the loop state) is launched from the host, then the
 // graph runs rounds until none is left.
@@ -230,7 +241,8 @@ int ssort_ctx::run_graph(const SortArgs &a, uint32_t n, const uint32_t *d_inst, 
         const Seg first{0, n, 0, 0};
         SS_CUDA(cudaMemcpyAsync(ws.R, &first, sizeof(Seg), cudaMemcpyHostToDevice, st));
     }
-    for (uint32_t launches = 0;; ++launches) {
+    uint32_t launches = 0;
+    for (;; ++launches) {
         // Every launch runs at least one round or ends the sort; a sort needs
         // at most one round per 16 bytes of its longest shared prefix.
         if (launches > (1u << 22))
@@ -264,6 +276,7 @@ int ssort_ctx::run_graph(const SortArgs &a, uint32_t n, const uint32_t *d_inst, 
     stats.full_sorted = h_gs->full_sorted;
     stats.window_saved = h_gs->window_saved;
     stats.window_used = h_gs->window_used;
+    stats.graph_launches = launches + 1;
     if (d_inst) LAUNCH(this, "localize", launch_localize(a.idx[0], n, d_inst, ninst, st));
     return SSORT_OK;
 }

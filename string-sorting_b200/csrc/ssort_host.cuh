@@ -80,13 +80,19 @@ struct ssort_ctx {
     uint32_t warp1_deep = ssort::WARP1_DEEP;        // in-warp refinement steps
     bool overlap = true;       // round-0 on-chip sorts on the side stream
     bool fused_gather = true;  // rounds >= 1 gather inside the first count
-    bool block_prefetch = true;  // double-buffered CTA sort (k_block2)
+    bool block_prefetch = false;  // double-buffered CTA sort (k_block2)
+    bool block_lean = false;      // CTA sort finish from the packed windows
     bool l2_prefetch = true;     // partition kernels prefetch their next tile into L2
     uint32_t digit_bits = 10;    // a partition pass makes at most 2^digit_bits buckets
+    uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
     // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
     // key it was built for, three streams to capture nested conditional
     // bodies on, and a pinned copy of the loop state.
-    bool graph_mode = false;
+    // 0: host loop; 1: device-driven loop always; 2 (auto): the device-driven
+    // loop once a sort repeats the previous sort's arguments (buffers, size,
+    // workspace), since building a graph costs more than one host-driven sort
+    uint32_t graph_mode = 2;
+    std::vector<unsigned char> last_key;  // arguments of the previous sort (auto mode)
     uint32_t graph_max_levels = ssort::GRAPH_MAX_LEVELS;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -96,10 +102,13 @@ struct ssort_ctx {
     // Autotuned values per (size class * 4 + entropy class), applied to later
     // sorts of the same classes; not while the tuner itself runs.
     struct Tuned {
-        uint32_t target_bucket, warp8_cap, digit_bits;
-        bool overlap, fused_gather, block_prefetch, l2_prefetch, graph;
+        uint32_t target_bucket, warp8_cap, digit_bits, graph;
+        bool overlap, fused_gather, block_prefetch, l2_prefetch, block_lean;
     };
     std::map<uint32_t, Tuned> tuned;
+    // target buckets per segment size class for the next batched sort
+    // (SortArgs::target_by_class), from the tuned entries of each class
+    uint16_t class_targets[32] = {};
     bool tuning = false;
     ssort::DBuf hist_buf;
     uint32_t *h_hist = nullptr;
@@ -212,6 +221,7 @@ struct ssort_ctx {
                uint32_t ninst = 0);
     // device-driven round loop (ssort_graph.cu)
     int run_graph(const ssort::SortArgs &a, uint32_t n, const uint32_t *d_inst, uint32_t ninst);
+    bool graph_wanted(const ssort::SortArgs &a);
     int graph_build(const ssort::SortArgs &a);
     int graph_small(const ssort::SortArgs &a, cudaStream_t s);
     void graph_release();

@@ -137,7 +137,13 @@ struct SortArgs {
     uint32_t warp8_cap;      // largest segment for the one-warp sort (64..WARP8_CAP)
     uint32_t warp1_deep;     // in-warp refinement steps of the one-per-lane sort
     uint32_t l2_prefetch;    // partition kernels stream their next tile into L2 ahead
+    uint32_t scatter_staged_idx;  // scatter stages indices only (k_scatter2)
+    uint32_t block_lean;     // CTA sort: neighbour LCPs from the packed windows
     uint32_t max_splitters;  // splitters per partition pass, 2^(digit bits - 1) - 1 <= KMAX
+    // Per segment size class (floor(log2 len)): the wanted strings per range
+    // bucket autotuned for that class (0: target_bucket).  Set for batched
+    // sorts, whose instances and segments span many size classes.
+    uint16_t target_by_class[32];
     // Per string id, key bytes 16..31 as round 0's gather read them (it reads
     // those sectors of the arena anyway); round 1's first partition level
     // takes its keys from here instead of the offset and a random arena read.

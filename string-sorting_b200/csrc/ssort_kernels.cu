@@ -1236,7 +1236,9 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     const Seg s = L[si];
     const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t k = (s.len + a.target_bucket - 1) / a.target_bucket;
+    const uint32_t tcls = a.target_by_class[31 - __clz(s.len)];
+    const uint32_t tb = tcls ? tcls : a.target_bucket;
+    uint32_t k = (s.len + tb - 1) / tb;
     if (k > a.max_splitters) k = a.max_splitters;
     if (k < 1) k = 1;
     uint32_t S = next_pow2(8 * (k + 1));
@@ -1697,6 +1699,133 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
             const uint32_t o = sm.dst[i];
             Kout[o] = sm.key[i];
             Iout[o] = sm.idx[i];
+        }
+        __syncthreads();
+    }
+}
+
+
+// The same scatter with only indices and destinations staged: the slots of
+// the tile in output order record where each record sits in the tile, and
+// the write-out reads the keys from there (the tile was streamed into L2 by
+// the previous tile's bulk prefetch, and the reads stay inside the tile's
+// 64 KB).  48 KB of shared memory and about half the registers of k_scatter,
+// so three or four CTAs share an SM instead of two.
+struct Scatter2Smem {
+    uint32_t idx[PART_TILE];    // indices in output order
+    uint32_t dst[PART_TILE];    // destinations in output order
+    uint16_t src[PART_TILE];    // tile position of the record at each output slot
+    uint32_t gbase[NB_MAX + 1];
+    uint32_t tstart[NB_MAX + 1];
+    uint32_t wsum[SCATTER_THREADS / 32];
+};
+constexpr int SCATTER2_BATCH = 4;  // keys in flight per thread in the write-out
+
+__global__ void __launch_bounds__(SCATTER_THREADS, 3) k_scatter2(
+    SortArgs a, const Seg *__restrict__ L, Count cnt, const uint32_t *__restrict__ tile_base,
+    const uint32_t *__restrict__ nspl, const uint32_t *__restrict__ cm_base,
+    const uint32_t *__restrict__ cm_scan) {
+    extern __shared__ __align__(16) unsigned char scatter_smem[];
+    Scatter2Smem &sm = *reinterpret_cast<Scatter2Smem *>(scatter_smem);
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr uint32_t QPT = (NB_MAX + 1) / SCATTER_THREADS;  // buckets per thread (4)
+    const uint32_t nL = count_of(cnt);
+    const uint32_t total_tiles = tile_base[nL];
+    for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        const uint32_t si = find_seg(tile_base, nL, t);
+        const Seg s = L[si];
+        const uint32_t u = nspl[si] & 0xFFFF, nb = 2 * u + 1;
+        if (a.l2_prefetch && threadIdx.x == 0 && t + gridDim.x < total_tiles) {
+            const uint32_t t2 = t + gridDim.x;
+            const uint32_t s2i = find_seg(tile_base, nL, t2);
+            const Seg s2 = L[s2i];
+            const uint32_t lo2 = (t2 - tile_base[s2i]) * PART_TILE;
+            const uint32_t len2 = min((uint32_t)PART_TILE, s2.len - lo2);
+            const int b2 = s2.flags & SEG_BUF1;
+            prefetch_l2(a.keyb(b2) + s2.start + lo2, (uint64_t)len2 * 16);
+            prefetch_l2(a.idxb(b2) + s2.start + lo2, (uint64_t)len2 * 4);
+            prefetch_l2(a.bkt + s2.start + lo2, (uint64_t)len2 * 4);
+        }
+        const uint32_t tl = t - tile_base[si];
+        const uint32_t nt = tile_base[si + 1] - tile_base[si];
+        const uint32_t cmb = cm_base[si];
+        const uint32_t seg0 = cm_scan[cmb];
+        const uint32_t lo = tl * PART_TILE;
+        const uint32_t tlen = min((uint32_t)PART_TILE, s.len - lo);
+        const int ib = s.flags & SEG_BUF1;
+        const ulonglong2 *__restrict__ Kin = a.keyb(ib) + s.start + lo;
+        const uint32_t *Iin = a.idxb(ib) + s.start;
+        const uint32_t *Din = a.bkt + s.start;
+        uint32_t ii[SCATTER_ITEMS], dd[SCATTER_ITEMS];
+#pragma unroll
+        for (int c = 0; c < SCATTER_ITEMS; ++c) {
+            const uint32_t e = c * SCATTER_THREADS + threadIdx.x;
+            if (e < tlen) {
+                ii[c] = Iin[lo + e];
+                dd[c] = Din[lo + e];
+            }
+        }
+        uint32_t cnt4[QPT];
+        uint32_t mysum = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < QPT; ++j) {
+            const uint32_t q = threadIdx.x * QPT + j;
+            uint32_t c0 = 0;
+            if (q < nb) {
+                const uint64_t at = cmb + (uint64_t)q * nt + tl;
+                const uint32_t g = cm_scan[at];
+                c0 = cm_scan[at + 1] - g;
+                sm.gbase[q] = g - seg0;
+            }
+            cnt4[j] = c0;
+            mysum += c0;
+        }
+        uint32_t incl = mysum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (uint32_t)d) incl += y;
+        }
+        if (lane == 31) sm.wsum[w] = incl;
+        __syncthreads();
+        uint32_t run = incl - mysum;
+        for (uint32_t q = 0; q < w; ++q) run += sm.wsum[q];
+#pragma unroll
+        for (uint32_t j = 0; j < QPT; ++j) {
+            sm.tstart[threadIdx.x * QPT + j] = run;
+            run += cnt4[j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < SCATTER_ITEMS; ++c) {
+            const uint32_t e = c * SCATTER_THREADS + threadIdx.x;
+            if (e < tlen) {
+                const uint32_t b = dd[c] >> 12, off = dd[c] & (PART_TILE - 1);
+                const uint32_t slot = sm.tstart[b] + off;
+                sm.src[slot] = (uint16_t)e;
+                sm.idx[slot] = ii[c];
+                sm.dst[slot] = sm.gbase[b] + off;
+            }
+        }
+        __syncthreads();
+        ulonglong2 *Kout = a.keyb(ib ^ 1) + s.start;
+        uint32_t *Iout = a.idxb(ib ^ 1) + s.start;
+        for (uint32_t i0 = 0; i0 < tlen; i0 += SCATTER2_BATCH * SCATTER_THREADS) {
+            ulonglong2 kv[SCATTER2_BATCH];
+#pragma unroll
+            for (int q = 0; q < SCATTER2_BATCH; ++q) {
+                const uint32_t i = i0 + q * SCATTER_THREADS + threadIdx.x;
+                if (i < tlen) kv[q] = __ldg(Kin + sm.src[i]);
+            }
+#pragma unroll
+            for (int q = 0; q < SCATTER2_BATCH; ++q) {
+                const uint32_t i = i0 + q * SCATTER_THREADS + threadIdx.x;
+                if (i < tlen) {
+                    const uint32_t o = sm.dst[i];
+                    Kout[o] = kv[q];
+                    Iout[o] = sm.idx[i];
+                }
+            }
         }
         __syncthreads();
     }
@@ -2334,8 +2463,9 @@ __device__ __forceinline__ void group_merge_passes64(uint64_t *sv, uint32_t span
 }
 
 // The CTAs cta0 .. cta0 + ncta - 1 of the launch sort the segments of one
-// size class (list S of nS segments) with groups of GT threads.
-template <int GT>
+// size class (list S of nS segments) with groups of GT threads.  LEAN: the
+// finish takes neighbour LCPs from the packed windows (finish_packed).
+template <int GT, bool LEAN = false>
 __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__restrict__ S,
                                             uint32_t nS, uint32_t cta0, uint32_t ncta, Seg *N,
                                             Counters *c) {
@@ -2413,8 +2543,8 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
             dl |= red[1][gi * (GT / 32) + q];
         }
         bool packed = false;
-        if (dh | dl) {
-            const uint32_t f = clz128(dh, dl);
+        const uint32_t f = (dh | dl) ? clz128(dh, dl) : 128u;
+        if (f < 128) {
             if (gw < nruns) warp_run_packed<SMALL_ITEMS>(sk, sv, gw * BLOCK_RUN, s.len, f, lane);
             group_sync<GT>(gi);
             group_merge_passes64<GT>(sv, span, t, gi);
@@ -2434,7 +2564,9 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
             }
         }
         group_sync<GT>(gi);
-        if (packed)
+        if (packed && LEAN)
+            finish_packed<true>(a, s, sk, sx, sv, f, t, GT, N, c);
+        else if (packed)
             finish_segment<true>(a, s, sk, sx, sv, t, GT, N, c);
         else
             finish_segment<false>(a, s, sk, sx, sv, t, GT, N, c);
@@ -2449,11 +2581,11 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
 
 // One size class per launch (a single launch for all three inlines all
 // three bodies and spills more; measured slower).
-template <int GT>
+template <int GT, bool LEAN>
 __global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
                                                             Span sp, Seg *N, Counters *c) {
     const uint32_t lo = count_of(sp.lo);
-    block_class<GT>(a, S + lo, count_of(sp.hi) - lo, 0, gridDim.x, N, c);
+    block_class<GT, LEAN>(a, S + lo, count_of(sp.hi) - lo, 0, gridDim.x, N, c);
 }
 
 // ---- segments of 257..SMALL_CAP strings, with the next segment prefetched ---
@@ -2836,12 +2968,20 @@ static void set_smem_attrs() {
                          (int)sizeof(PartSmem));
     cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(ScatterSmem));
+    cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(Scatter2Smem));
     cudaFuncSetAttribute(k_warp8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W8_SMEM);
-    cudaFuncSetAttribute(k_block<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
-    cudaFuncSetAttribute(k_block<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
-    cudaFuncSetAttribute(k_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
     cudaFuncSetAttribute(k_block2<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK2_SMEM);
@@ -2992,6 +3132,12 @@ void launch_scatter(const SortArgs &a, const Seg *L, Count nL, const uint32_t *t
                     const uint32_t *cm_base, const uint32_t *cm_scan, int grid, cudaStream_t st) {
     if (!nL.dev && !nL.host) return;
     set_smem_attrs();
+    if (a.scatter_staged_idx) {
+        // three CTAs per SM where k_scatter fits two (grid: two per SM)
+        k_scatter2<<<grid / 2 * 3, SCATTER_THREADS, sizeof(Scatter2Smem), st>>>(
+            a, L, nL, tile_base, nspl, cm_base, cm_scan);
+        return;
+    }
     k_scatter<<<grid, SCATTER_THREADS, sizeof(ScatterSmem), st>>>(a, L, nL, tile_base, nspl,
                                                                   cm_base, cm_scan);
 }
@@ -3037,12 +3183,21 @@ void launch_block(const SortArgs &a, const Seg *S, Span sp, int cls, Seg *N, Cou
             k_block2<256><<<grid, SMALL_THREADS, BLOCK2_SMEM, st>>>(a, S, sp, N, c);
         return;
     }
+    if (a.block_lean) {
+        if (cls == 0)
+            k_block<64, true><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+        else if (cls == 1)
+            k_block<128, true><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+        else
+            k_block<256, true><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+        return;
+    }
     if (cls == 0)
-        k_block<64><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+        k_block<64, false><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
     else if (cls == 1)
-        k_block<128><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+        k_block<128, false><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
     else
-        k_block<256><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+        k_block<256, false><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
 }
 
 void launch_equal(const SortArgs &a, const Seg *E, Span sp, Seg *N, Counters *c, int grid,

@@ -42,6 +42,8 @@ SSORT_PARAM_GRAPH = 7
 SSORT_PARAM_GRAPH_MAX_LEVELS = 8
 SSORT_PARAM_L2_PREFETCH = 9
 SSORT_PARAM_DIGIT_BITS = 10
+SSORT_PARAM_SCATTER = 11
+SSORT_PARAM_BLOCK_LEAN = 12
 
 
 class SsortError(RuntimeError):
@@ -75,6 +77,7 @@ class Stats(ctypes.Structure):
         ("full_sorted", ctypes.c_uint64),
         ("window_saved", ctypes.c_uint64),
         ("window_used", ctypes.c_uint64),
+        ("graph_launches", ctypes.c_uint64),
     ]
 
     def as_dict(self):

@@ -116,3 +116,26 @@ def test_graph_rebuilds_for_new_buffers():
             p, l = s.sort_host(ss.arena, ss.offs)
             rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
             assert np.array_equal(p, rp) and np.array_equal(l, rl)
+
+
+def test_auto_mode_uses_the_graph_from_the_second_identical_sort():
+    """The default (SSORT_PARAM_GRAPH = 2): a sort whose buffers and size
+    differ from the previous sort's runs on the host loop; the second sort
+    in a row with the same arguments builds and runs the graph, and so do
+    later ones; results stay the oracle's throughout."""
+    torch = pytest.importorskip("torch")
+    ss = pyssort.gen_urls(400_000, seed=24)
+    rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+    d_arena = torch.from_numpy(ss.arena).cuda()
+    d_offs = torch.from_numpy(ss.offs.view(np.int64)).cuda()
+    d_perm = torch.empty(ss.n, dtype=torch.int32, device="cuda")
+    d_lcp = torch.empty(ss.n, dtype=torch.int32, device="cuda")
+    used = []
+    with pyssort.Sorter(0) as s:
+        for _ in range(3):
+            s.sort_device(d_arena, ss.arena.nbytes, d_offs, 8, ss.n, d_perm, d_lcp)
+            torch.cuda.synchronize()
+            used.append(s.stats().graph_launches)
+            assert np.array_equal(d_perm.cpu().numpy().view(np.uint32), rp)
+            assert np.array_equal(d_lcp.cpu().numpy().view(np.uint32), rl)
+    assert used[0] == 0 and used[1] >= 1 and used[2] >= 1

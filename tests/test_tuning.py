@@ -29,6 +29,9 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_GRAPH, 1),
     (pyssort.SSORT_PARAM_DIGIT_BITS, 8),
     (pyssort.SSORT_PARAM_DIGIT_BITS, 9),
+    (pyssort.SSORT_PARAM_SCATTER, 1),
+    (pyssort.SSORT_PARAM_BLOCK_LEAN, 1),
+    (pyssort.SSORT_PARAM_GRAPH, 0),
 ]
 
 
@@ -84,10 +87,12 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_WARP1_DEEP, 4097),
                              (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 2),
                              (pyssort.SSORT_PARAM_L2_PREFETCH, 2),
-                             (pyssort.SSORT_PARAM_GRAPH, 2),
+                             (pyssort.SSORT_PARAM_GRAPH, 3),
+                             (pyssort.SSORT_PARAM_BLOCK_LEAN, 2),
                              (pyssort.SSORT_PARAM_GRAPH_MAX_LEVELS, 0),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 7),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 11),
+                             (pyssort.SSORT_PARAM_SCATTER, 2),
                              (99, 1)]:
             with pytest.raises(pyssort.SsortError) as e:
                 s.set_param(param, value)
@@ -110,9 +115,9 @@ def test_autotune_then_sort_stays_exact():
         assert t["tuned_ms"] <= t["default_ms"]
         assert t["digit_bits"] in (8, 9, 10)
         assert t["block_prefetch"] in (0, 1) and t["l2_prefetch"] in (0, 1)
-        assert t["graph"] in (0, 1)
+        assert t["graph"] in (0, 2)
         # base, then every other candidate of every knob
-        assert t["trials"] == 2 + 2 * (2 + 2 + 2 + 1 + 1 + 1 + 1 + 1)
+        assert t["trials"] == 2 + 2 * (2 + 2 + 2 + 1 + 1 + 1 + 1 + 1 + 1)
         # a later sort of the same class uses the recorded values
         d_perm = torch.empty(ss.n, dtype=torch.int32, device="cuda")
         d_lcp = torch.empty(ss.n, dtype=torch.int32, device="cuda")
@@ -134,3 +139,27 @@ def test_kept_keys_with_separate_gather():
         st = s.stats()
     assert st.gather_fused == 0 and st.window_saved > 0 and st.window_used > 0
     assert np.array_equal(p, rp) and np.array_equal(l, rl)
+
+
+def test_batched_sort_uses_per_class_tuning():
+    """After autotuning plain sorts of two size classes, a batched call
+    partitions each segment with the bucket size tuned for its own size
+    class; every instance is still the oracle's result."""
+    torch = pytest.importorskip("torch")
+    with pyssort.Sorter(0) as s:
+        for n in (300_000, 40_000):
+            ss = pyssort.gen_uniform(n, 1, 20, ord("a"), 26, seed=n)
+            d_arena = torch.from_numpy(ss.arena).cuda()
+            d_offs = torch.from_numpy(ss.offs.view(np.int64)).cuda()
+            s.autotune(d_arena, ss.arena.nbytes, d_offs, 8, ss.n)
+        params = pyssort.batch_instance_params(120, 41, lo=2, hi=400_000)
+        b = pyssort.gen_instances(params, seed=42)
+        perm, lcp = s.sort_batch_host(b.arena, b.offs, b.inst_start)
+    st = b.inst_start
+    for i in range(len(params)):
+        lo, hi = int(st[i]), int(st[i + 1])
+        if hi - lo < 1:
+            continue
+        rp, rl = pyoracle.oracle_sort(b.arena, b.offs[lo:hi])
+        assert np.array_equal(perm[lo:hi], rp), i
+        assert np.array_equal(lcp[lo:hi], rl), i
