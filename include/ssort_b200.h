@@ -253,8 +253,10 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         sorts the current one (two CTAs per SM) */
 #define SSORT_PARAM_BLOCK_LEAN 12    /* 1: the CTA sort takes the LCPs of neighbours whose
                                         packed windows differ from the windows alone and
-                                        reads full keys only for equal windows; 0 (default):
-                                        it reads both neighbours' keys for every string */
+                                        reads full keys only for equal windows; 2: that, and
+                                        its first sort runs on 32-bit packed keys (21 key
+                                        bits and the position; ties on those bits are put in
+                                        order afterwards); 0 (default): full-key finish */
 #define SSORT_PARAM_L2_PREFETCH 9    /* 1 (default): the partition's count and scatter
                                         kernels ask for their next tile to be streamed into
                                         L2 (bulk prefetch) while they work on the current one */

@@ -283,7 +283,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.warp1_deep = warp1_deep;
     a.l2_prefetch = l2_prefetch ? 1u : 0u;
     a.scatter_staged_idx = scatter_variant;
-    a.block_lean = block_lean ? 1u : 0u;
+    a.block_lean = block_lean;
     a.max_splitters = (1u << (digit_bits - 1)) - 1;
     std::copy(std::begin(class_targets), std::end(class_targets), std::begin(a.target_by_class));
     a.key2 = key2;
@@ -748,8 +748,8 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
             ctx->digit_bits = (uint32_t)value;
             return SSORT_OK;
         case SSORT_PARAM_BLOCK_LEAN:
-            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "block_lean must be 0 or 1");
-            ctx->block_lean = value != 0;
+            if (value < 0 || value > 2) return fail(SSORT_EINVAL, "block_lean must be 0, 1 or 2");
+            ctx->block_lean = (uint32_t)value;
             return SSORT_OK;
         case SSORT_PARAM_SCATTER:
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "scatter must be 0 or 1");
@@ -1017,7 +1017,7 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                                   {SSORT_PARAM_OVERLAP, {1, 0}},
                                   {SSORT_PARAM_BLOCK_PREFETCH, {1, 0}},
                                   {SSORT_PARAM_L2_PREFETCH, {1, 0}},
-                                  {SSORT_PARAM_BLOCK_LEAN, {0, 1}},
+                                  {SSORT_PARAM_BLOCK_LEAN, {0, 1, 2}},
                                   {SSORT_PARAM_GRAPH, {2, 0}}};
             auto get = [&](int p) -> int64_t {
                 switch (p) {
@@ -1027,7 +1027,7 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                     case SSORT_PARAM_FUSED_GATHER: return ctx->fused_gather ? 1 : 0;
                     case SSORT_PARAM_BLOCK_PREFETCH: return ctx->block_prefetch ? 1 : 0;
                     case SSORT_PARAM_L2_PREFETCH: return ctx->l2_prefetch ? 1 : 0;
-                    case SSORT_PARAM_BLOCK_LEAN: return ctx->block_lean ? 1 : 0;
+                    case SSORT_PARAM_BLOCK_LEAN: return ctx->block_lean;
                     case SSORT_PARAM_GRAPH: return ctx->graph_mode;
                     default: return ctx->overlap ? 1 : 0;
                 }
@@ -1049,9 +1049,9 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
             }
             const uint32_t sc = size_class(n), ec = entropy_class(bits);
             ctx->tuned[sc * 4 + ec] = ssort_ctx::Tuned{
-                ctx->target_bucket, ctx->warp8_cap,     ctx->digit_bits,  ctx->graph_mode,
-                ctx->overlap,       ctx->fused_gather,  ctx->block_prefetch, ctx->l2_prefetch,
-                ctx->block_lean};
+                ctx->target_bucket, ctx->warp8_cap,    ctx->digit_bits,     ctx->graph_mode,
+                ctx->block_lean,    ctx->overlap,      ctx->fused_gather,   ctx->block_prefetch,
+                ctx->l2_prefetch};
             out->size_class = sc;
             out->entropy_class = ec;
             out->entropy_bits = bits;

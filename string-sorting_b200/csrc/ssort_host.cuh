@@ -81,7 +81,8 @@ struct ssort_ctx {
     bool overlap = true;       // round-0 on-chip sorts on the side stream
     bool fused_gather = true;  // rounds >= 1 gather inside the first count
     bool block_prefetch = false;  // double-buffered CTA sort (k_block2)
-    bool block_lean = false;      // CTA sort finish from the packed windows
+    uint32_t block_lean = 0;      // CTA sort: 1 finish from the packed windows, 2 also a
+                                  // first sort on 32-bit packed keys
     bool l2_prefetch = true;     // partition kernels prefetch their next tile into L2
     uint32_t digit_bits = 10;    // a partition pass makes at most 2^digit_bits buckets
     uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
@@ -102,8 +103,8 @@ struct ssort_ctx {
     // Autotuned values per (size class * 4 + entropy class), applied to later
     // sorts of the same classes; not while the tuner itself runs.
     struct Tuned {
-        uint32_t target_bucket, warp8_cap, digit_bits, graph;
-        bool overlap, fused_gather, block_prefetch, l2_prefetch, block_lean;
+        uint32_t target_bucket, warp8_cap, digit_bits, graph, block_lean;
+        bool overlap, fused_gather, block_prefetch, l2_prefetch;
     };
     std::map<uint32_t, Tuned> tuned;
     // target buckets per segment size class for the next batched sort

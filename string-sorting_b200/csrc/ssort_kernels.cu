@@ -378,14 +378,14 @@ __device__ __forceinline__ uint64_t sort_key(const Key &k, uint32_t f, uint32_t 
     return (window64(k, f) & ~POS_MASK) | pos;
 }
 
-template <int ITEMS, int J>
-__device__ __forceinline__ void stage_local64(uint64_t (&v)[ITEMS], uint32_t kk, uint32_t lane) {
+template <int ITEMS, int J, typename V = uint64_t>
+__device__ __forceinline__ void stage_local64(V (&v)[ITEMS], uint32_t kk, uint32_t lane) {
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         if ((i & J) == 0) {
             const int l = i | J;
             const bool asc = (((lane * ITEMS + i) & kk) == 0);
-            const uint64_t a = v[i], b = v[l];
+            const V a = v[i], b = v[l];
             const bool sw = (b < a) == asc;
             v[i] = sw ? b : a;
             v[l] = sw ? a : b;
@@ -395,8 +395,8 @@ __device__ __forceinline__ void stage_local64(uint64_t (&v)[ITEMS], uint32_t kk,
 
 // Bitonic sort of 32 * ITEMS distinct uint64 values held by one warp (lane l
 // holds elements l * ITEMS ..), ITEMS = 1, 2, 4 or 8.
-template <int ITEMS>
-__device__ __forceinline__ void warp_bitonic64(uint64_t (&v)[ITEMS], uint32_t lane) {
+template <int ITEMS, typename V = uint64_t>
+__device__ __forceinline__ void warp_bitonic64(V (&v)[ITEMS], uint32_t lane) {
     constexpr uint32_t P = 32 * ITEMS;
 #pragma unroll
     for (uint32_t kk = 2; kk <= P; kk <<= 1) {
@@ -406,7 +406,7 @@ __device__ __forceinline__ void warp_bitonic64(uint64_t (&v)[ITEMS], uint32_t la
                 const uint32_t lm = j / ITEMS;
 #pragma unroll
                 for (int i = 0; i < ITEMS; ++i) {
-                    const uint64_t o = __shfl_xor_sync(0xffffffffu, v[i], lm);
+                    const V o = __shfl_xor_sync(0xffffffffu, v[i], lm);
                     const uint32_t e = lane * ITEMS + i;
                     const bool keep_min = ((lane & lm) == 0) == ((e & kk) == 0);
                     v[i] = keep_min ? (o < v[i] ? o : v[i]) : (o > v[i] ? o : v[i]);
@@ -414,24 +414,25 @@ __device__ __forceinline__ void warp_bitonic64(uint64_t (&v)[ITEMS], uint32_t la
             } else {
                 if constexpr (ITEMS > 4) {
                     if (j == 4) {
-                        stage_local64<ITEMS, 4>(v, kk, lane);
+                        stage_local64<ITEMS, 4, V>(v, kk, lane);
                         continue;
                     }
                 }
                 if constexpr (ITEMS > 2) {
                     if (j == 2) {
-                        stage_local64<ITEMS, 2>(v, kk, lane);
+                        stage_local64<ITEMS, 2, V>(v, kk, lane);
                         continue;
                     }
                 }
-                if constexpr (ITEMS > 1) stage_local64<ITEMS, 1>(v, kk, lane);
+                if constexpr (ITEMS > 1) stage_local64<ITEMS, 1, V>(v, kk, lane);
             }
         }
     }
 }
 
 // Merge-path split over two sorted uint64 runs (values distinct).
-__device__ __forceinline__ uint32_t merge_split64(const uint64_t *s, uint32_t a0, uint32_t la,
+template <typename V = uint64_t>
+__device__ __forceinline__ uint32_t merge_split64(const V *s, uint32_t a0, uint32_t la,
                                                   uint32_t b0, uint32_t lb, uint32_t d) {
     uint32_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
     while (lo < hi) {
@@ -653,6 +654,61 @@ __device__ __forceinline__ void sort_window_runs(const ulonglong2 *sk, uint64_t 
             sv[pad(j)] = v;
         }
     }
+}
+
+// 32-bit packed keys for a first sort: the 21 window bits after the common
+// prefix and the 11-bit position.  Their order is the 64-bit packed order
+// except among keys whose 21 bits tie; see block_class.
+constexpr uint32_t NARROW_SHIFT = 64 - 21;  // 64-bit packed key >> this = the 21 bits
+
+__device__ __forceinline__ uint32_t sort_key32(const Key &k, uint32_t f, uint32_t pos) {
+    return (uint32_t)(window64(k, f) >> 32) & ~(uint32_t)POS_MASK | pos;
+}
+
+// In sv[0..len), the 64-bit packed keys of records in 32-bit order: runs of
+// keys whose top 21 bits tie are put into 64-bit order in place by the
+// thread that owns the run's first entry (insertion sort); returns false in
+// that thread when a run is longer than FIX_RUN_CAP (the caller then sorts
+// the segment on 64-bit keys from scratch).
+__device__ __forceinline__ bool sort_narrow_runs(uint64_t *sv, uint32_t len, uint32_t t,
+                                                 uint32_t threads) {
+    bool ok = true;
+    for (uint32_t e = t; e + 1 < len; e += threads) {
+        const uint64_t w = sv[pad(e)] >> NARROW_SHIFT;
+        if ((sv[pad(e + 1)] >> NARROW_SHIFT) != w) continue;
+        if (e > 0 && (sv[pad(e - 1)] >> NARROW_SHIFT) == w) continue;  // not the run's start
+        uint32_t r = e + 2;
+        while (r < len && (sv[pad(r)] >> NARROW_SHIFT) == w && r - e <= FIX_RUN_CAP) ++r;
+        if (r - e > FIX_RUN_CAP) {
+            ok = false;
+            continue;
+        }
+        for (uint32_t i = e + 1; i < r; ++i) {
+            const uint64_t v = sv[pad(i)];
+            uint32_t j = i;
+            while (j > e && sv[pad(j - 1)] > v) {
+                sv[pad(j)] = sv[pad(j - 1)];
+                --j;
+            }
+            sv[pad(j)] = v;
+        }
+    }
+    return ok;
+}
+
+template <int ITEMS>
+__device__ __forceinline__ void warp_run_packed32(const ulonglong2 *sk, uint32_t *sv32,
+                                                  uint32_t base, uint32_t len, uint32_t f,
+                                                  uint32_t lane) {
+    uint32_t v[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t e = base + lane * ITEMS + i;
+        v[i] = e < len ? sort_key32(to_key(sk[pad(e)]), f, e) : ~0u;
+    }
+    warp_bitonic64<ITEMS, uint32_t>(v, lane);
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) sv32[pad(base + lane * ITEMS + i)] = v[i];
 }
 
 // One warp: packed keys of the records at slots base .. base + 32*ITEMS - 1
@@ -1393,12 +1449,19 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     const Key s0 = to_key(smp[0]), sl = to_key(smp[u - 1]);
     const uint32_t f = u >= 2 ? clz128(s0.hi ^ sl.hi, s0.lo ^ sl.lo) : 128u;
     if (f < 128) {
+        // The splitters' window bits first (non-decreasing, as the splitters
+        // are sorted), into the packed-key area, which is free by now; then
+        // each table entry is a binary search over those 16-bit values.
+        uint16_t *wb = reinterpret_cast<uint16_t *>(sv);
+        for (uint32_t j = threadIdx.x; j < u; j += SAMPLE_THREADS)
+            wb[j] = (uint16_t)window_bits(to_key(smp[j]), f);
+        __syncthreads();
         uint16_t *T = tbl + (uint64_t)si * TBL_STRIDE;
         for (uint32_t wv = threadIdx.x; wv <= (uint32_t)TBL_N; wv += SAMPLE_THREADS) {
             uint32_t lo = 0, hi = u;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (window_bits(to_key(smp[mid]), f) < wv)
+                if (wb[mid] < wv)
                     lo = mid + 1;
                 else
                     hi = mid;
@@ -2428,12 +2491,13 @@ __device__ __noinline__ void group_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
 
 // Pairwise merge-path merges of the sorted packed-key runs of BLOCK_RUN in
 // sv[0..span) until one run is left; SMALL_ITEMS outputs per thread and pass.
-template <int GT>
-__device__ __forceinline__ void group_merge_passes64(uint64_t *sv, uint32_t span, uint32_t t,
+template <int GT, typename V = uint64_t>
+__device__ __forceinline__ void group_merge_passes64(V *sv, uint32_t span, uint32_t t,
                                                      uint32_t gi) {
+    constexpr V VMAX = (V)~(V)0;
     for (uint32_t run = BLOCK_RUN; run < span; run <<= 1) {
         const uint32_t o = t * SMALL_ITEMS;
-        uint64_t ov[SMALL_ITEMS];
+        V ov[SMALL_ITEMS];
         const bool active = o < span;
         if (active) {
             const uint32_t a0 = o / (2 * run) * (2 * run);
@@ -2441,12 +2505,12 @@ __device__ __forceinline__ void group_merge_passes64(uint64_t *sv, uint32_t span
             const uint32_t la = min(run, span - a0);
             const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
             const uint32_t d = o - a0;
-            uint32_t ia = merge_split64(sv, a0, la, b0, lb, d);
+            uint32_t ia = merge_split64<V>(sv, a0, la, b0, lb, d);
             uint32_t ib = d - ia;
 #pragma unroll
             for (int i = 0; i < SMALL_ITEMS; ++i) {
-                const uint64_t va = ia < la ? sv[pad(a0 + ia)] : ~0ull;
-                const uint64_t vb = ib < lb ? sv[pad(b0 + ib)] : ~0ull;
+                const V va = ia < la ? sv[pad(a0 + ia)] : VMAX;
+                const V vb = ib < lb ? sv[pad(b0 + ib)] : VMAX;
                 const bool take_a = ib >= lb || (ia < la && va < vb);
                 ov[i] = take_a ? va : vb;
                 ia += take_a;
@@ -2465,7 +2529,10 @@ __device__ __forceinline__ void group_merge_passes64(uint64_t *sv, uint32_t span
 // The CTAs cta0 .. cta0 + ncta - 1 of the launch sort the segments of one
 // size class (list S of nS segments) with groups of GT threads.  LEAN: the
 // finish takes neighbour LCPs from the packed windows (finish_packed).
-template <int GT, bool LEAN = false>
+// VAR 0: full-key finish; 1: LEAN; 2: LEAN, and the first sort is on 32-bit
+// packed keys (half the work of the 64-bit network), widened to 64-bit keys
+// afterwards; ties on their 21 window bits are then put in order in place.
+template <int GT, int VAR = 0>
 __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__restrict__ S,
                                             uint32_t nS, uint32_t cta0, uint32_t ncta, Seg *N,
                                             Counters *c) {
@@ -2475,7 +2542,8 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
     static_assert(G * PADC == SMALL_PAD, "group slots");
     extern __shared__ __align__(16) unsigned char block_smem[];
     __shared__ uint64_t red[2][SMALL_THREADS / 32];
-    __shared__ int ok_flag[G], fix_flag[G];
+    __shared__ int ok_flag[G], fix_flag[G], nar_flag[G];
+    constexpr bool LEAN = VAR >= 1;
     const uint32_t gi = threadIdx.x / GT, t = threadIdx.x % GT;
     const uint32_t lane = threadIdx.x & 31, gw = t >> 5, w = threadIdx.x >> 5;
     ulonglong2 *sk_all = reinterpret_cast<ulonglong2 *>(block_smem);
@@ -2514,7 +2582,7 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
                 }
             }
         }
-        if (t == 0) ok_flag[gi] = fix_flag[gi] = 1;
+        if (t == 0) ok_flag[gi] = fix_flag[gi] = nar_flag[gi] = 1;
         group_sync<GT>(gi);
         // f: first bit in which the keys differ.
         {
@@ -2545,9 +2613,40 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
         bool packed = false;
         const uint32_t f = (dh | dl) ? clz128(dh, dl) : 128u;
         if (f < 128) {
-            if (gw < nruns) warp_run_packed<SMALL_ITEMS>(sk, sv, gw * BLOCK_RUN, s.len, f, lane);
-            group_sync<GT>(gi);
-            group_merge_passes64<GT>(sv, span, t, gi);
+            bool sorted64 = false;
+            if constexpr (VAR == 2) {
+                uint32_t *sv32 = reinterpret_cast<uint32_t *>(sv);  // same bytes
+                if (gw < nruns)
+                    warp_run_packed32<SMALL_ITEMS>(sk, sv32, gw * BLOCK_RUN, s.len, f, lane);
+                group_sync<GT>(gi);
+                group_merge_passes64<GT, uint32_t>(sv32, span, t, gi);
+                // Widen to 64-bit packed keys in this order; the two arrays
+                // share their bytes, so the values pass through registers.
+                const uint32_t o = t * SMALL_ITEMS;
+                uint32_t pv[SMALL_ITEMS];
+#pragma unroll
+                for (int i = 0; i < SMALL_ITEMS; ++i)
+                    pv[i] = o + i < span ? sv32[pad(o + i)] : 0u;
+                group_sync<GT>(gi);
+#pragma unroll
+                for (int i = 0; i < SMALL_ITEMS; ++i) {
+                    const uint32_t e = o + i;
+                    if (e < s.len) {
+                        const uint32_t pos = pv[i] & (uint32_t)POS_MASK;
+                        sv[pad(e)] = sort_key(to_key(sk[pad(pos)]), f, pos);
+                    }
+                }
+                group_sync<GT>(gi);
+                if (!sort_narrow_runs(sv, s.len, t, GT)) nar_flag[gi] = 0;
+                group_sync<GT>(gi);
+                sorted64 = nar_flag[gi] != 0;
+            }
+            if (!sorted64) {
+                if (gw < nruns)
+                    warp_run_packed<SMALL_ITEMS>(sk, sv, gw * BLOCK_RUN, s.len, f, lane);
+                group_sync<GT>(gi);
+                group_merge_passes64<GT>(sv, span, t, gi);
+            }
             if (!window_pairs_ok_ind(sk, sv, s.len, t, GT)) ok_flag[gi] = 0;
             group_sync<GT>(gi);
             packed = ok_flag[gi] != 0;
@@ -2581,11 +2680,11 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
 
 // One size class per launch (a single launch for all three inlines all
 // three bodies and spills more; measured slower).
-template <int GT, bool LEAN>
+template <int GT, int VAR>
 __global__ void __launch_bounds__(SMALL_THREADS, 3) k_block(SortArgs a, const Seg *__restrict__ S,
                                                             Span sp, Seg *N, Counters *c) {
     const uint32_t lo = count_of(sp.lo);
-    block_class<GT, LEAN>(a, S + lo, count_of(sp.hi) - lo, 0, gridDim.x, N, c);
+    block_class<GT, VAR>(a, S + lo, count_of(sp.hi) - lo, 0, gridDim.x, N, c);
 }
 
 // ---- segments of 257..SMALL_CAP strings, with the next segment prefetched ---
@@ -2971,17 +3070,23 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(Scatter2Smem));
     cudaFuncSetAttribute(k_warp8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W8_SMEM);
-    cudaFuncSetAttribute(k_block<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<64, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
-    cudaFuncSetAttribute(k_block<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
-    cudaFuncSetAttribute(k_block<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
-    cudaFuncSetAttribute(k_block<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<128, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
-    cudaFuncSetAttribute(k_block<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<128, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
-    cudaFuncSetAttribute(k_block<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_block<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<256, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BLOCK_SMEM);
+    cudaFuncSetAttribute(k_block<256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK_SMEM);
     cudaFuncSetAttribute(k_block2<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BLOCK2_SMEM);
@@ -3183,21 +3288,22 @@ void launch_block(const SortArgs &a, const Seg *S, Span sp, int cls, Seg *N, Cou
             k_block2<256><<<grid, SMALL_THREADS, BLOCK2_SMEM, st>>>(a, S, sp, N, c);
         return;
     }
-    if (a.block_lean) {
-        if (cls == 0)
-            k_block<64, true><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
-        else if (cls == 1)
-            k_block<128, true><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
-        else
-            k_block<256, true><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
-        return;
-    }
-    if (cls == 0)
-        k_block<64, false><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
-    else if (cls == 1)
-        k_block<128, false><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+#define SS_BLOCK_LAUNCH(VAR)                                                           \
+    do {                                                                               \
+        if (cls == 0)                                                                  \
+            k_block<64, VAR><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);  \
+        else if (cls == 1)                                                             \
+            k_block<128, VAR><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c); \
+        else                                                                           \
+            k_block<256, VAR><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c); \
+    } while (0)
+    if (a.block_lean == 2)
+        SS_BLOCK_LAUNCH(2);
+    else if (a.block_lean == 1)
+        SS_BLOCK_LAUNCH(1);
     else
-        k_block<256, false><<<grid, SMALL_THREADS, BLOCK_SMEM, st>>>(a, S, sp, N, c);
+        SS_BLOCK_LAUNCH(0);
+#undef SS_BLOCK_LAUNCH
 }
 
 void launch_equal(const SortArgs &a, const Seg *E, Span sp, Seg *N, Counters *c, int grid,

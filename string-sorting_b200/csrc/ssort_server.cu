@@ -163,7 +163,7 @@ struct ssort_server {
         a.warp1_deep = ctx->warp1_deep;
         a.l2_prefetch = ctx->l2_prefetch ? 1u : 0u;
         a.scatter_staged_idx = ctx->scatter_variant;
-        a.block_lean = ctx->block_lean ? 1u : 0u;
+        a.block_lean = ctx->block_lean;
         a.max_splitters = (1u << (ctx->digit_bits - 1)) - 1;
         return a;
     }

@@ -145,7 +145,7 @@ def _tied_window_strings(n, lead, alpha, seed):
     return out
 
 
-@pytest.mark.parametrize("prefetch,lean", [(0, 0), (0, 1), (1, 0)])
+@pytest.mark.parametrize("prefetch,lean", [(0, 0), (0, 1), (0, 2), (1, 0)])
 @pytest.mark.parametrize("n,lead,alpha,full", [(200, 2, 26, False), (1500, 2, 26, False),
                                                (700, 2, 26, False), (1500, 1, 2, True),
                                                (200, 1, 2, True), (300, 1, 2, True)])

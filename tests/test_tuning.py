@@ -31,6 +31,7 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_DIGIT_BITS, 9),
     (pyssort.SSORT_PARAM_SCATTER, 1),
     (pyssort.SSORT_PARAM_BLOCK_LEAN, 1),
+    (pyssort.SSORT_PARAM_BLOCK_LEAN, 2),
     (pyssort.SSORT_PARAM_GRAPH, 0),
 ]
 
@@ -88,7 +89,7 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 2),
                              (pyssort.SSORT_PARAM_L2_PREFETCH, 2),
                              (pyssort.SSORT_PARAM_GRAPH, 3),
-                             (pyssort.SSORT_PARAM_BLOCK_LEAN, 2),
+                             (pyssort.SSORT_PARAM_BLOCK_LEAN, 3),
                              (pyssort.SSORT_PARAM_GRAPH_MAX_LEVELS, 0),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 7),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 11),
@@ -117,7 +118,7 @@ def test_autotune_then_sort_stays_exact():
         assert t["block_prefetch"] in (0, 1) and t["l2_prefetch"] in (0, 1)
         assert t["graph"] in (0, 2)
         # base, then every other candidate of every knob
-        assert t["trials"] == 2 + 2 * (2 + 2 + 2 + 1 + 1 + 1 + 1 + 1 + 1)
+        assert t["trials"] == 2 + 2 * (2 + 2 + 2 + 1 + 1 + 1 + 1 + 2 + 1)
         # a later sort of the same class uses the recorded values
         d_perm = torch.empty(ss.n, dtype=torch.int32, device="cuda")
         d_lcp = torch.empty(ss.n, dtype=torch.int32, device="cuda")
