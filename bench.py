@@ -44,7 +44,8 @@ PARAMS = {"target_bucket": pyssort.SSORT_PARAM_TARGET_BUCKET,
           "l2_prefetch": pyssort.SSORT_PARAM_L2_PREFETCH,
           "digit_bits": pyssort.SSORT_PARAM_DIGIT_BITS,
           "scatter": pyssort.SSORT_PARAM_SCATTER,
-          "block_lean": pyssort.SSORT_PARAM_BLOCK_LEAN}
+          "block_lean": pyssort.SSORT_PARAM_BLOCK_LEAN,
+          "match_vote": pyssort.SSORT_PARAM_MATCH_VOTE}
 
 
 def apply_params(sorter, args):

@@ -251,6 +251,9 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         registers at three CTAs per SM; 1: it copies the
                                         next segment's records into shared memory while it
                                         sorts the current one (two CTAs per SM) */
+#define SSORT_PARAM_MATCH_VOTE 13    /* 1 (default): the partition's count kernel finds the
+                                        lanes of a warp that share a bucket with one ballot
+                                        per bucket-id bit; 0: with __match_any_sync */
 #define SSORT_PARAM_BLOCK_LEAN 12    /* 1: the CTA sort takes the LCPs of neighbours whose
                                         packed windows differ from the windows alone and
                                         reads full keys only for equal windows; 2: that, and
@@ -273,7 +276,8 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         conditional loops (no host round trip between
                                         kernels; one host read per up to 64 rounds);
                                         0: the host drives the rounds; 2 (default): the
-                                        graph from the second of two sorts in a row with
+                                        graph for batched sorts and sorts of at most 2^24
+                                        strings, from the second of two sorts in a row with
                                         the same buffers and size on (building a graph
                                         costs more than a host-driven sort) */
 #define SSORT_PARAM_GRAPH_MAX_LEVELS 8 /* 1..4096 (default 4096): partition levels one round

@@ -199,10 +199,15 @@ int ssort_ctx::graph_build(const SortArgs &a) {
     return SSORT_OK;
 }
 
-// Whether this sort runs through the graph: always in mode 1; in mode 2 when
-// a graph for these arguments exists or the previous sort had them too.
-bool ssort_ctx::graph_wanted(const SortArgs &a) {
+// Whether this sort runs through the graph: always in mode 1; in mode 2 for
+// batched sorts and sorts of at most GRAPH_AUTO_MAX_N strings (where launch
+// and host round-trip costs are a large share; large single sorts keep the
+// host loop, whose round 0 overlaps the on-chip sorts with the partition on a
+// second stream), when a graph for these arguments exists or the previous
+// sort had them too.
+bool ssort_ctx::graph_wanted(const SortArgs &a, bool batched) {
     if (graph_mode == 1) return true;
+    if (!batched && a.n > GRAPH_AUTO_MAX_N) return false;
     std::vector<unsigned char> k = graph_key(a, *this);
     if (!gkey.empty() && k == gkey) return true;
     const bool repeat = k == last_key;

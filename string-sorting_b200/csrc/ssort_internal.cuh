@@ -139,6 +139,7 @@ struct SortArgs {
     uint32_t l2_prefetch;    // partition kernels stream their next tile into L2 ahead
     uint32_t scatter_staged_idx;  // scatter stages indices only (k_scatter2)
     uint32_t block_lean;     // CTA sort: neighbour LCPs from the packed windows
+    uint32_t match_vote;     // count kernel ranks with ballots instead of the match unit
     uint32_t max_splitters;  // splitters per partition pass, 2^(digit bits - 1) - 1 <= KMAX
     // Per segment size class (floor(log2 len)): the wanted strings per range
     // bucket autotuned for that class (0: target_bucket).  Set for batched
@@ -157,6 +158,7 @@ struct SortArgs {
 // kernels advance them and set the loops' conditions).  One per workspace.
 constexpr uint32_t GRAPH_MAX_LEVELS = 4096;  // partition levels per round
 constexpr uint32_t GRAPH_ROUNDS_PER_LAUNCH = 64;
+constexpr uint32_t GRAPH_AUTO_MAX_N = 16u << 20;  // single sorts the auto mode runs as a graph
 
 struct GraphState {
     uint32_t n_cur;    // segments of the current round (list R)

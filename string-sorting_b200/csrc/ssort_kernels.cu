@@ -166,6 +166,20 @@ __device__ __forceinline__ uint32_t find_seg(const uint32_t *base, uint32_t n, u
     return lo;
 }
 
+// Lanes of the warp whose value v equals this lane's, for values below
+// 2^bits: one ballot per bit (lanes agreeing on every bit are the peers).
+// The same set as __match_any_sync(full, v), from vote and logic
+// instructions instead of the match unit.  Warp-collective; bits is
+// warp-uniform.
+__device__ __forceinline__ uint32_t match_bits(uint32_t v, uint32_t bits) {
+    uint32_t peers = 0xffffffffu;
+    for (uint32_t k = 0; k < bits; ++k) {
+        const uint32_t m = __ballot_sync(0xffffffffu, (v >> k) & 1u);
+        peers &= ((v >> k) & 1u) ? m : ~m;
+    }
+    return peers;
+}
+
 // Warp-aggregated append to a list counter: all 32 lanes call it together;
 // each lane with `want` gets its own slot, at the cost of one atomic per warp
 // (appends from millions of small segments would otherwise serialise on one
@@ -1526,6 +1540,7 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
         const uint32_t u = nspl[si] & 0xFFFF, f = nspl[si] >> 16, nb = 2 * u + 1;
+        const uint32_t bbits = 32 - __clz(nb);  // bucket ids are 0..nb
         if (a.l2_prefetch && threadIdx.x == 0 && t + gridDim.x < total_tiles) {
             // the keys (or, when gathering, the indices) of this CTA's next tile
             const uint32_t t2 = t + gridDim.x;
@@ -1606,7 +1621,8 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
         for (int c = 0; c < PART_ITEMS; ++c) {
             const uint32_t e = lo + c * 32 + lane;
             const uint32_t b = e < s.len ? classify_tbl(sm.spl, sm.tbl, u, f, kk[c]) : nb;
-            const uint32_t peers = __match_any_sync(0xffffffffu, b);
+            const uint32_t peers =
+                a.match_vote ? match_bits(b, bbits) : __match_any_sync(0xffffffffu, b);
             const uint32_t r = __popc(peers & lt);
             const uint32_t base = hist[w][b];
             __syncwarp();

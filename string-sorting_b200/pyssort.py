@@ -44,6 +44,7 @@ SSORT_PARAM_L2_PREFETCH = 9
 SSORT_PARAM_DIGIT_BITS = 10
 SSORT_PARAM_SCATTER = 11
 SSORT_PARAM_BLOCK_LEAN = 12
+SSORT_PARAM_MATCH_VOTE = 13
 
 
 class SsortError(RuntimeError):
