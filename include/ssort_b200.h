@@ -251,9 +251,9 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         registers at three CTAs per SM; 1: it copies the
                                         next segment's records into shared memory while it
                                         sorts the current one (two CTAs per SM) */
-#define SSORT_PARAM_MATCH_VOTE 13    /* 1 (default): the partition's count kernel finds the
-                                        lanes of a warp that share a bucket with one ballot
-                                        per bucket-id bit; 0: with __match_any_sync */
+#define SSORT_PARAM_MATCH_VOTE 13    /* 1: the partition's count kernel finds the lanes of a
+                                        warp that share a bucket with one ballot per
+                                        bucket-id bit; 0 (default): with __match_any_sync */
 #define SSORT_PARAM_BLOCK_LEAN 12    /* 1: the CTA sort takes the LCPs of neighbours whose
                                         packed windows differ from the windows alone and
                                         reads full keys only for equal windows; 2: that, and
@@ -275,7 +275,7 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         graph whose rounds and partition levels are
                                         conditional loops (no host round trip between
                                         kernels; one host read per up to 64 rounds);
-                                        0: the host drives the rounds; 2 (default): the
+                                        0 (default): the host drives the rounds; 2: the
                                         graph for batched sorts and sorts of at most 2^24
                                         strings, from the second of two sorts in a row with
                                         the same buffers and size on (building a graph

@@ -1024,7 +1024,7 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                                   {SSORT_PARAM_BLOCK_PREFETCH, {1, 0}},
                                   {SSORT_PARAM_L2_PREFETCH, {1, 0}},
                                   {SSORT_PARAM_BLOCK_LEAN, {0, 1, 2}},
-                                  {SSORT_PARAM_GRAPH, {2, 0}}};
+                                  {SSORT_PARAM_GRAPH, {0, 1}}};
             auto get = [&](int p) -> int64_t {
                 switch (p) {
                     case SSORT_PARAM_TARGET_BUCKET: return ctx->target_bucket;

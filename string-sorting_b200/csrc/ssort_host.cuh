@@ -86,15 +86,16 @@ struct ssort_ctx {
     bool l2_prefetch = true;     // partition kernels prefetch their next tile into L2
     uint32_t digit_bits = 10;    // a partition pass makes at most 2^digit_bits buckets
     uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
-    bool match_vote = true;        // count kernel ranks keys with ballots
+    bool match_vote = false;       // count kernel ranks keys with ballots
     // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
     // key it was built for, three streams to capture nested conditional
     // bodies on, and a pinned copy of the loop state.
-    // 0: host loop; 1: device-driven loop always; 2 (auto): the device-driven
-    // loop for batched sorts and sorts of at most GRAPH_AUTO_MAX_N strings,
-    // once a sort repeats the previous sort's arguments (buffers, size,
-    // workspace), since building a graph costs more than one host-driven sort
-    uint32_t graph_mode = 2;
+    // 0 (default): host loop; 1: device-driven loop always; 2 (auto): the
+    // device-driven loop for batched sorts and sorts of at most
+    // GRAPH_AUTO_MAX_N strings, once a sort repeats the previous sort's
+    // arguments (buffers, size, workspace), since building a graph costs more
+    // than one host-driven sort
+    uint32_t graph_mode = 0;
     std::vector<unsigned char> last_key;  // arguments of the previous sort (auto mode)
     uint32_t graph_max_levels = ssort::GRAPH_MAX_LEVELS;
     cudaGraph_t graph = nullptr;

@@ -119,10 +119,10 @@ def test_graph_rebuilds_for_new_buffers():
 
 
 def test_auto_mode_uses_the_graph_from_the_second_identical_sort():
-    """The default (SSORT_PARAM_GRAPH = 2): a sort whose buffers and size
-    differ from the previous sort's runs on the host loop; the second sort
-    in a row with the same arguments builds and runs the graph, and so do
-    later ones; results stay the oracle's throughout."""
+    """SSORT_PARAM_GRAPH = 2: a sort whose buffers and size differ from the
+    previous sort's runs on the host loop; the second sort in a row with the
+    same arguments builds and runs the graph, and so do later ones; results
+    stay the oracle's throughout."""
     torch = pytest.importorskip("torch")
     ss = pyssort.gen_urls(400_000, seed=24)
     rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
@@ -132,6 +132,7 @@ def test_auto_mode_uses_the_graph_from_the_second_identical_sort():
     d_lcp = torch.empty(ss.n, dtype=torch.int32, device="cuda")
     used = []
     with pyssort.Sorter(0) as s:
+        s.set_param(pyssort.SSORT_PARAM_GRAPH, 2)
         for _ in range(3):
             s.sort_device(d_arena, ss.arena.nbytes, d_offs, 8, ss.n, d_perm, d_lcp)
             torch.cuda.synchronize()

@@ -32,8 +32,8 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_SCATTER, 1),
     (pyssort.SSORT_PARAM_BLOCK_LEAN, 1),
     (pyssort.SSORT_PARAM_BLOCK_LEAN, 2),
-    (pyssort.SSORT_PARAM_GRAPH, 0),
-    (pyssort.SSORT_PARAM_MATCH_VOTE, 0),
+    (pyssort.SSORT_PARAM_GRAPH, 2),
+    (pyssort.SSORT_PARAM_MATCH_VOTE, 1),
 ]
 
 
@@ -118,7 +118,7 @@ def test_autotune_then_sort_stays_exact():
         assert t["tuned_ms"] <= t["default_ms"]
         assert t["digit_bits"] in (8, 9, 10)
         assert t["block_prefetch"] in (0, 1) and t["l2_prefetch"] in (0, 1)
-        assert t["graph"] in (0, 2)
+        assert t["graph"] in (0, 1)
         # base, then every other candidate of every knob
         assert t["trials"] == 2 + 2 * (2 + 2 + 2 + 1 + 1 + 1 + 1 + 2 + 1)
         # a later sort of the same class uses the recorded values
