@@ -45,7 +45,8 @@ PARAMS = {"target_bucket": pyssort.SSORT_PARAM_TARGET_BUCKET,
           "digit_bits": pyssort.SSORT_PARAM_DIGIT_BITS,
           "scatter": pyssort.SSORT_PARAM_SCATTER,
           "block_lean": pyssort.SSORT_PARAM_BLOCK_LEAN,
-          "match_vote": pyssort.SSORT_PARAM_MATCH_VOTE}
+          "match_vote": pyssort.SSORT_PARAM_MATCH_VOTE,
+          "warp_merge": pyssort.SSORT_PARAM_WARP_MERGE}
 
 
 def apply_params(sorter, args):

@@ -285,6 +285,7 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     a.scatter_staged_idx = scatter_variant;
     a.block_lean = block_lean;
     a.match_vote = match_vote ? 1u : 0u;
+    a.warp_merge = warp_merge ? 1u : 0u;
     a.max_splitters = (1u << (digit_bits - 1)) - 1;
     std::copy(std::begin(class_targets), std::end(class_targets), std::begin(a.target_by_class));
     a.key2 = key2;
@@ -748,6 +749,10 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
         case SSORT_PARAM_DIGIT_BITS:
             if (value < 8 || value > 10) return fail(SSORT_EINVAL, "digit_bits out of range (8..10)");
             ctx->digit_bits = (uint32_t)value;
+            return SSORT_OK;
+        case SSORT_PARAM_WARP_MERGE:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "warp_merge must be 0 or 1");
+            ctx->warp_merge = value != 0;
             return SSORT_OK;
         case SSORT_PARAM_MATCH_VOTE:
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "match_vote must be 0 or 1");

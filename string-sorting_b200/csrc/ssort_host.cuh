@@ -87,6 +87,7 @@ struct ssort_ctx {
     uint32_t digit_bits = 10;    // a partition pass makes at most 2^digit_bits buckets
     uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
     bool match_vote = false;       // count kernel ranks keys with ballots
+    bool warp_merge = false;       // warp sorts: local networks + merge passes
     // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
     // key it was built for, three streams to capture nested conditional
     // bodies on, and a pinned copy of the loop state.

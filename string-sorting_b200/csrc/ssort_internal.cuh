@@ -140,6 +140,7 @@ struct SortArgs {
     uint32_t scatter_staged_idx;  // scatter stages indices only (k_scatter2)
     uint32_t block_lean;     // CTA sort: neighbour LCPs from the packed windows
     uint32_t match_vote;     // count kernel ranks with ballots instead of the match unit
+    uint32_t warp_merge;     // warp sorts of packed keys: local networks + merge passes
     uint32_t max_splitters;  // splitters per partition pass, 2^(digit bits - 1) - 1 <= KMAX
     // Per segment size class (floor(log2 len)): the wanted strings per range
     // bucket autotuned for that class (0: target_bucket).  Set for batched

@@ -725,9 +725,75 @@ __device__ __forceinline__ void warp_run_packed32(const ulonglong2 *sk, uint32_t
     for (int i = 0; i < ITEMS; ++i) sv32[pad(base + lane * ITEMS + i)] = v[i];
 }
 
-// One warp: packed keys of the records at slots base .. base + 32*ITEMS - 1
-// (positions >= len pad with all-ones), sorted, stored to sv.
+// Compare-exchange: afterwards a <= b.
+__device__ __forceinline__ void cas64(uint64_t &a, uint64_t &b) {
+    const bool lt = a < b;
+    const uint64_t lo = lt ? a : b, hi = lt ? b : a;
+    a = lo;
+    b = hi;
+}
+
+// Sorts ITEMS (2, 4 or 8) values held by one thread: optimal sorting networks
+// of 1, 5 and 19 comparators.
 template <int ITEMS>
+__device__ __forceinline__ void sort_local64(uint64_t (&v)[ITEMS]) {
+    if constexpr (ITEMS == 2) {
+        cas64(v[0], v[1]);
+    } else if constexpr (ITEMS == 4) {
+        cas64(v[0], v[1]); cas64(v[2], v[3]);
+        cas64(v[0], v[2]); cas64(v[1], v[3]);
+        cas64(v[1], v[2]);
+    } else {
+        static_assert(ITEMS == 8, "2, 4 or 8 values per thread");
+        cas64(v[0], v[2]); cas64(v[1], v[3]); cas64(v[4], v[6]); cas64(v[5], v[7]);
+        cas64(v[0], v[4]); cas64(v[1], v[5]); cas64(v[2], v[6]); cas64(v[3], v[7]);
+        cas64(v[0], v[1]); cas64(v[2], v[3]); cas64(v[4], v[5]); cas64(v[6], v[7]);
+        cas64(v[2], v[4]); cas64(v[3], v[5]);
+        cas64(v[1], v[4]); cas64(v[3], v[6]);
+        cas64(v[1], v[2]); cas64(v[3], v[4]); cas64(v[5], v[6]);
+    }
+}
+
+// One warp sorts the 32 * ITEMS values v (lane l holds any ITEMS of them)
+// into sv[pad(base .. base + 32 * ITEMS)]: every lane sorts its own values in
+// registers, then merge-path passes (synchronised by __syncwarp only) double
+// the sorted runs up to the whole warp.  Fewer instructions than the bitonic
+// network, whose 15 cross-lane stages each move every value through a
+// shuffle; equal values (the all-ones padding) merge consistently.
+template <int ITEMS>
+__device__ __forceinline__ void warp_merge_sort64(uint64_t (&v)[ITEMS], uint64_t *sv,
+                                                  uint32_t base, uint32_t lane) {
+    sort_local64<ITEMS>(v);
+    const uint32_t o = lane * ITEMS;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) sv[pad(base + o + i)] = v[i];
+    __syncwarp();
+#pragma unroll
+    for (uint32_t run = ITEMS; run < 32 * ITEMS; run <<= 1) {
+        const uint32_t a0 = base + (o & ~(2 * run - 1)), b0 = a0 + run;
+        const uint32_t d = o & (2 * run - 1);
+        uint32_t ia = merge_split64(sv, a0, run, b0, run, d);
+        uint32_t ib = d - ia;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const uint64_t va = ia < run ? sv[pad(a0 + ia)] : ~0ull;
+            const uint64_t vb = ib < run ? sv[pad(b0 + ib)] : ~0ull;
+            const bool take_a = ib >= run || (ia < run && va < vb);
+            v[i] = take_a ? va : vb;
+            ia += take_a;
+            ib += !take_a;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) sv[pad(base + o + i)] = v[i];
+        __syncwarp();
+    }
+}
+
+// One warp: packed keys of the records at slots base .. base + 32*ITEMS - 1
+// (positions >= len pad with all-ones), sorted, stored to sv; by the bitonic
+// network or (MERGE) by warp_merge_sort64.
+template <int ITEMS, bool MERGE = false>
 __device__ __forceinline__ void warp_run_packed(const ulonglong2 *sk, uint64_t *sv,
                                                 uint32_t base, uint32_t len, uint32_t f,
                                                 uint32_t lane) {
@@ -737,9 +803,13 @@ __device__ __forceinline__ void warp_run_packed(const ulonglong2 *sk, uint64_t *
         const uint32_t e = base + lane * ITEMS + i;
         v[i] = e < len ? sort_key(to_key(sk[pad(e)]), f, e) : ~0ull;
     }
-    warp_bitonic64<ITEMS>(v, lane);
+    if constexpr (MERGE) {
+        warp_merge_sort64<ITEMS>(v, sv, base, lane);
+    } else {
+        warp_bitonic64<ITEMS>(v, lane);
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) sv[pad(base + lane * ITEMS + i)] = v[i];
+        for (int i = 0; i < ITEMS; ++i) sv[pad(base + lane * ITEMS + i)] = v[i];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1373,7 +1443,7 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
         uint64_t ov[8];
         const bool active = o < S;
         if (active) {
-            const uint32_t a0 = o / (2 * run) * (2 * run), b0 = a0 + run;
+            const uint32_t a0 = o & ~(2 * run - 1), b0 = a0 + run;  // run: a power of two
             const uint32_t d = o - a0;
             uint32_t ia = merge_split64(sv, a0, run, b0, run, d);
             uint32_t ib = d - ia;
@@ -2382,12 +2452,21 @@ __global__ void __launch_bounds__(WARP_THREADS, 3) k_warp8(SortArgs a, const Seg
         const uint32_t f = warp_diff_bit(sk, s.len, lane);
         bool packed = false;
         if (f < 128) {
-            if (P <= 64)
-                warp_run_packed<2>(sk, sv, 0, s.len, f, lane);
-            else if (P <= 128)
-                warp_run_packed<4>(sk, sv, 0, s.len, f, lane);
-            else
-                warp_run_packed<8>(sk, sv, 0, s.len, f, lane);
+            if (a.warp_merge) {
+                if (P <= 64)
+                    warp_run_packed<2, true>(sk, sv, 0, s.len, f, lane);
+                else if (P <= 128)
+                    warp_run_packed<4, true>(sk, sv, 0, s.len, f, lane);
+                else
+                    warp_run_packed<8, true>(sk, sv, 0, s.len, f, lane);
+            } else {
+                if (P <= 64)
+                    warp_run_packed<2>(sk, sv, 0, s.len, f, lane);
+                else if (P <= 128)
+                    warp_run_packed<4>(sk, sv, 0, s.len, f, lane);
+                else
+                    warp_run_packed<8>(sk, sv, 0, s.len, f, lane);
+            }
             __syncwarp();
             packed = __all_sync(0xffffffffu, window_pairs_ok_ind(sk, sv, s.len, lane, 32));
             if (!packed) {
@@ -2461,7 +2540,7 @@ __device__ __noinline__ void group_sort_full(ulonglong2 *sk, uint32_t *sx, uint3
         uint32_t ox[SMALL_ITEMS];
         const bool active = o < span;
         if (active) {
-            const uint32_t a0 = o / (2 * run) * (2 * run);
+            const uint32_t a0 = o & ~(2 * run - 1);  // run: a power of two
             const uint32_t b0 = a0 + run;
             const uint32_t la = min(run, span - a0);
             const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
@@ -2516,7 +2595,7 @@ __device__ __forceinline__ void group_merge_passes64(V *sv, uint32_t span, uint3
         V ov[SMALL_ITEMS];
         const bool active = o < span;
         if (active) {
-            const uint32_t a0 = o / (2 * run) * (2 * run);
+            const uint32_t a0 = o & ~(2 * run - 1);  // run: a power of two
             const uint32_t b0 = a0 + run;
             const uint32_t la = min(run, span - a0);
             const uint32_t lb = b0 < span ? min(run, span - b0) : 0u;
@@ -2658,8 +2737,12 @@ __device__ __forceinline__ void block_class(const SortArgs &a, const Seg *__rest
                 sorted64 = nar_flag[gi] != 0;
             }
             if (!sorted64) {
-                if (gw < nruns)
-                    warp_run_packed<SMALL_ITEMS>(sk, sv, gw * BLOCK_RUN, s.len, f, lane);
+                if (gw < nruns) {
+                    if (a.warp_merge)
+                        warp_run_packed<SMALL_ITEMS, true>(sk, sv, gw * BLOCK_RUN, s.len, f, lane);
+                    else
+                        warp_run_packed<SMALL_ITEMS>(sk, sv, gw * BLOCK_RUN, s.len, f, lane);
+                }
                 group_sync<GT>(gi);
                 group_merge_passes64<GT>(sv, span, t, gi);
             }

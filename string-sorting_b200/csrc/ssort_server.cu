@@ -165,6 +165,7 @@ struct ssort_server {
         a.scatter_staged_idx = ctx->scatter_variant;
         a.block_lean = ctx->block_lean;
         a.match_vote = ctx->match_vote ? 1u : 0u;
+        a.warp_merge = ctx->warp_merge ? 1u : 0u;
         a.max_splitters = (1u << (ctx->digit_bits - 1)) - 1;
         return a;
     }

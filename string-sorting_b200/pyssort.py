@@ -45,6 +45,7 @@ SSORT_PARAM_DIGIT_BITS = 10
 SSORT_PARAM_SCATTER = 11
 SSORT_PARAM_BLOCK_LEAN = 12
 SSORT_PARAM_MATCH_VOTE = 13
+SSORT_PARAM_WARP_MERGE = 14
 
 
 class SsortError(RuntimeError):

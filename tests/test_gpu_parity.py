@@ -145,11 +145,12 @@ def _tied_window_strings(n, lead, alpha, seed):
     return out
 
 
-@pytest.mark.parametrize("prefetch,lean", [(0, 0), (0, 1), (0, 2), (1, 0)])
+@pytest.mark.parametrize("prefetch,lean,merge", [(0, 0, 0), (0, 1, 0), (0, 2, 0), (1, 0, 0),
+                                                (0, 0, 1)])
 @pytest.mark.parametrize("n,lead,alpha,full", [(200, 2, 26, False), (1500, 2, 26, False),
                                                (700, 2, 26, False), (1500, 1, 2, True),
                                                (200, 1, 2, True), (300, 1, 2, True)])
-def test_tied_packed_windows(n, lead, alpha, full, prefetch, lean):
+def test_tied_packed_windows(n, lead, alpha, full, prefetch, lean, merge):
     """Segments of the one-warp (<= 256) and CTA (<= 2048) sorts whose packed
     keys tie: runs of up to 64 tied records are put in order in place, longer
     ones fall back to the full comparator; both give the oracle's order and
@@ -159,6 +160,7 @@ def test_tied_packed_windows(n, lead, alpha, full, prefetch, lean):
     with pyssort.Sorter(0) as sorter:
         sorter.set_param(pyssort.SSORT_PARAM_BLOCK_PREFETCH, prefetch)
         sorter.set_param(pyssort.SSORT_PARAM_BLOCK_LEAN, lean)
+        sorter.set_param(pyssort.SSORT_PARAM_WARP_MERGE, merge)
         perm, lcp = sorter.sort_host(arena, offs)
         full_sorted = sorter.stats().full_sorted
     ref_perm, ref_lcp = pyoracle.oracle_sort(arena, offs)
