@@ -254,10 +254,11 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
 #define SSORT_PARAM_MATCH_VOTE 13    /* 1: the partition's count kernel finds the lanes of a
                                         warp that share a bucket with one ballot per
                                         bucket-id bit; 0 (default): with __match_any_sync */
-#define SSORT_PARAM_WARP_MERGE 14    /* 1: the warp-level sorts of packed keys (one-warp and
-                                        CTA sorts) sort each lane's values with a sorting
-                                        network and merge runs with merge-path passes;
-                                        0 (default): a bitonic network across the warp */
+#define SSORT_PARAM_WARP_MERGE 14    /* 1 (default): the warp-level sorts of packed keys
+                                        (one-warp and CTA sorts) sort each lane's values
+                                        with a sorting network and merge runs with
+                                        merge-path passes; 0: a bitonic network across
+                                        the warp */
 #define SSORT_PARAM_BLOCK_LEAN 12    /* 1: the CTA sort takes the LCPs of neighbours whose
                                         packed windows differ from the windows alone and
                                         reads full keys only for equal windows; 2: that, and

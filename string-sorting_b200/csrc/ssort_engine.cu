@@ -324,6 +324,44 @@ int ssort_ctx::run_ws(const uint8_t *arena_p, uint64_t arena_bytes, const void *
     return SSORT_OK;
 }
 
+// Copies `bytes` of ordinary (pageable) host memory to the device on st
+// through two pinned chunks: the host threads copy chunk k + 1 into one while
+// the DMA engine moves chunk k from the other, so the transfer runs at the
+// rate of the slower of the two instead of the driver's pageable staging.
+// Returns with the last transfer queued (not complete); the chunks are
+// reused by the next call only after their events.
+int ssort_ctx::copy_pageable(void *d_dst, const void *h_src, uint64_t bytes) {
+    constexpr uint64_t CHUNK = 64ull << 20;
+    if (bytes < 2 * CHUNK) {  // small: the driver's own path is as good
+        SS_CUDA(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, st));
+        return SSORT_OK;
+    }
+    for (int b = 0; b < 2; ++b) {
+        SS_TRY(ensure_host(h_stage[b], CHUNK));
+        if (!ev_stage[b]) SS_CUDA(cudaEventCreateWithFlags(&ev_stage[b], cudaEventDisableTiming));
+    }
+    const unsigned char *src = (const unsigned char *)h_src;
+    unsigned char *dst = (unsigned char *)d_dst;
+    uint64_t k = 0;
+    for (uint64_t at = 0; at < bytes; at += CHUNK, ++k) {
+        const int b = (int)(k & 1);
+        const uint64_t len = std::min(CHUNK, bytes - at);
+        // the chunk's previous transfer (two chunks back) has finished
+        SS_CUDA(cudaEventSynchronize(ev_stage[b]));
+        unsigned char *stage = (unsigned char *)h_stage[b].p;
+        const int64_t pieces = 64;
+        const uint64_t piece = (len + pieces - 1) / pieces;
+#pragma omp parallel for
+        for (int64_t q = 0; q < pieces; ++q) {
+            const uint64_t o = (uint64_t)q * piece;
+            if (o < len) std::memcpy(stage + o, src + at + o, std::min(piece, len - o));
+        }
+        SS_CUDA(cudaMemcpyAsync(dst + at, stage, len, cudaMemcpyHostToDevice, st));
+        SS_CUDA(cudaEventRecord(ev_stage[b], st));
+    }
+    return SSORT_OK;
+}
+
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -503,8 +541,11 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
         for (DBuf *b : {&ctx->ws_buf, &ctx->arena, &ctx->offs, &ctx->perm, &ctx->inst, &ctx->aux,
                      &ctx->aux2})
             if (b->p) cudaFree(b->p);
-        for (HBuf *b : {&ctx->h_offs, &ctx->h_arena, &ctx->h_perm})
+        for (HBuf *b : {&ctx->h_offs, &ctx->h_arena, &ctx->h_perm, &ctx->h_stage[0],
+                        &ctx->h_stage[1]})
             if (b->p) cudaFreeHost(b->p);
+        for (cudaEvent_t e : ctx->ev_stage)
+            if (e) cudaEventDestroy(e);
         if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
         if (ctx->h_hist) cudaFreeHost(ctx->h_hist);
         if (ctx->hist_buf.p) cudaFree(ctx->hist_buf.p);
@@ -704,14 +745,35 @@ int ssort_sort_strings(ssort_ctx *ctx, unsigned char **strings, size_t n, uint32
         uint8_t *d_arena = (uint8_t *)ctx->arena.p;
         uint32_t *d_perm = (uint32_t *)ctx->perm.p;
         uint32_t *d_lcp = lcp_out ? d_perm + n : nullptr;
-        SS_CUDA(cudaMemcpyAsync(d_arena, src, bytes, cudaMemcpyHostToDevice, ctx->st));
+        // The caller's span is ordinary memory: staged through pinned chunks.
+        if (use_span)
+            SS_TRY(ctx->copy_pageable(d_arena, src, bytes));
+        else
+            SS_CUDA(cudaMemcpyAsync(d_arena, src, bytes, cudaMemcpyHostToDevice, ctx->st));
         SS_CUDA(cudaMemsetAsync(d_arena + bytes, 0, 16, ctx->st));
         SS_CUDA(cudaMemcpyAsync(ctx->offs.p, ctx->h_offs.p, n * ow, cudaMemcpyHostToDevice,
                                 ctx->st));
         SS_TRY(sort_device_impl(ctx, d_arena, bytes + 16, ctx->offs.p, ow, n, d_perm, d_lcp));
-        SS_CUDA(cudaMemcpyAsync(perm, d_perm, n * 4, cudaMemcpyDeviceToHost, ctx->st));
         if (lcp_out)
             SS_CUDA(cudaMemcpyAsync(lcp_out, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+        if (use_span) {
+            // One span: the sorted strings' offsets into it come back in
+            // order, and the pointer array is rewritten sequentially (no
+            // random gather through a copy of the old array).
+            SS_TRY(ctx->ensure(ctx->aux2, n * 8));
+            SS_TRY(ctx->ensure_host(ctx->h_arena, n * 8));  // unused by the span path
+            LAUNCH(ctx, "sorted_offs",
+                   launch_sorted_offs(d_perm, ctx->offs.p, ow, n, (uint64_t *)ctx->aux2.p,
+                                      ctx->st));
+            uint64_t *so = (uint64_t *)ctx->h_arena.p;
+            SS_CUDA(cudaMemcpyAsync(so, ctx->aux2.p, n * 8, cudaMemcpyDeviceToHost, ctx->st));
+            SS_CUDA(cudaStreamSynchronize(ctx->st));
+            unsigned char *base = (unsigned char *)lo;
+#pragma omp parallel for if (nn > 100000)
+            for (int64_t i = 0; i < nn; ++i) strings[i] = base + so[i];
+            return SSORT_OK;
+        }
+        SS_CUDA(cudaMemcpyAsync(perm, d_perm, n * 4, cudaMemcpyDeviceToHost, ctx->st));
         SS_CUDA(cudaStreamSynchronize(ctx->st));
         std::vector<unsigned char *> orig(strings, strings + n);
 #pragma omp parallel for if (nn > 100000)

@@ -68,6 +68,11 @@ struct ssort_ctx {
     ulonglong2 *key2 = nullptr;  // set by run() for the sort it starts
     double round1_live = -1.0;   // share of strings entering round 1 in the last sort
     ssort::HBuf h_offs, h_arena, h_perm;
+    // Pinned staging ring for copying pageable host spans to the device
+    // (copy_pageable): two chunks, each reused once its transfer is done.
+    ssort::HBuf h_stage[2];
+    cudaEvent_t ev_stage[2] = {nullptr, nullptr};
+    int copy_pageable(void *d_dst, const void *h_src, uint64_t bytes);
     ssort::Counters *h_ctr = nullptr;
 
     ssort_stats stats{};
@@ -87,7 +92,7 @@ struct ssort_ctx {
     uint32_t digit_bits = 10;    // a partition pass makes at most 2^digit_bits buckets
     uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
     bool match_vote = false;       // count kernel ranks keys with ballots
-    bool warp_merge = false;       // warp sorts: local networks + merge passes
+    bool warp_merge = true;        // warp sorts: local networks + merge passes
     // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
     // key it was built for, three streams to capture nested conditional
     // bodies on, and a pinned copy of the loop state.

@@ -224,3 +224,22 @@ def test_saved_round1_keys_u32_offsets():
         p, l = s.sort_host(ss.arena, ss.offs.astype(np.uint32))
         assert s.stats().window_saved == ss.n
     assert np.array_equal(p, rp) and np.array_equal(l, rl)
+
+
+def test_pointer_array_one_large_span(sorter):
+    """The drop-in's fast path: every pointer inside one readable span of
+    more than 128 MB (copied through the pinned staging chunks), sorted
+    pointers rebuilt from the sorted offsets; the order is the oracle's."""
+    import ctypes
+    ss = pyssort.gen_urls(3_000_000, seed=71)
+    assert ss.text_bytes > (128 << 20)
+    base = ss.arena.ctypes.data
+    ptrs = (ctypes.c_void_p * ss.n)(*[base + int(o) for o in ss.offs])
+    lcp = np.empty(ss.n, dtype=np.uint32)
+    rc = pyssort.lib().ssort_sort_strings(sorter._ctx, ptrs, ss.n, lcp.ctypes.data)
+    assert rc == 0, pyssort.lib().ssort_last_error()
+    got = np.array([p - base for p in ptrs], dtype=np.uint64)
+    perm = np.searchsorted(ss.offs, got).astype(np.uint32)  # offsets ascend with the index
+    ref_perm, ref_lcp = pyoracle.oracle_sort(ss.arena, ss.offs)
+    assert np.array_equal(perm, ref_perm)
+    assert np.array_equal(lcp, ref_lcp)
