@@ -46,7 +46,8 @@ PARAMS = {"target_bucket": pyssort.SSORT_PARAM_TARGET_BUCKET,
           "scatter": pyssort.SSORT_PARAM_SCATTER,
           "block_lean": pyssort.SSORT_PARAM_BLOCK_LEAN,
           "match_vote": pyssort.SSORT_PARAM_MATCH_VOTE,
-          "warp_merge": pyssort.SSORT_PARAM_WARP_MERGE}
+          "warp_merge": pyssort.SSORT_PARAM_WARP_MERGE,
+          "scan": pyssort.SSORT_PARAM_SCAN}
 
 
 def apply_params(sorter, args):
@@ -1113,7 +1114,7 @@ def time_dropin(ss, n, steps):
     return {"value": n / t, "unit": UNIT, "ms_per_step": round(1000 * t, 3), "steps": steps,
             "api": "msd_gpu(unsigned char **, size_t) through the reference registry's r->f",
             "h2d_bytes_per_step": int(ss.text_bytes + n * (4 if ss.text_bytes < 2**32 else 8)),
-            "d2h_bytes_per_step": int(n * 4)}
+            "d2h_bytes_per_step": int(n * 8)}  # sorted 8-byte offsets into the span
 
 
 def time_cpu_sort(ss, m):

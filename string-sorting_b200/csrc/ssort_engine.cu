@@ -67,7 +67,20 @@ int ssort_ctx::sample_entropy(const uint8_t *arena_p, uint64_t arena_bytes, cons
 }
 
 int ssort_ctx::scan(const uint32_t *in, uint32_t *out, uint32_t cap, Count n) {
-    LAUNCH(this, "scan", launch_scan(in, out, cap, n, ws.partials, st));
+    return scan_on(in, out, cap, n, st);
+}
+
+// The count-matrix scan on stream s: single-pass with decoupled look-back
+// (SSORT_PARAM_SCAN = 1; its state is cleared first), or reduce-then-scan.
+int ssort_ctx::scan_on(const uint32_t *in, uint32_t *out, uint32_t cap, Count n,
+                       cudaStream_t s) {
+    if (scan_lookback) {
+        SS_CUDA(cudaMemsetAsync(ws.lookback, 0, lookback_state_bytes(cap), s));
+        LAUNCH(this, "scan",
+               launch_scan_lookback(in, out, cap, n, ws.lookback, &ws.ctr->error, s));
+    } else {
+        LAUNCH(this, "scan", launch_scan(in, out, cap, n, ws.partials, s));
+    }
     return SSORT_OK;
 }
 
@@ -811,6 +824,10 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
         case SSORT_PARAM_DIGIT_BITS:
             if (value < 8 || value > 10) return fail(SSORT_EINVAL, "digit_bits out of range (8..10)");
             ctx->digit_bits = (uint32_t)value;
+            return SSORT_OK;
+        case SSORT_PARAM_SCAN:
+            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "scan must be 0 or 1");
+            ctx->scan_lookback = value != 0;
             return SSORT_OK;
         case SSORT_PARAM_WARP_MERGE:
             if (value != 0 && value != 1) return fail(SSORT_EINVAL, "warp_merge must be 0 or 1");

@@ -175,9 +175,8 @@ int ssort_ctx::graph_build(const SortArgs &a) {
                                     ws.cm_base, ws.cm, dc, gather, g2, s2));
                 SS_CUDA(cudaStreamEndCapture(s2, &out));
             }
-            LAUNCH(this, "scan",
-                   launch_scan(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
-                               dcount(ws.cm_base, &g->n_large), ws.partials, s1));
+            SS_TRY(scan_on(ws.cm, ws.cm, (uint32_t)(ws.cm_cap - 1),
+                           dcount(ws.cm_base, &g->n_large), s1));
             LAUNCH(this, "scatter",
                    launch_scatter(a, ws.L, nl, ws.tile_base, ws.spl, ws.nspl, ws.tbl, ws.cm_base,
                                   ws.cm, g2, s1));
@@ -255,6 +254,8 @@ int ssort_ctx::run_graph(const SortArgs &a, uint32_t n, const uint32_t *d_inst, 
         SS_CUDA(cudaGraphLaunch(gexec, st));
         SS_CUDA(cudaMemcpyAsync(h_gs, g, sizeof(GraphState), cudaMemcpyDeviceToHost, st));
         SS_CUDA(cudaStreamSynchronize(st));
+        if (h_gs->error == 2)
+            return fail(SSORT_EINTERNAL, "a scan's look-back waited past its bound");
         if (h_gs->error)
             return fail(SSORT_EINTERNAL, "partition levels exceeded " +
                                              std::to_string(graph_max_levels) + " in a round");

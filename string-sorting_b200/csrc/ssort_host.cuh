@@ -93,6 +93,7 @@ struct ssort_ctx {
     uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
     bool match_vote = false;       // count kernel ranks keys with ballots
     bool warp_merge = true;        // warp sorts: local networks + merge passes
+    bool scan_lookback = false;    // count-matrix scan in one pass (decoupled look-back)
     // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
     // key it was built for, three streams to capture nested conditional
     // bodies on, and a pinned copy of the loop state.
@@ -205,6 +206,8 @@ struct ssort_ctx {
     int sync_counters() {
         SS_CUDA(cudaMemcpyAsync(h_ctr, ws.ctr, sizeof(ssort::Counters), cudaMemcpyDeviceToHost, st));
         SS_CUDA(cudaStreamSynchronize(st));
+        if (h_ctr->error)
+            return ssort::fail(SSORT_EINTERNAL, "a scan's look-back waited past its bound");
         return SSORT_OK;
     }
 
@@ -212,6 +215,7 @@ struct ssort_ctx {
 
     int reserve(uint32_t n);
     int scan(const uint32_t *in, uint32_t *out, uint32_t cap, ssort::Count n);
+    int scan_on(const uint32_t *in, uint32_t *out, uint32_t cap, ssort::Count n, cudaStream_t s);
     int run(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
             uint32_t n, uint32_t *d_perm, uint32_t *d_lcp, const uint32_t *d_inst = nullptr,
             uint32_t ninst = 0);

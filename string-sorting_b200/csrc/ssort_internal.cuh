@@ -192,7 +192,7 @@ constexpr uint32_t scan_partials_for(uint64_t n) {
 
 struct WsLayout {
     size_t idx1, key0, key1, lcp, bkt, R, N, W1, W8, S, S2, S3, E, B, L, L2, spl, nspl, tbl, ntiles,
-        cm_size, cm_base, tile_base, tmp, cm, partials, ctr, gs;
+        cm_size, cm_base, tile_base, tmp, cm, partials, ctr, gs, lookback;
     size_t cm_cap, total;
 };
 
@@ -236,6 +236,8 @@ constexpr WsLayout ws_layout(uint64_t n) {
     o.cm_cap = (size_t)NB_MAX * (n / PART_TILE + nlarge + 1) + 1;
     o.cm = take(o.cm_cap * 4);
     o.partials = take((size_t)scan_partials_for(o.cm_cap) * 4);
+    // single-pass scan: a ticket word, then one status word per tile
+    o.lookback = take(8 + (size_t)scan_partials_for(o.cm_cap) * 8);
     o.ctr = take(sizeof(Counters));
     o.gs = take(sizeof(GraphState));
     o.total = off;
@@ -244,6 +246,7 @@ constexpr WsLayout ws_layout(uint64_t n) {
 
 struct Workspace {
     uint32_t *idx1, *lcp, *nspl, *ntiles, *cm_size, *cm_base, *tile_base, *tmp, *cm, *partials;
+    unsigned char *lookback;  // ticket + tile status words of the single-pass scan
     ulonglong2 *key0, *key1, *spl;
     Seg *R, *N, *W1, *W8, *S, *S2, *S3, *E, *L, *L2;
     uint2 *B;
@@ -282,6 +285,7 @@ inline Workspace ws_bind(const WsLayout &o, unsigned char *base) {
     w.tmp = (uint32_t *)(base + o.tmp);
     w.cm = (uint32_t *)(base + o.cm);
     w.partials = (uint32_t *)(base + o.partials);
+    w.lookback = base + o.lookback;
     w.ctr = (Counters *)(base + o.ctr);
     w.gs = (GraphState *)(base + o.gs);
     w.cm_cap = o.cm_cap;
@@ -333,6 +337,13 @@ void launch_seg_tiles(const Seg *segs, Count n, uint32_t tile, uint32_t *out, cu
 void launch_scan(const uint32_t *in, uint32_t *out, uint32_t cap, Count n, uint32_t *partials,
                  cudaStream_t st);
 uint32_t scan_partials_needed(uint32_t n);
+// The same scan in one pass with decoupled look-back: tiles take their order
+// from a ticket and add up their predecessors' published sums; `state` holds
+// a ticket word and one status word per tile and must be zeroed first
+// (lookback_state_bytes(cap)); a look-back that waits too long sets *err.
+size_t lookback_state_bytes(uint32_t cap);
+void launch_scan_lookback(const uint32_t *in, uint32_t *out, uint32_t cap, Count n,
+                          unsigned char *state, uint32_t *err, cudaStream_t st);
 void launch_gather(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,
                    Counters *c, int grid, cudaStream_t st);
 // from_arena / gather: first partition level of a round, whose keys the

@@ -3134,12 +3134,111 @@ __global__ void k_g_round_end(GraphState *g, const Counters *c, Seg *R, const Se
     g->full_sorted += c->full_sorted;
     g->window_saved += c->window_saved;
     g->window_used += c->window_used;
+    if (c->error) g->error = 2;  // a scan's look-back waited past its bound
     g->n_cur = n;
     g->round += 1;
     g->round_in_launch += 1;
     g->done = n == 0 ? 1u : 0u;
     const bool more = n > 0 && !g->error && g->round_in_launch < GRAPH_ROUNDS_PER_LAUNCH;
     cudaGraphSetConditional(h_round, more ? 1u : 0u);
+}
+
+// ---- exclusive scan (u32), one pass with decoupled look-back ---------------
+// Each CTA takes the next tile from a ticket (so every tile it waits for has
+// started), scans its 4096 values, publishes its sum, and warp 0 walks back
+// over its predecessors' status words 32 at a time, adding sums until it
+// meets an inclusive prefix; then it publishes its own inclusive prefix.
+// Status word: flag (1 = tile sum, 2 = inclusive prefix) << 32 | value.  The
+// wait for a predecessor is bounded; past the bound the CTA records an
+// error and goes on (the host reports it; the result is then not used).
+constexpr uint64_t LB_SUM = 1ull << 32, LB_INCL = 2ull << 32;
+constexpr uint32_t LB_SPIN_MAX = 1u << 22;
+
+__device__ __forceinline__ uint32_t warp_sum32(uint32_t v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    return v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_lookback(const uint32_t *in, uint32_t *out,
+                                                                Count cnt,
+                                                                unsigned long long *status,
+                                                                uint32_t *ticket, uint32_t *err) {
+    __shared__ uint32_t buf[SCAN_CHUNK];
+    __shared__ uint32_t s_tile, s_prefix;
+    const uint32_t n = count_of(cnt);
+    const uint32_t lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const uint64_t base = (uint64_t)t * SCAN_CHUNK;
+    if (base >= n) {
+        if (n == 0 && t == 0 && threadIdx.x == 0) out[0] = 0;
+        return;
+    }
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int j = k * SCAN_THREADS + threadIdx.x;
+        const uint64_t i = base + j;
+        buf[j] = i < n ? in[i] : 0;
+    }
+    __syncthreads();
+    uint32_t s = 0;
+    for (int k = 0; k < SCAN_ITEMS; ++k) s += buf[threadIdx.x * SCAN_ITEMS + k];
+    uint32_t excl;
+    const uint32_t total = block_exclusive_scan(s, excl);
+    if (threadIdx.x < 32) {
+        uint32_t prefix = 0;
+        if (t == 0) {
+            if (lane == 0) atomicExch(&status[0], LB_INCL | total);
+        } else {
+            if (lane == 0) atomicExch(&status[t], LB_SUM | total);
+            int64_t j = (int64_t)t - 1;  // nearest predecessor not yet added
+            uint32_t spins = 0;
+            bool failed = false;
+            while (true) {
+                const int64_t idx = j - (int64_t)lane;
+                const volatile unsigned long long *sp = status + (idx >= 0 ? idx : 0);
+                unsigned long long w = idx >= 0 ? *sp : LB_INCL;
+                while (__any_sync(0xffffffffu, (w >> 32) == 0)) {
+                    if (++spins > LB_SPIN_MAX) {
+                        failed = true;
+                        break;
+                    }
+                    __nanosleep(32);
+                    if ((w >> 32) == 0) w = *sp;
+                }
+                if (failed) break;
+                const uint32_t incl = __ballot_sync(0xffffffffu, (w >> 32) == 2);
+                if (incl) {
+                    const uint32_t k = __ffs(incl) - 1;  // the nearest inclusive prefix
+                    prefix += warp_sum32(lane <= k ? (uint32_t)w : 0u);
+                    break;
+                }
+                prefix += warp_sum32((uint32_t)w);
+                j -= 32;
+            }
+            if (lane == 0) {
+                if (failed) atomicExch(err, 1u);
+                atomicExch(&status[t], LB_INCL | (prefix + total));
+            }
+        }
+        if (lane == 0) s_prefix = prefix;
+    }
+    __syncthreads();
+    uint32_t run = s_prefix + excl;
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int j = threadIdx.x * SCAN_ITEMS + k;
+        const uint32_t v = buf[j];
+        buf[j] = run;
+        run += v;
+    }
+    __syncthreads();
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int j = k * SCAN_THREADS + threadIdx.x;
+        const uint64_t i = base + j;
+        if (i < n) out[i] = buf[j];
+    }
+    if (threadIdx.x == 0 && base + SCAN_CHUNK >= n) out[n] = s_prefix + total;
 }
 
 }  // namespace
@@ -3292,6 +3391,16 @@ void launch_seg_tiles(const Seg *segs, Count n, uint32_t tile, uint32_t *out, cu
 }
 
 uint32_t scan_partials_needed(uint32_t n) { return cdiv(n ? n : 1, SCAN_CHUNK) + 1; }
+
+size_t lookback_state_bytes(uint32_t cap) { return 8 + (size_t)cdiv(cap ? cap : 1, SCAN_CHUNK) * 8; }
+
+void launch_scan_lookback(const uint32_t *in, uint32_t *out, uint32_t cap, Count n,
+                          unsigned char *state, uint32_t *err, cudaStream_t st) {
+    const uint32_t nb = cdiv(cap ? cap : 1, SCAN_CHUNK);
+    k_scan_lookback<<<nb, SCAN_THREADS, 0, st>>>(in, out, n,
+                                                  reinterpret_cast<unsigned long long *>(state + 8),
+                                                  reinterpret_cast<uint32_t *>(state), err);
+}
 
 void launch_scan(const uint32_t *in, uint32_t *out, uint32_t cap, Count n, uint32_t *partials,
                  cudaStream_t st) {

@@ -46,6 +46,7 @@ SSORT_PARAM_SCATTER = 11
 SSORT_PARAM_BLOCK_LEAN = 12
 SSORT_PARAM_MATCH_VOTE = 13
 SSORT_PARAM_WARP_MERGE = 14
+SSORT_PARAM_SCAN = 15
 
 
 class SsortError(RuntimeError):

@@ -140,3 +140,15 @@ def test_auto_mode_uses_the_graph_from_the_second_identical_sort():
             assert np.array_equal(d_perm.cpu().numpy().view(np.uint32), rp)
             assert np.array_equal(d_lcp.cpu().numpy().view(np.uint32), rl)
     assert used[0] == 0 and used[1] >= 1 and used[2] >= 1
+
+
+def test_graph_with_single_pass_scan():
+    """The device-driven loop with the decoupled look-back scan inside its
+    level loop (its state cleared by a memset node each level)."""
+    ss = pyssort.gen_zipf_words(2_000_000, vocab=20_000, seed=25)
+    rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+    with graph_sorter() as s:
+        s.set_param(pyssort.SSORT_PARAM_SCAN, 1)
+        for _ in range(2):
+            p, l = s.sort_host(ss.arena, ss.offs)
+            assert np.array_equal(p, rp) and np.array_equal(l, rl)

@@ -34,7 +34,8 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_BLOCK_LEAN, 2),
     (pyssort.SSORT_PARAM_GRAPH, 2),
     (pyssort.SSORT_PARAM_MATCH_VOTE, 1),
-    (pyssort.SSORT_PARAM_WARP_MERGE, 1),
+    (pyssort.SSORT_PARAM_WARP_MERGE, 0),
+    (pyssort.SSORT_PARAM_SCAN, 1),
 ]
 
 
@@ -94,6 +95,7 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_BLOCK_LEAN, 3),
                              (pyssort.SSORT_PARAM_MATCH_VOTE, 2),
                              (pyssort.SSORT_PARAM_WARP_MERGE, 2),
+                             (pyssort.SSORT_PARAM_SCAN, 2),
                              (pyssort.SSORT_PARAM_GRAPH_MAX_LEVELS, 0),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 7),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 11),
