@@ -254,10 +254,10 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
 #define SSORT_PARAM_MATCH_VOTE 13    /* 1: the partition's count kernel finds the lanes of a
                                         warp that share a bucket with one ballot per
                                         bucket-id bit; 0 (default): with __match_any_sync */
-#define SSORT_PARAM_SCAN 15          /* 1: the partition's count-matrix scan runs in one
-                                        pass with decoupled look-back (tiles in ticket order
-                                        add up their predecessors' published sums); 0
-                                        (default): reduce, scan of the partials, down-sweep */
+#define SSORT_PARAM_SCAN 15          /* 1 (default): the partition's count-matrix scan runs
+                                        in one pass with decoupled look-back (tiles in
+                                        ticket order add up their predecessors' published
+                                        sums); 0: reduce, scan of the partials, down-sweep */
 #define SSORT_PARAM_WARP_MERGE 14    /* 1 (default): the warp-level sorts of packed keys
                                         (one-warp and CTA sorts) sort each lane's values
                                         with a sorting network and merge runs with

@@ -93,7 +93,7 @@ struct ssort_ctx {
     uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
     bool match_vote = false;       // count kernel ranks keys with ballots
     bool warp_merge = true;        // warp sorts: local networks + merge passes
-    bool scan_lookback = false;    // count-matrix scan in one pass (decoupled look-back)
+    bool scan_lookback = true;     // count-matrix scan in one pass (decoupled look-back)
     // Device-driven round loop (ssort_graph.cu): the instantiated graph, the
     // key it was built for, three streams to capture nested conditional
     // bodies on, and a pinned copy of the loop state.

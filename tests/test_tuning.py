@@ -35,7 +35,7 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_GRAPH, 2),
     (pyssort.SSORT_PARAM_MATCH_VOTE, 1),
     (pyssort.SSORT_PARAM_WARP_MERGE, 0),
-    (pyssort.SSORT_PARAM_SCAN, 1),
+    (pyssort.SSORT_PARAM_SCAN, 0),
 ]
 
 
