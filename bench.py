@@ -258,12 +258,15 @@ def kernel_bytes(st, w):
         return fresh * (4 + w + KB) + keyed * (KB + 4) + (fresh + keyed) * 8
     # Round 0's gather may also keep key bytes 16..31 per string (read 16 more,
     # write 16); round 1's first level then reads those (idx 4 + 16) instead of
-    # the offset and the arena, in whichever kernel gathers that level.
+    # the offset and the arena, in whichever kernel gathers that level.  Round
+    # 0 gathers in a separate pass whenever any round does (a small round 0
+    # gathers inside its count, and so does every round under mode 2).
     saved = getattr(st, "window_saved", 0)
     used = getattr(st, "window_used", 0)
     used_by = "count_gather" if st.gather_fused else "gather"
+    saved_by = "gather" if st.gather_elems > st.gather_fused else "count_gather"
     out = {
-        "gather": (st.gather_elems - st.gather_fused) * (4 + w + KB + KB) + saved * 2 * KB,
+        "gather": (st.gather_elems - st.gather_fused) * (4 + w + KB + KB),
         "count_gather": st.gather_fused * (4 + w + KB + KB),
         "count": (st.partitioned - st.gather_fused) * KB,
         "scatter": st.partitioned * 2 * (KB + 4),
@@ -272,6 +275,7 @@ def kernel_bytes(st, w):
         "block": sort_bytes(st.block_fresh, st.block_keyed),
         "equal": st.equal_moved * 8 + st.equal_final * 4,
     }
+    out[saved_by] += saved * 2 * KB
     out[used_by] -= used * w
     return out
 

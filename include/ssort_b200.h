@@ -240,8 +240,11 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                        (default 256); larger ones go to the CTA sort */
 #define SSORT_PARAM_OVERLAP 3       /* 1 (default): in round 0 the on-chip sorts run
                                        on a side stream beside the partition; 0: one stream */
-#define SSORT_PARAM_FUSED_GATHER 4  /* 1 (default): from round 1 on, the first partition
-                                       level gathers the keys it counts; 0: separate gather */
+#define SSORT_PARAM_FUSED_GATHER 4  /* 1 (default): the first partition level of a
+                                       round gathers the keys it counts, except in a round 0
+                                       of more than 4 M keys, which streams them in a
+                                       separate pass first; 2: every round; 0: separate
+                                       gather in every round */
 #define SSORT_PARAM_WARP1_DEEP 5    /* 0..4096 (default 64): 16-byte steps the warp that
                                        sorts a segment of <= 32 strings takes on its own
                                        runs of equal keys before handing what is left to

@@ -174,11 +174,12 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     SS_TRY(fork_small());
     uint32_t n_large = h_ctr->n_large;
     Seg *lcur = ws.L, *lnext = ws.L2;
-    // Keys of the large segments at this depth.  In round 0 the indices are
-    // the identity, so a separate gather streams the arena in order; later
-    // rounds read it at random, and the count kernel of the first partition
-    // level gathers the keys itself so that those reads overlap its work.
-    const bool fused_gather = !fresh_round && this->fused_gather;
+    // Keys of the large segments at this depth.  In a large round 0 the
+    // indices are the identity, so a separate gather streams the arena in
+    // order; later rounds read it at random, and the count kernel of the first
+    // partition level gathers the keys itself so that those reads overlap its
+    // work (gather_fused).
+    const bool fused_gather = gather_fused(this->fused_gather, fresh_round, h_ctr->gather_elems);
     if (n_large && !fused_gather) {
         LAUNCH(this, "seg_tiles",
                launch_seg_tiles(lcur, hcount(n_large), GATHER_TILE, ws.tile_base, st));
@@ -818,8 +819,8 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
             ctx->overlap = value != 0;
             return SSORT_OK;
         case SSORT_PARAM_FUSED_GATHER:
-            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "fused_gather must be 0 or 1");
-            ctx->fused_gather = value != 0;
+            if (value < 0 || value > 2) return fail(SSORT_EINVAL, "fused_gather must be 0, 1 or 2");
+            ctx->fused_gather = (uint32_t)value;
             return SSORT_OK;
         case SSORT_PARAM_DIGIT_BITS:
             if (value < 8 || value > 10) return fail(SSORT_EINVAL, "digit_bits out of range (8..10)");
@@ -1114,7 +1115,7 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
                     case SSORT_PARAM_TARGET_BUCKET: return ctx->target_bucket;
                     case SSORT_PARAM_DIGIT_BITS: return ctx->digit_bits;
                     case SSORT_PARAM_WARP8_CAP: return ctx->warp8_cap;
-                    case SSORT_PARAM_FUSED_GATHER: return ctx->fused_gather ? 1 : 0;
+                    case SSORT_PARAM_FUSED_GATHER: return ctx->fused_gather;
                     case SSORT_PARAM_BLOCK_PREFETCH: return ctx->block_prefetch ? 1 : 0;
                     case SSORT_PARAM_L2_PREFETCH: return ctx->l2_prefetch ? 1 : 0;
                     case SSORT_PARAM_BLOCK_LEAN: return ctx->block_lean;
@@ -1139,8 +1140,8 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
             }
             const uint32_t sc = size_class(n), ec = entropy_class(bits);
             ctx->tuned[sc * 4 + ec] = ssort_ctx::Tuned{
-                ctx->target_bucket, ctx->warp8_cap,    ctx->digit_bits,     ctx->graph_mode,
-                ctx->block_lean,    ctx->overlap,      ctx->fused_gather,   ctx->block_prefetch,
+                ctx->target_bucket, ctx->warp8_cap, ctx->digit_bits,     ctx->graph_mode,
+                ctx->block_lean,    ctx->fused_gather, ctx->overlap,    ctx->block_prefetch,
                 ctx->l2_prefetch};
             out->size_class = sc;
             out->entropy_class = ec;
@@ -1148,7 +1149,7 @@ int ssort_autotune(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_bytes,
             out->target_bucket = ctx->target_bucket;
             out->warp8_cap = ctx->warp8_cap;
             out->overlap = ctx->overlap ? 1 : 0;
-            out->fused_gather = ctx->fused_gather ? 1 : 0;
+            out->fused_gather = ctx->fused_gather;
             out->digit_bits = ctx->digit_bits;
             out->block_prefetch = ctx->block_prefetch ? 1 : 0;
             out->l2_prefetch = ctx->l2_prefetch ? 1 : 0;

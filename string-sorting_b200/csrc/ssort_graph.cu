@@ -231,7 +231,7 @@ int ssort_ctx::run_graph(const SortArgs &a, uint32_t n, const uint32_t *d_inst, 
     LAUNCH(this, "iota", launch_iota(a.idx[0], n, st));
     SS_CUDA(cudaMemsetAsync(a.lcp, 0, 4, st));
     std::memset(h_gs, 0, sizeof(GraphState));
-    h_gs->fused = fused_gather ? 1u : 0u;
+    h_gs->fused = fused_gather;
     h_gs->max_levels = graph_max_levels;
     if (d_inst) {
         SS_CUDA(cudaMemcpyAsync(g, h_gs, sizeof(GraphState), cudaMemcpyHostToDevice, st));

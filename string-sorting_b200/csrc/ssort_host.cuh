@@ -84,7 +84,7 @@ struct ssort_ctx {
     uint32_t warp8_cap = ssort::WARP8_CAP;          // largest one-warp segment
     uint32_t warp1_deep = ssort::WARP1_DEEP;        // in-warp refinement steps
     bool overlap = true;       // round-0 on-chip sorts on the side stream
-    bool fused_gather = true;  // rounds >= 1 gather inside the first count
+    uint32_t fused_gather = 1;  // 1: rounds >= 1 gather inside the first count; 2: all rounds
     bool block_prefetch = false;  // double-buffered CTA sort (k_block2)
     uint32_t block_lean = 0;      // CTA sort: 1 finish from the packed windows, 2 also a
                                   // first sort on 32-bit packed keys
@@ -113,8 +113,8 @@ struct ssort_ctx {
     // Autotuned values per (size class * 4 + entropy class), applied to later
     // sorts of the same classes; not while the tuner itself runs.
     struct Tuned {
-        uint32_t target_bucket, warp8_cap, digit_bits, graph, block_lean;
-        bool overlap, fused_gather, block_prefetch, l2_prefetch;
+        uint32_t target_bucket, warp8_cap, digit_bits, graph, block_lean, fused_gather;
+        bool overlap, block_prefetch, l2_prefetch;
     };
     std::map<uint32_t, Tuned> tuned;
     // target buckets per segment size class for the next batched sort

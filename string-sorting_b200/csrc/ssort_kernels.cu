@@ -184,15 +184,25 @@ __device__ __forceinline__ uint32_t match_bits(uint32_t v, uint32_t bits) {
 // each lane with `want` gets its own slot, at the cost of one atomic per warp
 // (appends from millions of small segments would otherwise serialise on one
 // address).
-__device__ __forceinline__ uint32_t warp_append(uint32_t *ctr, bool want) {
+// In two steps: warp_reserve issues the warp's atomic without waiting for
+// it, so that the reservations a kernel makes on several counters overlap
+// their round trips; warp_slot then hands each wanting lane its slot.
+struct WarpRes {
+    uint32_t mask, base;
+};
+__device__ __forceinline__ WarpRes warp_reserve(uint32_t *ctr, bool want) {
     const uint32_t mask = __ballot_sync(0xffffffffu, want);
-    if (!mask) return 0;
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t leader = __ffs(mask) - 1;
     uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    return base + __popc(mask & lanemask_lt());
+    if (mask && (threadIdx.x & 31) == (uint32_t)(__ffs(mask) - 1))
+        base = atomicAdd(ctr, (uint32_t)__popc(mask));
+    return WarpRes{mask, base};
+}
+__device__ __forceinline__ uint32_t warp_slot(const WarpRes &r) {
+    if (!r.mask) return 0;  // warp-uniform
+    return __shfl_sync(0xffffffffu, r.base, __ffs(r.mask) - 1) + __popc(r.mask & lanemask_lt());
+}
+__device__ __forceinline__ uint32_t warp_append(uint32_t *ctr, bool want) {
+    return warp_slot(warp_reserve(ctr, want));
 }
 
 // Append a next-round segment; warp-collective like warp_append.
@@ -819,17 +829,31 @@ __global__ void k_iota(uint32_t *idx, uint32_t n) {
 }
 
 // Appends o (when sm) to the CTA-sort list of its size class; warp-collective.
-__device__ __forceinline__ void append_small(const SmallLists &S, Counters *c, bool sm,
-                                             const Seg &o) {
+// Appends segment o (when v) to the list its length selects: one-warp sorts
+// of <= 32 or <= warp8_cap strings, the CTA sorts' three size classes, or the
+// large list L (counter nl).  Warp-collective; the six reservations are all
+// issued before any is waited for.
+__device__ __forceinline__ void append_by_length(const Seg &o, bool v, uint32_t warp8_cap,
+                                                 Seg *W1, Seg *W8, const SmallLists &S, Seg *L,
+                                                 uint32_t *nl, Counters *c) {
+    const bool w1 = v && o.len <= (uint32_t)WARP1_CAP;
+    const bool w8 = v && !w1 && o.len <= warp8_cap;
+    const bool sm = v && !w1 && !w8 && o.len <= (uint32_t)SMALL_CAP;
     const bool c0 = sm && o.len <= (uint32_t)BLOCK_CAP1;
     const bool c1 = sm && !c0 && o.len <= (uint32_t)BLOCK_CAP2;
     const bool c2 = sm && !c0 && !c1;
-    uint32_t slot = warp_append(&c->n_small, c0);
-    if (c0) S.s[0][slot] = o;
-    slot = warp_append(&c->n_small2, c1);
-    if (c1) S.s[1][slot] = o;
-    slot = warp_append(&c->n_small3, c2);
-    if (c2) S.s[2][slot] = o;
+    const bool lg = v && !w1 && !w8 && !sm;
+    const WarpRes r1 = warp_reserve(&c->n_w1, w1), r8 = warp_reserve(&c->n_w8, w8),
+                  rs0 = warp_reserve(&c->n_small, c0), rs1 = warp_reserve(&c->n_small2, c1),
+                  rs2 = warp_reserve(&c->n_small3, c2), rl = warp_reserve(nl, lg);
+    const uint32_t t1 = warp_slot(r1), t8 = warp_slot(r8), ts0 = warp_slot(rs0),
+                   ts1 = warp_slot(rs1), ts2 = warp_slot(rs2), tl = warp_slot(rl);
+    if (w1) W1[t1] = o;
+    if (w8) W8[t8] = o;
+    if (c0) S.s[0][ts0] = o;
+    if (c1) S.s[1][ts1] = o;
+    if (c2) S.s[2][ts2] = o;
+    if (lg) L[tl] = o;
 }
 
 __global__ void k_classify(const Seg *__restrict__ R, Count cnt, uint32_t warp8_cap, Seg *W1,
@@ -840,17 +864,8 @@ __global__ void k_classify(const Seg *__restrict__ R, Count cnt, uint32_t warp8_
     const uint32_t i = b0 + threadIdx.x;
     const bool v = i < nR;
     const Seg s = v ? R[i] : Seg{0, 0, 0, 0};
-    const bool w1 = v && s.len <= (uint32_t)WARP1_CAP;
-    const bool w8 = v && !w1 && s.len <= warp8_cap;
-    const bool sm = v && !w1 && !w8 && s.len <= (uint32_t)SMALL_CAP;
-    const bool lg = v && !w1 && !w8 && !sm;
-    uint32_t slot = warp_append(&c->n_w1, w1);
-    if (w1) W1[slot] = s;
-    slot = warp_append(&c->n_w8, w8);
-    if (w8) W8[slot] = s;
-    append_small(S, c, sm, s);
-    slot = warp_append(&c->n_large, lg);
-    if (lg) L[slot] = s;
+    append_by_length(s, v, warp8_cap, W1, W8, S, L, &c->n_large, c);
+    const bool lg = v && s.len > (uint32_t)SMALL_CAP && s.len > warp8_cap;
     const unsigned long long live = warp_sum(v ? s.len : 0);
     const unsigned long long big = warp_sum(lg ? s.len : 0);
     if ((threadIdx.x & 31) == 0) {
@@ -1350,7 +1365,7 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
                                                bool from_arena);
 
 // One CTA per large segment at a time (segments si = blockIdx.x, + gridDim.x, ...).
-__global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SortArgs a, const Seg *__restrict__ L,
+__global__ void __launch_bounds__(SAMPLE_THREADS, 2) k_sample(SortArgs a, const Seg *__restrict__ L,
                                                            Count cnt, ulonglong2 *spl,
                                                            uint32_t *nspl, uint16_t *tbl,
                                                            uint32_t *ntiles, uint32_t *cm_size,
@@ -1366,13 +1381,13 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
                                                uint32_t si, ulonglong2 *spl, uint32_t *nspl,
                                                uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size,
                                                bool from_arena) {
-    // smp: SAMPLES_MAX keys; sv: their packed sort keys (padded layout)
+    // sv: the samples' packed sort keys (padded layout).  The sampled keys
+    // themselves stay in registers; the chosen candidates are read again.
     extern __shared__ __align__(16) unsigned char sample_smem[];
-    ulonglong2 *smp = reinterpret_cast<ulonglong2 *>(sample_smem);
-    uint64_t *sv = reinterpret_cast<uint64_t *>(smp + SAMPLES_MAX);
+    uint64_t *sv = reinterpret_cast<uint64_t *>(sample_smem);
     __shared__ ulonglong2 cands[SAMPLE_THREADS];
     __shared__ uint32_t warp_cnt[SAMPLE_THREADS / 32 + 1];
-    __shared__ uint64_t red[2][SAMPLE_THREADS / 32];
+    __shared__ uint64_t red[4][SAMPLE_THREADS / 32];
     const Seg s = L[si];
     const ulonglong2 *K = a.keyb(s.flags & SEG_BUF1) + s.start;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1384,65 +1399,81 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     uint32_t S = next_pow2(8 * (k + 1));
     if (S < 256) S = 256;
     if (S > (uint32_t)SAMPLES_MAX) S = SAMPLES_MAX;
-    // On the first partition level of a round the segment's keys are not in
-    // the key buffer yet (the count kernel gathers them): read the sampled
-    // strings straight from the arena.
-    for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
+    // Sample i is the string at position pos_of(i) of the segment.  On the
+    // first partition level of a round the segment's keys are not in the key
+    // buffer yet (the count kernel gathers them): read them from the arena.
+    auto pos_of = [&](uint32_t i) -> uint32_t {
         const uint32_t r = hash32(s.start * 0x9E3779B1u + i * 0x85EBCA77u + s.len);
-        const uint32_t e = (uint32_t)(((uint64_t)r * s.len) >> 32);
-        smp[i] = from_arena
-                     ? from_key(load_key(a.arena, a.arena_bytes,
-                                         string_offset(a.offs, a.off_width,
-                                                       a.idx[0][s.start + e]) + s.depth))
-                     : K[e];
-    }
-    __syncthreads();
-    // Order the samples by packed keys (window after the samples' common
-    // prefix, 12-bit sample index): warp runs of 256, then merges.  The order
-    // only picks quantiles; the chosen candidates are sorted by full key below.
-    {
-        const Key k0 = to_key(smp[0]);
-        uint64_t dh = 0, dl = 0;
-        for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS) {
-            const Key x = to_key(smp[i]);
-            dh |= x.hi ^ k0.hi;
-            dl |= x.lo ^ k0.lo;
-        }
+        return (uint32_t)(((uint64_t)r * s.len) >> 32);
+    };
+    auto key_at = [&](uint32_t e) -> Key {
+        return from_arena ? load_key(a.arena, a.arena_bytes,
+                                     string_offset(a.offs, a.off_width, a.idx[0][s.start + e]) +
+                                         s.depth)
+                          : to_key(K[e]);
+    };
+    // Warp w < S / 256 holds samples w * 256 + lane * 8 + i (i < 8).
+    const bool active = w * 256 < S;
+    Key kk[8];
+    uint64_t oh = 0, ol = 0, ah = ~0ull, al = ~0ull;
+    if (active) {
 #pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-            dh |= __shfl_xor_sync(0xffffffffu, dh, d);
-            dl |= __shfl_xor_sync(0xffffffffu, dl, d);
+        for (int i = 0; i < 8; ++i) kk[i] = key_at(pos_of(w * 256 + lane * 8 + i));
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            oh |= kk[i].hi;
+            ol |= kk[i].lo;
+            ah &= kk[i].hi;
+            al &= kk[i].lo;
         }
-        if (lane == 0) {
-            red[0][w] = dh;
-            red[1][w] = dl;
-        }
+    }
+    // fs: the first bit in which the samples differ (where OR and AND differ).
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        oh |= __shfl_xor_sync(0xffffffffu, oh, d);
+        ol |= __shfl_xor_sync(0xffffffffu, ol, d);
+        ah &= __shfl_xor_sync(0xffffffffu, ah, d);
+        al &= __shfl_xor_sync(0xffffffffu, al, d);
+    }
+    if (lane == 0) {
+        red[0][w] = oh;
+        red[1][w] = ol;
+        red[2][w] = ah;
+        red[3][w] = al;
     }
     __syncthreads();
     uint64_t dh = 0, dl = 0;
+    {
+        uint64_t h1 = 0, l1 = 0, h0 = ~0ull, l0 = ~0ull;
 #pragma unroll
-    for (int q = 0; q < SAMPLE_THREADS / 32; ++q) {
-        dh |= red[0][q];
-        dl |= red[1][q];
+        for (int q = 0; q < SAMPLE_THREADS / 32; ++q) {
+            h1 |= red[0][q];
+            l1 |= red[1][q];
+            h0 &= red[2][q];
+            l0 &= red[3][q];
+        }
+        dh = h1 ^ h0;
+        dl = l1 ^ l0;
     }
     const uint32_t fs = (dh | dl) ? clz128(dh, dl) : 128u;
-    if (w * 256 < S) {
+    // Order the samples by packed keys (window after the samples' common
+    // prefix, 12-bit sample index): warp runs of 256, then merges.  The order
+    // only picks quantiles; the chosen candidates are sorted by full key below.
+    if (active) {
         uint64_t v[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const uint32_t e = w * 256 + lane * 8 + i;
-            v[i] = fs < 128 ? ((window64(to_key(smp[e]), fs) & ~0xFFFull) | e) : e;
+            v[i] = fs < 128 ? ((window64(kk[i], fs) & ~0xFFFull) | e) : e;
         }
-        warp_bitonic64<8>(v, lane);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) sv[pad(w * 256 + lane * 8 + i)] = v[i];
+        warp_merge_sort64<8>(v, sv, w * 256, lane);
     }
     __syncthreads();
     for (uint32_t run = 256; run < S; run <<= 1) {
         const uint32_t o = threadIdx.x * 8;
         uint64_t ov[8];
-        const bool active = o < S;
-        if (active) {
+        const bool act = o < S;
+        if (act) {
             const uint32_t a0 = o & ~(2 * run - 1), b0 = a0 + run;  // run: a power of two
             const uint32_t d = o - a0;
             uint32_t ia = merge_split64(sv, a0, run, b0, run, d);
@@ -1458,7 +1489,7 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
             }
         }
         __syncthreads();
-        if (active) {
+        if (act) {
 #pragma unroll
             for (int i = 0; i < 8; ++i) sv[pad(o + i)] = ov[i];
         }
@@ -1470,7 +1501,8 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     // sorts them by full key.
     {
         const uint32_t j = threadIdx.x;
-        cands[j] = j < k ? smp[sv[pad(((j + 1) * S) / (k + 1))] & 0xFFF] : from_key(key_max());
+        cands[j] = from_key(j < k ? key_at(pos_of(sv[pad(((j + 1) * S) / (k + 1))] & 0xFFF))
+                                  : key_max());
     }
     __syncthreads();
     const bool out_of_order = threadIdx.x + 1 < k &&
@@ -1523,26 +1555,29 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     if (keep) {
         const uint32_t pos = warp_cnt[w] + __popc(bal & lanemask_lt());
         out[pos] = from_key(cand);
-        smp[pos] = from_key(cand);  // candidates were read before the barrier
+        cands[pos] = from_key(cand);  // candidates were read before the barriers
     }
     const uint32_t kp2 = next_pow2(u + 1);
     for (uint32_t q = u + threadIdx.x; q + 1 < kp2; q += SAMPLE_THREADS)
         out[q] = from_key(key_max());
     __syncthreads();
     // Lookup table over the TBL_BITS bits after the splitters' common prefix.
-    const Key s0 = to_key(smp[0]), sl = to_key(smp[u - 1]);
+    const Key s0 = to_key(cands[0]), sl = to_key(cands[u - 1]);
     const uint32_t f = u >= 2 ? clz128(s0.hi ^ sl.hi, s0.lo ^ sl.lo) : 128u;
     if (f < 128) {
         // The splitters' window bits first (non-decreasing, as the splitters
         // are sorted), into the packed-key area, which is free by now; then
-        // each table entry is a binary search over those 16-bit values.
+        // each table entry is the number of splitters whose window bits are
+        // below the entry's value (a binary search over those values).
         uint16_t *wb = reinterpret_cast<uint16_t *>(sv);
         for (uint32_t j = threadIdx.x; j < u; j += SAMPLE_THREADS)
-            wb[j] = (uint16_t)window_bits(to_key(smp[j]), f);
+            wb[j] = (uint16_t)window_bits(to_key(cands[j]), f);
         __syncthreads();
+        // Thread t fills entries 8t .. 8t + 7 (and one more thread the last
+        // entry): two searches bound the splitters of its 8 window values,
+        // then each entry searches only between them.
         uint16_t *T = tbl + (uint64_t)si * TBL_STRIDE;
-        for (uint32_t wv = threadIdx.x; wv <= (uint32_t)TBL_N; wv += SAMPLE_THREADS) {
-            uint32_t lo = 0, hi = u;
+        auto lower = [&](uint32_t lo, uint32_t hi, uint32_t wv) -> uint32_t {
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
                 if (wb[mid] < wv)
@@ -1550,8 +1585,21 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
                 else
                     hi = mid;
             }
-            T[wv] = (uint16_t)lo;
+            return lo;
+        };
+        static_assert(TBL_N == SAMPLE_THREADS * 8, "table entries per thread");
+        const uint32_t w0 = threadIdx.x * 8;
+        uint32_t lo = lower(0, u, w0);
+        const uint32_t hi = lower(lo, u, w0 + 8);
+        uint32_t tv[4];
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+            const uint32_t t0 = lower(lo, hi, w0 + i);
+            lo = lower(t0, hi, w0 + i + 1);
+            tv[i / 2] = t0 | (lo << 16);
         }
+        *reinterpret_cast<uint4 *>(T + w0) = make_uint4(tv[0], tv[1], tv[2], tv[3]);
+        if (threadIdx.x == 0) T[TBL_N] = (uint16_t)lower(0, u, TBL_N);
     }
     if (threadIdx.x == 0) {
         nspl[si] = u | (f << 16);
@@ -1659,21 +1707,34 @@ __global__ void __launch_bounds__(PART_THREADS, 2) k_count(SortArgs a, const Seg
                 const unsigned long long g = warp_sum((unsigned long long)got);
                 if (lane == 0 && g) atomicAdd(&cnt_ctr->window_used, g);
             } else {
+                // Depth 0 with a.key2 (a fresh round gathered here): also keep
+                // key bytes 16..31 for round 1, as k_gather does.
+                const bool save = a.key2 && s.depth == 0;
                 uint64_t off[PART_ITEMS];
 #pragma unroll
                 for (int c = 0; c < PART_ITEMS; ++c) {
                     const uint32_t e = lo + c * 32 + lane;
                     off[c] = e < s.len ? string_offset(a.offs, a.off_width, I[e]) + s.depth : 0;
                 }
+                uint32_t got = 0;
 #pragma unroll
                 for (int c = 0; c < PART_ITEMS; ++c) {
                     const uint32_t e = lo + c * 32 + lane;
                     if (e < s.len) {
                         kk[c] = load_key(a.arena, a.arena_bytes, off[c]);
                         KW[e] = from_key(kk[c]);
+                        if (save) {
+                            a.key2[I[e]] =
+                                from_key(load_key(a.arena, a.arena_bytes, off[c] + KEY_BYTES));
+                            ++got;
+                        }
                     } else {
                         kk[c] = key_max();
                     }
+                }
+                if (save) {
+                    const unsigned long long g = warp_sum((unsigned long long)got);
+                    if (lane == 0 && g) atomicAdd(&cnt_ctr->window_saved, g);
                 }
             }
         } else {
@@ -2006,8 +2067,7 @@ __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, Count cnt,
             len = end - off;
         }
         const uint32_t p = s.start + off;
-        uint32_t slot = warp_append(&c->n_bound, len > 0 && off > 0);
-        if (len > 0 && off > 0) B[slot] = make_uint2(p, s.depth);
+        const bool bnd = len > 0 && off > 0;
         if (len == 1 && ob) {
             a.idx[0][p] = a.idx[1][p];
             a.key[0][p] = a.key[1][p];
@@ -2022,35 +2082,29 @@ __global__ void k_emit(SortArgs a, const Seg *__restrict__ L, Count cnt,
             direct = !ob && !key_is_end(k);
             if (!direct) nch = (len + EQ_TILE - 1) / EQ_TILE;
         }
-        emit_next_warp(N, c, direct, p, len, s.depth + KEY_BYTES);
-        {
-            // nch equality work items per bucket: warp-level exclusive sum.
-            uint32_t incl = nch;
+        // Every list reservation of the bucket is issued before any result
+        // is used (boundary, next round, equality work items here; the
+        // length-selected lists in append_by_length).
+        const WarpRes rb = warp_reserve(&c->n_bound, bnd), rn = warp_reserve(&c->n_next, direct);
+        // nch equality work items per bucket: warp-level exclusive sum.
+        uint32_t incl = nch;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-                if ((threadIdx.x & 31) >= (uint32_t)d) incl += y;
-            }
-            const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
-            uint32_t base = 0;
-            if ((threadIdx.x & 31) == 31 && tot) base = atomicAdd(&c->n_equal, tot);
-            base = __shfl_sync(0xffffffffu, base, 31) + incl - nch;
-            for (uint32_t ch = 0; ch < nch; ++ch)
-                E[base + ch] = Seg{p, len, s.depth, ob | (ch << SEG_CHUNK_SHIFT)};
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if ((threadIdx.x & 31) >= (uint32_t)d) incl += y;
         }
-        const Seg o{p, len, s.depth, flags};
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t ebase = 0;
+        if ((threadIdx.x & 31) == 31 && tot) ebase = atomicAdd(&c->n_equal, tot);
         const bool rng = multi && !(b & 1);
-        const bool w1 = rng && len <= (uint32_t)WARP1_CAP;
-        const bool w8 = rng && !w1 && len <= a.warp8_cap;
-        const bool sm = rng && !w1 && !w8 && len <= (uint32_t)SMALL_CAP;
-        const bool lg = rng && !w1 && !w8 && !sm;
-        slot = warp_append(&c->n_w1, w1);
-        if (w1) W1[slot] = o;
-        slot = warp_append(&c->n_w8, w8);
-        if (w8) W8[slot] = o;
-        append_small(S, c, sm, o);
-        slot = warp_append(&c->n_large_next, lg);
-        if (lg) L2[slot] = o;
+        append_by_length(Seg{p, len, s.depth, flags}, rng, a.warp8_cap, W1, W8, S, L2,
+                         &c->n_large_next, c);
+        const uint32_t tb = warp_slot(rb), tn = warp_slot(rn);
+        if (bnd) B[tb] = make_uint2(p, s.depth);
+        if (direct) N[tn] = Seg{p, len, s.depth + KEY_BYTES, 0u};
+        ebase = __shfl_sync(0xffffffffu, ebase, 31) + incl - nch;
+        for (uint32_t ch = 0; ch < nch; ++ch)
+            E[ebase + ch] = Seg{p, len, s.depth, ob | (ch << SEG_CHUNK_SHIFT)};
     }
     if (threadIdx.x == 0) atomicAdd(&c->partitioned, (unsigned long long)s.len);
     }
@@ -3055,11 +3109,10 @@ __global__ void k_g_after_classify(GraphState *g, const Counters *c,
     g->n_large = nl;
     g->levels = 0;
     if (g->round < 64) g->live[g->round] = c->live_next;
-    const bool fresh = g->round == 0;
-    // Round 0 streams the arena in index order with a separate gather; later
-    // rounds gather inside the first level's count unless that is switched off.
-    g->first = (!fresh && g->fused) ? 1u : 0u;
-    cudaGraphSetConditional(h_gather, (nl > 0 && (fresh || !g->fused)) ? 1u : 0u);
+    const bool fused = gather_fused(g->fused, g->round == 0, c->gather_elems);
+    g->fused_round = fused ? 1u : 0u;
+    g->first = fused ? 1u : 0u;
+    cudaGraphSetConditional(h_gather, (nl > 0 && !fused) ? 1u : 0u);
     cudaGraphSetConditional(h_level, nl > 0 ? 1u : 0u);
 }
 
@@ -3115,7 +3168,7 @@ __global__ void k_g_round_end(GraphState *g, const Counters *c, Seg *R, const Se
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         R[i] = N[i];
     if (!last_cta(&g->ticket)) return;
-    const bool fused = g->round > 0 && g->fused;
+    const bool fused = g->fused_round != 0;
     g->small_segments += (unsigned long long)c->n_w1 + c->n_w8 + c->n_small + c->n_small2 +
                          c->n_small3;
     g->partitioned += c->partitioned;
@@ -3250,8 +3303,7 @@ static inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b -
 // it.  The attribute belongs to the function in the current device's context,
 // so it is set once per device (bit d of the mask), for all kernels at once;
 // two threads that race here both set the same values, which is harmless.
-static constexpr int SAMPLE_SMEM =
-    SAMPLES_MAX * sizeof(ulonglong2) + (SAMPLES_MAX + SAMPLES_MAX / 8) * sizeof(uint64_t);
+static constexpr int SAMPLE_SMEM = (SAMPLES_MAX + SAMPLES_MAX / 8) * sizeof(uint64_t);
 static void set_smem_attrs() {
     static std::atomic<uint64_t> done{0};
     int dev = 0;

@@ -105,3 +105,7 @@ def test_kernel_bytes_with_kept_windows():
     sep = bench.kernel_bytes(NS(**base, window_saved=100, window_used=40), w)
     assert sep["gather"] == 150 * (4 + w + 32) + 100 * 32 - 40 * w
     assert sep["count_gather"] == 0
+    base["gather_fused"] = 150  # round 0 gathers inside its count too
+    fused = bench.kernel_bytes(NS(**base, window_saved=100, window_used=40), w)
+    assert fused["gather"] == 0
+    assert fused["count_gather"] == 150 * (4 + w + 32) + 100 * 32 - 40 * w

@@ -18,6 +18,7 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_WARP8_CAP, 128),
     (pyssort.SSORT_PARAM_OVERLAP, 0),
     (pyssort.SSORT_PARAM_FUSED_GATHER, 0),
+    (pyssort.SSORT_PARAM_FUSED_GATHER, 2),
     (pyssort.SSORT_PARAM_TARGET_BUCKET, 128),
     (pyssort.SSORT_PARAM_TARGET_BUCKET, 1024),
     (pyssort.SSORT_PARAM_WARP1_DEEP, 0),
@@ -86,6 +87,7 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_WARP8_CAP, 512),
                              (pyssort.SSORT_PARAM_OVERLAP, 2),
                              (pyssort.SSORT_PARAM_FUSED_GATHER, -1),
+                             (pyssort.SSORT_PARAM_FUSED_GATHER, 3),
                              (pyssort.SSORT_PARAM_TARGET_BUCKET, 4096),
                              (pyssort.SSORT_PARAM_WARP1_DEEP, -1),
                              (pyssort.SSORT_PARAM_WARP1_DEEP, 4097),
@@ -145,6 +147,24 @@ def test_kept_keys_with_separate_gather():
         p, l = s.sort_host(ss.arena, ss.offs)
         st = s.stats()
     assert st.gather_fused == 0 and st.window_saved > 0 and st.window_used > 0
+    assert np.array_equal(p, rp) and np.array_equal(l, rl)
+
+
+@pytest.mark.parametrize("mode,graph", [(1, 0), (1, 1), (2, 0), (2, 1)])
+def test_round0_gather_inside_count(mode, graph):
+    """Round 0's first partition level gathers its keys inside the count and
+    keeps key bytes 16..31 there for round 1, under mode 2 and, for a round 0
+    of at most 4 M keys (here 2 M URLs), under the default mode 1; in the host
+    loop and in the device-driven loop."""
+    ss = pyssort.gen_urls(2_000_000, seed=64)
+    rp, rl = pyoracle.oracle_sort(ss.arena, ss.offs)
+    with pyssort.Sorter(0) as s:
+        s.set_param(pyssort.SSORT_PARAM_FUSED_GATHER, mode)
+        s.set_param(pyssort.SSORT_PARAM_GRAPH, graph)
+        p, l = s.sort_host(ss.arena, ss.offs)
+        st = s.stats()
+    assert st.gather_fused == st.gather_elems > 0
+    assert st.window_saved > 0 and st.window_used > 0
     assert np.array_equal(p, rp) and np.array_equal(l, rl)
 
 
