@@ -282,7 +282,9 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
 #define SSORT_PARAM_SCATTER 11       /* 0 (default): the partition scatter lays each tile out
                                         in shared memory in output order; 1: it stages only
                                         indices and destinations and reads each key from the
-                                        tile (in L2) in output order, at more CTAs per SM */
+                                        tile (in L2) in output order, at more CTAs per SM;
+                                        2: as 0, with each bucket run of keys written by one
+                                        asynchronous bulk copy from shared memory */
 #define SSORT_PARAM_GRAPH 7          /* 1: device-driven round loop: the sort runs as a CUDA
                                         graph whose rounds and partition levels are
                                         conditional loops (no host round trip between

@@ -843,7 +843,7 @@ int ssort_set_param(ssort_ctx *ctx, int param, int64_t value) {
             ctx->block_lean = (uint32_t)value;
             return SSORT_OK;
         case SSORT_PARAM_SCATTER:
-            if (value != 0 && value != 1) return fail(SSORT_EINVAL, "scatter must be 0 or 1");
+            if (value < 0 || value > 2) return fail(SSORT_EINVAL, "scatter must be 0, 1 or 2");
             ctx->scatter_variant = (uint32_t)value;
             return SSORT_OK;
         case SSORT_PARAM_L2_PREFETCH:

@@ -137,7 +137,7 @@ struct SortArgs {
     uint32_t warp8_cap;      // largest segment for the one-warp sort (64..WARP8_CAP)
     uint32_t warp1_deep;     // in-warp refinement steps of the one-per-lane sort
     uint32_t l2_prefetch;    // partition kernels stream their next tile into L2 ahead
-    uint32_t scatter_staged_idx;  // scatter stages indices only (k_scatter2)
+    uint32_t scatter_staged_idx;  // 0: k_scatter; 1: indices only (k_scatter2); 2: bulk key runs
     uint32_t block_lean;     // CTA sort: neighbour LCPs from the packed windows
     uint32_t match_vote;     // count kernel ranks with ballots instead of the match unit
     uint32_t warp_merge;     // warp sorts of packed keys: local networks + merge passes

@@ -1807,6 +1807,11 @@ struct ScatterSmem {
     uint32_t wsum[SCATTER_THREADS / 32];
 };
 
+// BULK: each bucket run of keys leaves shared memory as one asynchronous bulk
+// copy to global memory (cp.async.bulk, issued by the thread that owns the
+// bucket; keys are 16 bytes, so every run starts and ends on a 16-byte
+// boundary at both ends); the indices are stored by the threads as before.
+template <bool BULK>
 __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const Seg *__restrict__ L,
                                                              Count cnt,
                                                              const uint32_t *__restrict__ tile_base,
@@ -1819,6 +1824,7 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
     constexpr uint32_t QPT = (NB_MAX + 1) / SCATTER_THREADS;  // buckets per thread (4)
     const uint32_t nL = count_of(cnt);
     const uint32_t total_tiles = tile_base[nL];
+    bool any_bulk = false;  // this thread issued bulk copies (BULK)
     for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const uint32_t si = find_seg(tile_base, nL, t);
         const Seg s = L[si];
@@ -1905,13 +1911,43 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
         __syncthreads();
         ulonglong2 *Kout = a.keyb(ib ^ 1) + s.start;
         uint32_t *Iout = a.idxb(ib ^ 1) + s.start;
-        for (uint32_t i = threadIdx.x; i < tlen; i += SCATTER_THREADS) {
-            const uint32_t o = sm.dst[i];
-            Kout[o] = sm.key[i];
-            Iout[o] = sm.idx[i];
+        if constexpr (BULK) {
+            // The staged keys were written by other threads through the
+            // generic proxy; make them visible to the bulk copies' async proxy.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bool issued = false;
+#pragma unroll
+            for (uint32_t j = 0; j < QPT; ++j) {
+                const uint32_t q = threadIdx.x * QPT + j;
+                if (cnt[j]) {
+                    const uint32_t src =
+                        (uint32_t)__cvta_generic_to_shared(&sm.key[sm.tstart[q]]);
+                    asm volatile(
+                        "cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(
+                            Kout + sm.gbase[q]),
+                        "r"(src), "r"(cnt[j] * 16u)
+                        : "memory");
+                    issued = true;
+                }
+            }
+            if (issued) asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            for (uint32_t i = threadIdx.x; i < tlen; i += SCATTER_THREADS)
+                Iout[sm.dst[i]] = sm.idx[i];
+            // The next tile restages into sm.key: wait until the copies have
+            // read it (their global writes complete by the kernel's end).
+            if (issued) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+            any_bulk |= issued;
+        } else {
+            for (uint32_t i = threadIdx.x; i < tlen; i += SCATTER_THREADS) {
+                const uint32_t o = sm.dst[i];
+                Kout[o] = sm.key[i];
+                Iout[o] = sm.idx[i];
+            }
         }
         __syncthreads();
     }
+    // Every bulk copy's writes complete before the thread exits.
+    if (BULK && any_bulk) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 
@@ -3315,7 +3351,9 @@ static void set_smem_attrs() {
                          (int)sizeof(PartSmem));
     cudaFuncSetAttribute(k_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(PartSmem));
-    cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(ScatterSmem));
+    cudaFuncSetAttribute(k_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(ScatterSmem));
     cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(Scatter2Smem));
@@ -3497,14 +3535,19 @@ void launch_scatter(const SortArgs &a, const Seg *L, Count nL, const uint32_t *t
                     const uint32_t *cm_base, const uint32_t *cm_scan, int grid, cudaStream_t st) {
     if (!nL.dev && !nL.host) return;
     set_smem_attrs();
+    if (a.scatter_staged_idx == 2) {
+        k_scatter<true><<<grid, SCATTER_THREADS, sizeof(ScatterSmem), st>>>(
+            a, L, nL, tile_base, nspl, cm_base, cm_scan);
+        return;
+    }
     if (a.scatter_staged_idx) {
         // three CTAs per SM where k_scatter fits two (grid: two per SM)
         k_scatter2<<<grid / 2 * 3, SCATTER_THREADS, sizeof(Scatter2Smem), st>>>(
             a, L, nL, tile_base, nspl, cm_base, cm_scan);
         return;
     }
-    k_scatter<<<grid, SCATTER_THREADS, sizeof(ScatterSmem), st>>>(a, L, nL, tile_base, nspl,
-                                                                  cm_base, cm_scan);
+    k_scatter<false><<<grid, SCATTER_THREADS, sizeof(ScatterSmem), st>>>(
+        a, L, nL, tile_base, nspl, cm_base, cm_scan);
 }
 
 void launch_emit(const SortArgs &a, const Seg *L, Count nL, const uint32_t *tile_base,

@@ -31,6 +31,7 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_DIGIT_BITS, 8),
     (pyssort.SSORT_PARAM_DIGIT_BITS, 9),
     (pyssort.SSORT_PARAM_SCATTER, 1),
+    (pyssort.SSORT_PARAM_SCATTER, 2),
     (pyssort.SSORT_PARAM_BLOCK_LEAN, 1),
     (pyssort.SSORT_PARAM_BLOCK_LEAN, 2),
     (pyssort.SSORT_PARAM_GRAPH, 2),
@@ -101,7 +102,7 @@ def test_out_of_range_parameters_are_rejected():
                              (pyssort.SSORT_PARAM_GRAPH_MAX_LEVELS, 0),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 7),
                              (pyssort.SSORT_PARAM_DIGIT_BITS, 11),
-                             (pyssort.SSORT_PARAM_SCATTER, 2),
+                             (pyssort.SSORT_PARAM_SCATTER, 3),
                              (99, 1)]:
             with pytest.raises(pyssort.SsortError) as e:
                 s.set_param(param, value)
