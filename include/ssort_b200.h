@@ -86,9 +86,11 @@ int ssort_sort_device(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byt
  * SSORT_EINVAL.  The caller still passes the inputs and the perm (and
  * optional lcp) outputs, and a cudaStream_t (NULL = the legacy default
  * stream); the call waits for that stream (cudaStreamSynchronize) before it
- * returns, on failure too, so the results are complete.  The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress), so
- * it should come before any stream capture.  Every call uses the same array
+ * returns, on failure too, so the results are complete.  Because of that
+ * wait, and the host reads of counters between kernels, it must not be called
+ * while its stream (or, for its first call on a device, which looks up the
+ * array's address with cudaGetSymbolAddress, any stream) is being captured
+ * into a CUDA graph.  Every call uses the same array
  * and leaves its contents behind (what must start at zero is cleared by each
  * call).  Calls that overlapped on the GPU would race on the array; the
  * library prevents that within one process by taking a lock for the whole
