@@ -149,7 +149,8 @@ def _tied_window_strings(n, lead, alpha, seed):
                                                 (0, 0, 1)])
 @pytest.mark.parametrize("n,lead,alpha,full", [(200, 2, 26, False), (1500, 2, 26, False),
                                                (700, 2, 26, False), (1500, 1, 2, True),
-                                               (200, 1, 2, True), (300, 1, 2, True)])
+                                               (200, 1, 2, True), (300, 1, 2, True),
+                                               (3500, 2, 26, False), (3500, 1, 2, True)])
 def test_tied_packed_windows(n, lead, alpha, full, prefetch, lean, merge):
     """Segments of the one-warp (<= 256) and CTA (<= 2048) sorts whose packed
     keys tie: runs of up to 64 tied records are put in order in place, longer
@@ -194,7 +195,7 @@ def test_saved_round1_keys_batched():
     """A batched call of URL instances, small (sorted on chip in round 0) and
     large (gathered in round 0, keys kept for round 1): every instance is the
     oracle's sort of it alone."""
-    sizes = [3000, 1500, 700_000, 2000, 400_000, 10, 2049]
+    sizes = [3000, 1500, 700_000, 2000, 400_000, 10, 2049, 4096, 4097]
     sets = [pyssort.gen_urls(m, seed=500 + k) for k, m in enumerate(sizes)]
     parts, offs, base = [], [], 0
     for st in sets:
@@ -243,3 +244,18 @@ def test_pointer_array_one_large_span(sorter):
     ref_perm, ref_lcp = pyoracle.oracle_sort(ss.arena, ss.offs)
     assert np.array_equal(perm, ref_perm)
     assert np.array_equal(lcp, ref_lcp)
+
+
+@pytest.mark.parametrize("n", [2047, 2048, 2049, 3000, 4096, 8192])
+def test_cta_sort_cutoff(n, sorter):
+    """Inputs at and above the CTA sort's 2048-string cutoff: up to 2048
+    strings are sorted on chip without a partition pass, larger inputs are
+    partitioned first (round 0: the whole input; round 1: the shared-prefix
+    case's single segment).  Both match the oracle."""
+    for strings in (cases.uniform(n, 900 + n), cases.shared8(n, 950 + n)):
+        arena, offs = cases.arena_of(strings)
+        perm, lcp = sorter.sort_host(arena, offs)
+        st = sorter.stats()
+        ref_perm, ref_lcp = pyoracle.oracle_sort(arena, offs)
+        assert np.array_equal(perm, ref_perm) and np.array_equal(lcp, ref_lcp)
+        assert (st.partitioned == 0) == (n <= 2048)
