@@ -1349,6 +1349,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(SortArgs a, const Seg
 
 // ---- splitter selection: one CTA per large segment ------------------------
 constexpr int SAMPLE_THREADS = 512;
+constexpr uint32_t SAMPLE_KEEP = 1024;  // samples kept in shared memory (16 KB)
 
 __device__ __forceinline__ uint32_t hash32(uint32_t x) {
     x ^= x >> 16;
@@ -1381,10 +1382,13 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
                                                uint32_t si, ulonglong2 *spl, uint32_t *nspl,
                                                uint16_t *tbl, uint32_t *ntiles, uint32_t *cm_size,
                                                bool from_arena) {
-    // sv: the samples' packed sort keys (padded layout).  The sampled keys
-    // themselves stay in registers; the chosen candidates are read again.
+    // sv: the samples' packed sort keys (padded layout).  Up to SAMPLE_KEEP
+    // samples are loaded by all threads into smp and the candidates are read
+    // from there; larger samples stay in registers and only the chosen
+    // candidates are read again.
     extern __shared__ __align__(16) unsigned char sample_smem[];
     uint64_t *sv = reinterpret_cast<uint64_t *>(sample_smem);
+    ulonglong2 *smp = reinterpret_cast<ulonglong2 *>(sv + SAMPLES_MAX + SAMPLES_MAX / 8);
     __shared__ ulonglong2 cands[SAMPLE_THREADS];
     __shared__ uint32_t warp_cnt[SAMPLE_THREADS / 32 + 1];
     __shared__ uint64_t red[4][SAMPLE_THREADS / 32];
@@ -1414,11 +1418,20 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     };
     // Warp w < S / 256 holds samples w * 256 + lane * 8 + i (i < 8).
     const bool active = w * 256 < S;
+    const bool kept = S <= SAMPLE_KEEP;  // block-uniform
+    if (kept) {
+        for (uint32_t i = threadIdx.x; i < S; i += SAMPLE_THREADS)
+            smp[i] = from_key(key_at(pos_of(i)));
+        __syncthreads();
+    }
     Key kk[8];
     uint64_t oh = 0, ol = 0, ah = ~0ull, al = ~0ull;
     if (active) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) kk[i] = key_at(pos_of(w * 256 + lane * 8 + i));
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t e = w * 256 + lane * 8 + i;
+            kk[i] = kept ? to_key(smp[e]) : key_at(pos_of(e));
+        }
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             oh |= kk[i].hi;
@@ -1501,8 +1514,12 @@ __device__ __forceinline__ void sample_segment(const SortArgs &a, const Seg *__r
     // sorts them by full key.
     {
         const uint32_t j = threadIdx.x;
-        cands[j] = from_key(j < k ? key_at(pos_of(sv[pad(((j + 1) * S) / (k + 1))] & 0xFFF))
-                                  : key_max());
+        if (j < k) {
+            const uint32_t e = sv[pad(((j + 1) * S) / (k + 1))] & 0xFFF;
+            cands[j] = kept ? smp[e] : from_key(key_at(pos_of(e)));
+        } else {
+            cands[j] = from_key(key_max());
+        }
     }
     __syncthreads();
     const bool out_of_order = threadIdx.x + 1 < k &&
@@ -3339,7 +3356,8 @@ static inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b -
 // it.  The attribute belongs to the function in the current device's context,
 // so it is set once per device (bit d of the mask), for all kernels at once;
 // two threads that race here both set the same values, which is harmless.
-static constexpr int SAMPLE_SMEM = (SAMPLES_MAX + SAMPLES_MAX / 8) * sizeof(uint64_t);
+static constexpr int SAMPLE_SMEM =
+    (SAMPLES_MAX + SAMPLES_MAX / 8) * sizeof(uint64_t) + SAMPLE_KEEP * sizeof(ulonglong2);
 static void set_smem_attrs() {
     static std::atomic<uint64_t> done{0};
     int dev = 0;
