@@ -274,9 +274,10 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                         its first sort runs on 32-bit packed keys (21 key
                                         bits and the position; ties on those bits are put in
                                         order afterwards); 0 (default): full-key finish */
-#define SSORT_PARAM_L2_PREFETCH 9    /* 1 (default): the partition's count and scatter
-                                        kernels ask for their next tile to be streamed into
-                                        L2 (bulk prefetch) while they work on the current one */
+#define SSORT_PARAM_L2_PREFETCH 9    /* 1: the partition's count and scatter kernels ask
+                                        for their next tile to be streamed into L2 (bulk
+                                        prefetch) while they work on the current one;
+                                        0 (default): no such requests */
 #define SSORT_PARAM_DIGIT_BITS 10    /* 8, 9 or 10 (default 10): digit width of one
                                         partition pass, i.e. a pass splits a segment into
                                         at most 2^bits buckets (2^(bits-1) - 1 sampled

@@ -88,7 +88,7 @@ struct ssort_ctx {
     bool block_prefetch = false;  // double-buffered CTA sort (k_block2)
     uint32_t block_lean = 0;      // CTA sort: 1 finish from the packed windows, 2 also a
                                   // first sort on 32-bit packed keys
-    bool l2_prefetch = true;     // partition kernels prefetch their next tile into L2
+    bool l2_prefetch = false;    // partition kernels prefetch their next tile into L2
     uint32_t digit_bits = 10;    // a partition pass makes at most 2^digit_bits buckets
     uint32_t scatter_variant = 0;  // 1: the scatter stages indices only (k_scatter2)
     bool match_vote = false;       // count kernel ranks keys with ballots

@@ -26,7 +26,7 @@ SETTINGS = [
     (pyssort.SSORT_PARAM_WARP1_DEEP, 4096),
     (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 0),
     (pyssort.SSORT_PARAM_BLOCK_PREFETCH, 1),
-    (pyssort.SSORT_PARAM_L2_PREFETCH, 0),
+    (pyssort.SSORT_PARAM_L2_PREFETCH, 1),
     (pyssort.SSORT_PARAM_GRAPH, 1),
     (pyssort.SSORT_PARAM_DIGIT_BITS, 8),
     (pyssort.SSORT_PARAM_DIGIT_BITS, 9),
