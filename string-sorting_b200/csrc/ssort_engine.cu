@@ -659,15 +659,38 @@ int ssort_sort_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes, 
         ctx->st = ctx->own_stream;
         // Device arena: the bytes plus 16 zero bytes of padding.
         SS_TRY(ctx->ensure(ctx->arena, arena_bytes + 16));
-        SS_TRY(ctx->ensure(ctx->offs, n * off_width));
         SS_TRY(ctx->ensure(ctx->perm, n * 4 * (lcp ? 2 : 1)));
         uint8_t *d_arena = (uint8_t *)ctx->arena.p;
         uint32_t *d_perm = (uint32_t *)ctx->perm.p;
         uint32_t *d_lcp = lcp ? d_perm + n : nullptr;
         SS_CUDA(cudaMemcpyAsync(d_arena, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->st));
         SS_CUDA(cudaMemsetAsync(d_arena + arena_bytes, 0, 16, ctx->st));
-        SS_CUDA(cudaMemcpyAsync(ctx->offs.p, offs, n * off_width, cudaMemcpyHostToDevice, ctx->st));
-        SS_TRY(sort_device_impl(ctx, d_arena, arena_bytes + 16, ctx->offs.p, off_width, n, d_perm,
+        // 8-byte offsets into an arena below 4 GB cross the link as 4-byte
+        // ones: the host threads narrow them into a pinned buffer while the
+        // copy engine moves the arena, halving the offsets' share of the
+        // transfer.  If any offset does not fit, the 8-byte ones are sent.
+        int ow = off_width;
+        const void *src = offs;
+        if (off_width == 8 && arena_bytes + 16 <= 0xFFFFFFFFull && n >= NARROW_OFFS_MIN_N) {
+            SS_TRY(ctx->ensure_host(ctx->h_offs, n * 4));
+            uint32_t *o32 = (uint32_t *)ctx->h_offs.p;
+            const uint64_t *o64 = (const uint64_t *)offs;
+            const int64_t nn = (int64_t)n;
+            uint64_t mx = 0;
+#pragma omp parallel for reduction(max : mx)
+            for (int64_t i = 0; i < nn; ++i) {
+                const uint64_t v = o64[i];
+                mx = std::max(mx, v);
+                o32[i] = (uint32_t)v;
+            }
+            if (mx <= 0xFFFFFFFFull) {
+                ow = 4;
+                src = o32;
+            }
+        }
+        SS_TRY(ctx->ensure(ctx->offs, n * ow));
+        SS_CUDA(cudaMemcpyAsync(ctx->offs.p, src, n * ow, cudaMemcpyHostToDevice, ctx->st));
+        SS_TRY(sort_device_impl(ctx, d_arena, arena_bytes + 16, ctx->offs.p, ow, n, d_perm,
                                 d_lcp));
         SS_CUDA(cudaMemcpyAsync(perm, d_perm, n * 4, cudaMemcpyDeviceToHost, ctx->st));
         if (lcp) SS_CUDA(cudaMemcpyAsync(lcp, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));

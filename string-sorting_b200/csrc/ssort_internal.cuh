@@ -43,6 +43,7 @@ constexpr int WARP8_CAP = 256;
 constexpr uint32_t WARP1_DEEP = 64;       // default in-warp refinement steps (16 bytes each)
 constexpr uint32_t WARP1_DEEP_MAX = 4096;
 constexpr uint32_t KEY2_MIN_N = 1u << 20;           // sorts that may save round-1 keys
+constexpr uint64_t NARROW_OFFS_MIN_N = 1u << 20;    // host sorts that narrow 8-byte offsets
 constexpr uint32_t KEY2_MIN_BYTES_PER_STRING = 24;  // ... when the arena has this many
 constexpr double KEY2_MIN_ROUND1_LIVE = 0.25;       // ... and the last sort's round-1 share
 constexpr int SMALL_CAP = 2048;

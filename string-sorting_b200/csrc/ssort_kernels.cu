@@ -1970,9 +1970,9 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
 
 // The same scatter with only indices and destinations staged: the slots of
 // the tile in output order record where each record sits in the tile, and
-// the write-out reads the keys from there (the tile was streamed into L2 by
-// the previous tile's bulk prefetch, and the reads stay inside the tile's
-// 64 KB).  48 KB of shared memory and about half the registers of k_scatter,
+// the write-out reads the keys from there (the tile was just read, and with
+// SortArgs::l2_prefetch also streamed into L2 ahead; the reads stay inside
+// the tile's 64 KB).  48 KB of shared memory and about half the registers of k_scatter,
 // so three or four CTAs share an SM instead of two.
 struct Scatter2Smem {
     uint32_t idx[PART_TILE];    // indices in output order
