@@ -103,7 +103,10 @@ int ssort_sort_device_noalloc(const uint8_t *d_arena, uint64_t arena_bytes, cons
 
 /* The same from host buffers: copies arena and offsets to the device, sorts,
  * and copies perm (and lcp when not NULL) back.  Pinned host buffers make the
- * copies faster but are not required. */
+ * copies faster but are not required.  With off_width 8, an arena below 4 GB
+ * and n >= 2^20, the offsets are narrowed to 4 bytes on the host (into a
+ * pinned buffer the context keeps) while the arena is being copied, and only
+ * those cross to the device; the caller's buffers are only read. */
 int ssort_sort_host(ssort_ctx *ctx, const uint8_t *arena, uint64_t arena_bytes,
                     const void *offs, int off_width, uint64_t n, uint32_t *perm,
                     uint32_t *lcp);
