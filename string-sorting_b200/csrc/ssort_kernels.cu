@@ -1972,8 +1972,8 @@ __global__ void __launch_bounds__(SCATTER_THREADS) k_scatter(SortArgs a, const S
 // the tile in output order record where each record sits in the tile, and
 // the write-out reads the keys from there (the tile was just read, and with
 // SortArgs::l2_prefetch also streamed into L2 ahead; the reads stay inside
-// the tile's 64 KB).  48 KB of shared memory and about half the registers of k_scatter,
-// so three or four CTAs share an SM instead of two.
+// the tile's 64 KB).  48 KB of shared memory and about half the registers of
+// k_scatter, so three or four CTAs share an SM instead of two.
 struct Scatter2Smem {
     uint32_t idx[PART_TILE];    // indices in output order
     uint32_t dst[PART_TILE];    // destinations in output order
