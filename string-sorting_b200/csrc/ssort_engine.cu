@@ -794,20 +794,27 @@ int ssort_sort_strings(ssort_ctx *ctx, unsigned char **strings, size_t n, uint32
         if (lcp_out)
             SS_CUDA(cudaMemcpyAsync(lcp_out, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));
         if (use_span) {
-            // One span: the sorted strings' offsets into it come back in
-            // order, and the pointer array is rewritten sequentially (no
-            // random gather through a copy of the old array).
-            SS_TRY(ctx->ensure(ctx->aux2, n * 8));
-            SS_TRY(ctx->ensure_host(ctx->h_arena, n * 8));  // unused by the span path
+            // One span: the sorted strings' offsets into it (in the
+            // offsets' own width) come back in order, and the pointer array
+            // is rewritten sequentially (no random gather through a copy of
+            // the old array).
+            SS_TRY(ctx->ensure(ctx->aux2, n * ow));
+            SS_TRY(ctx->ensure_host(ctx->h_arena, n * ow));  // unused by the span path
             LAUNCH(ctx, "sorted_offs",
-                   launch_sorted_offs(d_perm, ctx->offs.p, ow, n, (uint64_t *)ctx->aux2.p,
-                                      ctx->st));
-            uint64_t *so = (uint64_t *)ctx->h_arena.p;
-            SS_CUDA(cudaMemcpyAsync(so, ctx->aux2.p, n * 8, cudaMemcpyDeviceToHost, ctx->st));
+                   launch_sorted_offs(d_perm, ctx->offs.p, ow, n, ctx->aux2.p, ow, ctx->st));
+            SS_CUDA(cudaMemcpyAsync(ctx->h_arena.p, ctx->aux2.p, n * ow, cudaMemcpyDeviceToHost,
+                                    ctx->st));
             SS_CUDA(cudaStreamSynchronize(ctx->st));
             unsigned char *base = (unsigned char *)lo;
+            if (ow == 4) {
+                const uint32_t *so = (const uint32_t *)ctx->h_arena.p;
 #pragma omp parallel for if (nn > 100000)
-            for (int64_t i = 0; i < nn; ++i) strings[i] = base + so[i];
+                for (int64_t i = 0; i < nn; ++i) strings[i] = base + so[i];
+            } else {
+                const uint64_t *so = (const uint64_t *)ctx->h_arena.p;
+#pragma omp parallel for if (nn > 100000)
+                for (int64_t i = 0; i < nn; ++i) strings[i] = base + so[i];
+            }
             return SSORT_OK;
         }
         SS_CUDA(cudaMemcpyAsync(perm, d_perm, n * 4, cudaMemcpyDeviceToHost, ctx->st));
@@ -1236,7 +1243,7 @@ int ssort_sort_text_host(ssort_ctx *ctx, const uint8_t *text, uint64_t text_len,
         SS_TRY(sort_device_impl(ctx, d_text, text_len + 16, ctx->offs.p, w, n, d_perm, d_lcp));
         SS_TRY(ctx->ensure(ctx->aux2, n * 8));
         LAUNCH(ctx, "sorted_offs",
-               launch_sorted_offs(d_perm, ctx->offs.p, w, n, (uint64_t *)ctx->aux2.p, ctx->st));
+               launch_sorted_offs(d_perm, ctx->offs.p, w, n, ctx->aux2.p, 8, ctx->st));
         SS_CUDA(cudaMemcpyAsync(sorted_offs, ctx->aux2.p, n * 8, cudaMemcpyDeviceToHost, ctx->st));
         if (lcp) SS_CUDA(cudaMemcpyAsync(lcp, d_lcp, n * 4, cudaMemcpyDeviceToHost, ctx->st));
         SS_CUDA(cudaStreamSynchronize(ctx->st));

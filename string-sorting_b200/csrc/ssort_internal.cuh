@@ -325,7 +325,7 @@ void launch_text_starts(uint8_t *text, uint64_t len, uint8_t delim, const uint32
                         uint64_t n, void *offs, int off_width, cudaStream_t st);
 void launch_iota_offs(void *offs, int off_width, uint64_t n, cudaStream_t st);
 void launch_sorted_offs(const uint32_t *perm, const void *offs, int off_width, uint64_t n,
-                        uint64_t *out, cudaStream_t st);
+                        void *out, int out_width, cudaStream_t st);
 // One request joining or leaving the server's batch (see k_join / k_unbase).
 struct ReqJob {
     uint64_t region_base, arena_bytes;

@@ -1103,13 +1103,19 @@ __global__ void k_iota_offs(void *offs, int off_width, uint64_t n) {
 }
 
 // out[k] = offs[perm[k]]: the sorted string starts.
+// out[k] = offs[perm[k]], as out_width-byte values (4 only when every
+// offset fits, which the caller knows).
 __global__ void k_sorted_offs(const uint32_t *__restrict__ perm, const void *offs, int off_width,
-                              uint64_t n, uint64_t *out) {
+                              uint64_t n, void *out, int out_width) {
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
          k += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t i = perm[k];
-        out[k] = off_width == 8 ? static_cast<const uint64_t *>(offs)[i]
-                                : static_cast<const uint32_t *>(offs)[i];
+        const uint64_t o = off_width == 8 ? static_cast<const uint64_t *>(offs)[i]
+                                          : static_cast<const uint32_t *>(offs)[i];
+        if (out_width == 8)
+            static_cast<uint64_t *>(out)[k] = o;
+        else
+            static_cast<uint32_t *>(out)[k] = (uint32_t)o;
     }
 }
 
@@ -3479,9 +3485,10 @@ void launch_iota_offs(void *offs, int off_width, uint64_t n, cudaStream_t st) {
 }
 
 void launch_sorted_offs(const uint32_t *perm, const void *offs, int off_width, uint64_t n,
-                        uint64_t *out, cudaStream_t st) {
+                        void *out, int out_width, cudaStream_t st) {
     const uint64_t g = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
-    k_sorted_offs<<<(unsigned)(g ? g : 1), 256, 0, st>>>(perm, offs, off_width, n, out);
+    k_sorted_offs<<<(unsigned)(g ? g : 1), 256, 0, st>>>(perm, offs, off_width, n, out,
+                                                         out_width);
 }
 
 void launch_byte_hist(const uint8_t *arena, uint64_t arena_bytes, const void *offs, int off_width,
