@@ -243,7 +243,7 @@ int ssort_get_stats(const ssort_ctx *ctx, ssort_stats *out);
                                        partition, 32..2048 (default 512) */
 #define SSORT_PARAM_WARP8_CAP 2     /* largest segment sorted by one warp, 64..256
                                        (default 256); larger ones go to the CTA sort */
-#define SSORT_PARAM_OVERLAP 3       /* 1 (default): in round 0 the on-chip sorts run
+#define SSORT_PARAM_OVERLAP 3       /* 1 (default): in every round the on-chip sorts run
                                        on a side stream beside the partition; 0: one stream */
 #define SSORT_PARAM_FUSED_GATHER 4  /* 1 (default): the first partition level of a
                                        round gathers the keys it counts, except in a round 0

@@ -137,12 +137,12 @@ int ssort_ctx::launch_small(const SortArgs &a, Seg *nxt, SmallDone &d) {
 int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint32_t &n_next,
                      uint32_t round_no) {
     // A fresh round (round 0 of a sort, or by the caller's choice) streams
-    // the arena in index order with a separate gather and overlaps the
-    // on-chip sorts with the partition; a deep round gathers keys at random
-    // inside the first count and keeps one stream (the random gather is
-    // latency-bound and measured slower when it shares its SMs).
+    // the arena in index order with a separate gather; a deep round gathers
+    // keys at random inside the first count.  Every round overlaps its
+    // on-chip sorts with its partition levels (a side stream), unless
+    // switched off or timing kernels one by one.
     fresh_round = round_mode >= 0 ? round_mode == 0 : round_no == 0;
-    overlap_round = side && hp && !prof && overlap && fresh_round;
+    overlap_round = side && hp && !prof && overlap;
     if (!overlap_round) return round_body(a, cur, n_cur, nxt, n_next, round_no);
     // Fork the round onto the high-priority stream and join it back.
     cudaStream_t user = st;
