@@ -48,10 +48,10 @@ struct ssort_ctx {
     // The on-chip sorts of a round run on `side` while the partition levels
     // continue on `st` (fork/join through the two events).  Without a side
     // stream, or while profiling, they run on `st`.
-    // Within a round the partition levels run on `hp` (highest priority,
-    // forked from and joined back into `st`) and the on-chip sorts on `side`
-    // (lowest priority), so that the CTA scheduler serves the partition's
-    // critical path first and the sorts fill the SMs it leaves idle.
+    // Within a round the partition levels run on `hp` (forked from and
+    // joined back into `st`) and the on-chip sorts on `side`, both at the
+    // default priority, so that the sorts fill the SMs the partition's
+    // latency-bound passes leave idle.
     cudaStream_t side = nullptr, hp = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_round = nullptr;
     bool overlap_round = false;  // this round runs its on-chip sorts on `side`
