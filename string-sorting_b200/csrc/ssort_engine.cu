@@ -98,8 +98,13 @@ int ssort_ctx::fork_small() {
 // the partition levels on the side stream.
 int ssort_ctx::launch_small(const SortArgs &a, Seg *nxt, SmallDone &d) {
     const bool overlap = overlap_round;
-    cudaStream_t s2 = overlap ? side : st;
-    if (overlap) SS_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));  // recorded by fork_small
+    // The warp and equality-bucket work on `side`, the CTA sorts on `side2`:
+    // disjoint segments, so the two also run beside each other.
+    cudaStream_t s2 = overlap ? side : st, s3 = overlap ? side2 : st;
+    if (overlap) {
+        SS_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));  // recorded by fork_small
+        SS_CUDA(cudaStreamWaitEvent(side2, ev_fork, 0));
+    }
     Counters *dc = ws.ctr;
     // One pass of CTAs over the entries (no CTA loops over several): short
     // CTAs let the scheduler give SMs back to the partition kernels.  The
@@ -121,7 +126,7 @@ int ssort_ctx::launch_small(const SortArgs &a, Seg *nxt, SmallDone &d) {
         const uint32_t per_cta = (uint32_t)SMALL_THREADS / (64u << k);
         LAUNCH(this, "block",
                launch_block(a, lists[k], hspan(d.s[k], d.s[k] + n), k, nxt, dc,
-                            grid(n, per_cta * (block_prefetch ? 4u : 1u)), s2, block_prefetch));
+                            grid(n, per_cta * (block_prefetch ? 4u : 1u)), s3, block_prefetch));
         d.s[k] += n;
     }
     n = h_ctr->n_equal - d.e;
@@ -142,7 +147,7 @@ int ssort_ctx::round(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt, uint
     // on-chip sorts with its partition levels (a side stream), unless
     // switched off or timing kernels one by one.
     fresh_round = round_mode >= 0 ? round_mode == 0 : round_no == 0;
-    overlap_round = side && hp && !prof && overlap;
+    overlap_round = side && side2 && hp && !prof && overlap;
     if (!overlap_round) return round_body(a, cur, n_cur, nxt, n_next, round_no);
     // Fork the round onto the high-priority stream and join it back.
     cudaStream_t user = st;
@@ -221,6 +226,8 @@ int ssort_ctx::round_body(const SortArgs &a, Seg *cur, uint32_t n_cur, Seg *nxt,
     if (overlap_round) {
         SS_CUDA(cudaEventRecord(ev_join, side));
         SS_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+        SS_CUDA(cudaEventRecord(ev_join2, side2));
+        SS_CUDA(cudaStreamWaitEvent(st, ev_join2, 0));
     }
     LAUNCH(this, "boundary", launch_boundary(a, ws.B, dc, g4, st));
     SS_TRY(sync_counters());
@@ -448,6 +455,7 @@ int sort_device_impl(ssort_ctx *ctx, const uint8_t *d_arena, uint64_t arena_byte
     if (rc != SSORT_OK) {
         cudaStreamSynchronize(ctx->st);
         if (ctx->side) cudaStreamSynchronize(ctx->side);
+        if (ctx->side2) cudaStreamSynchronize(ctx->side2);
         if (ctx->hp) cudaStreamSynchronize(ctx->hp);
         ctx->recs.clear();
         ctx->ev_used = 0;
@@ -528,6 +536,8 @@ int ssort_ctx_create(int device, ssort_ctx **out) {
         // on two streams of equal priority: giving the partition the higher
         // one measured 0.6 % slower on 50 M URLs.
         SS_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+        SS_CUDA(cudaStreamCreateWithFlags(&ctx->side2, cudaStreamNonBlocking));
+        SS_CUDA(cudaEventCreateWithFlags(&ctx->ev_join2, cudaEventDisableTiming));
         SS_CUDA(cudaStreamCreateWithFlags(&ctx->hp, cudaStreamNonBlocking));
         SS_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
         SS_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
@@ -568,11 +578,14 @@ void ssort_ctx_destroy(ssort_ctx *ctx) {
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
         if (ctx->side) cudaStreamSynchronize(ctx->side);
+        if (ctx->side2) cudaStreamSynchronize(ctx->side2);
         if (ctx->hp) cudaStreamSynchronize(ctx->hp);
         if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
         if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+        if (ctx->ev_join2) cudaEventDestroy(ctx->ev_join2);
         if (ctx->ev_round) cudaEventDestroy(ctx->ev_round);
         if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->side2) cudaStreamDestroy(ctx->side2);
         if (ctx->hp) cudaStreamDestroy(ctx->hp);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         return SSORT_OK;

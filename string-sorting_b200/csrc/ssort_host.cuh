@@ -49,11 +49,11 @@ struct ssort_ctx {
     // continue on `st` (fork/join through the two events).  Without a side
     // stream, or while profiling, they run on `st`.
     // Within a round the partition levels run on `hp` (forked from and
-    // joined back into `st`) and the on-chip sorts on `side`, both at the
-    // default priority, so that the sorts fill the SMs the partition's
-    // latency-bound passes leave idle.
-    cudaStream_t side = nullptr, hp = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_round = nullptr;
+    // joined back into `st`), the warp sorts and equality buckets on `side`
+    // and the CTA sorts on `side2`, all at the default priority, so that the
+    // sorts fill the SMs the partition's latency-bound passes leave idle.
+    cudaStream_t side = nullptr, side2 = nullptr, hp = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr, ev_round = nullptr;
     bool overlap_round = false;  // this round runs its on-chip sorts on `side`
     bool fresh_round = false;    // this round gathers round-0 style (see round())
     int round_mode = -1;         // -1: fresh iff round_no == 0; 0: fresh; 1: deep
